@@ -1,0 +1,390 @@
+"""Benchmark: FP64 strided-batch tridiagonal solves on a 256^3 cube.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = three solves of the 256^3 FP64 cube (65,536 systems of n=256),
+along solvedim 0, 1 and 2 in turn (tridDmtsvStridedBatch through the C ABI),
+on inputs resident in HBM.  Inputs: a_i, c_i ~ U(-1,1), b_i = |a_i|+|c_i|+U(1,2),
+d ~ N(0,1), seeded (synthetic stand-in for the workload's distribution).
+
+Metric: solve GB/s = algorithmic bytes (read a,b,c,d + write x = 40 B per
+unknown) / time, whole job (all ranks).  Each array is 134 MB, so every launch
+streams 671 MB (> 126 MB L2): no L2 flush is needed between steps.
+
+Extra keys: roofline (dominant kernel vs the measured HBM copy bandwidth),
+cpu_baseline (the reference CPU solver compiled from the reference sources,
+all host threads, on the same cube), e2e (the same solves through the C ABI
+from pinned host buffers, host<->device copies inside the timed region),
+clocks (nvidia-smi samples during the timed region), gpu_launches.
+
+--impl reference: times the reference's own CPU implementation of the path
+(scalar/src/cpu/trid_cpu.cpp built into oracle/_ref) on the same workload
+with every host thread; with N>1 only rank 0 runs it.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+N = 256
+DIMS = [N, N, N]
+BYTES_PER_UNKNOWN = 5 * 8          # read a,b,c,d + write x (FP64)
+UNKNOWNS = N * N * N
+BYTES_PER_SOLVE = BYTES_PER_UNKNOWN * UNKNOWNS
+METRIC = "Solve GB/s (% of B200 HBM peak); fwd+adjoint vs fwd-only time at <=1e-8 grad err"
+WORKLOAD = "FP64 256^3 strided-batch solves along solvedim 0,1,2 (65,536 systems of n=256 each)"
+FALLBACK_HBM = 6650.0
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM, "fallback"
+
+
+def make_inputs(seed=1234):
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(-1, 1, UNKNOWNS)
+    c = rng.uniform(-1, 1, UNKNOWNS)
+    b = np.abs(a) + np.abs(c) + rng.uniform(1, 2, UNKNOWNS)
+    d = rng.standard_normal(UNKNOWNS)
+    return a, b, c, d
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def read_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+    summary (profiles/dram_traffic_256cube_fp64.txt: 'solvedim <k> <bytes>')."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic_256cube_fp64.txt")
+    out = {}
+    try:
+        with open(path) as f:
+            for line in f:
+                p = line.split()
+                if len(p) == 3 and p[0] == "solvedim":
+                    out[int(p[1])] = float(p[2])
+    except OSError:
+        pass
+    return out
+
+
+def cpu_baseline_ref(a, b, c, d, reps=2):
+    """The reference CPU solver (oracle/_ref) on the full cube, all threads."""
+    import ctypes
+
+    from oracle import oracle
+
+    lib = oracle.ref_lib()
+    f = lib.tridDmtsvStridedBatch
+    f.restype = ctypes.c_int
+    dims = (ctypes.c_int * 3)(*DIMS)
+    best = None
+    placed = {}
+    for aligned in (False, True):
+        placed[aligned] = [oracle._placed(x, aligned) for x in (a, b, c, d)]
+    for _ in range(reps + 1):
+        t0 = time.perf_counter()
+        for sd in range(3):
+            arrs = placed[sd > 0]
+            st = f(*[x.ctypes.data_as(ctypes.c_void_p) for x in arrs], None, 3, sd, dims, dims)
+            assert st == 0
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    return best
+
+
+def run_ours(args):
+    import torch
+
+    import tridsolver_b200 as tb
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    a, b, c, d0 = make_inputs(1234 + rank)
+    ta, tb_, tc, td = (torch.from_numpy(x).cuda() for x in (a, b, c, d0))
+    stream = torch.cuda.current_stream()
+
+    def step(ev=None):
+        for sd in range(3):
+            if ev is not None:
+                ev[sd][0].record(stream)
+            st = tb.tridDmtsvStridedBatch(ta, tb_, tc, td, None, 3, sd, DIMS, DIMS)
+            if st != 0:
+                raise tb.TridError(st, "tridDmtsvStridedBatch")
+            if ev is not None:
+                ev[sd][1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # per-launch timing of each axis on the launching stream
+    per_axis = [0.0, 0.0, 0.0]
+    for _ in range(args.steps):
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(3)]
+        step(ev)
+        torch.cuda.synchronize()
+        for sd in range(3):
+            per_axis[sd] += ev[sd][0].elapsed_time(ev[sd][1]) / args.steps
+    # whole-step timing (the reported value)
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    cvd = [x for x in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if x.strip()]
+    gpu_index = cvd[local] if local < len(cvd) else str(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(gpu_index) as clk:
+        t_wall = time.time()
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        stop.record(stream)
+        torch.cuda.synchronize()
+        # short timed regions get the same load continued (untimed) so that the
+        # 200 ms clock samples see it
+        while time.time() < t_wall + 1.2:
+            step()
+            torch.cuda.synchronize()
+    ms_total = start.elapsed_time(stop)
+    if dist:
+        t = torch.tensor([ms_total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+        dist.barrier()
+    ms_step = ms_total / args.steps
+    value = world * 3 * BYTES_PER_SOLVE / (ms_step * 1e-3) / 1e9
+
+    # end to end through the C ABI from pinned host buffers
+    e2e_steps = max(1, min(args.steps, 5))
+    ha, hb, hc, hd = (torch.from_numpy(x).pin_memory() for x in (a, b, c, d0))
+    hout = torch.empty_like(hd).pin_memory()
+    for _ in range(2):
+        for h, t in ((ha, ta), (hb, tb_), (hc, tc), (hd, td)):
+            t.copy_(h, non_blocking=True)
+        step()
+        hout.copy_(td, non_blocking=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        for h, t in ((ha, ta), (hb, tb_), (hc, tc), (hd, td)):
+            t.copy_(h, non_blocking=True)
+        step()
+        hout.copy_(td, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_ms /= e2e_steps
+    e2e_value = world * 3 * BYTES_PER_SOLVE / (e2e_ms * 1e-3) / 1e9
+
+    peak, peak_kind = measured_peak()
+    dom = int(np.argmax(per_axis))
+    achieved = BYTES_PER_SOLVE / (per_axis[dom] * 1e-3) / 1e9
+    traffic = read_traffic().get(dom)
+    result = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded U/N distributions of the workload)",
+        "config": {"workload": WORKLOAD, "dims": DIMS, "solves_per_step": 3,
+                   "bytes_per_solve": BYTES_PER_SOLVE, "l2": "inputs 671 MB/launch > 126 MB L2, no flush",
+                   "parallelism": f"replicas{world}", "hbm_fraction_of_" + peak_kind: round(value / world / peak, 4),
+                   "per_axis_ms": [round(x, 5) for x in per_axis],
+                   "per_axis_gbs": [round(BYTES_PER_SOLVE / (x * 1e-3) / 1e9, 1) for x in per_axis]},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "kernel": f"solvedim {dom}",
+                     "traffic": traffic, "algorithmic_bytes": BYTES_PER_SOLVE},
+        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s",
+                "h2d_bytes_per_step": 4 * UNKNOWNS * 8, "d2h_bytes_per_step": UNKNOWNS * 8},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline_entry(a, b, c, d0)
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result))
+
+
+def cpu_baseline_entry(a, b, c, d):
+    from oracle import oracle
+
+    threads = os.cpu_count()
+    if oracle.ref_available():
+        sec = cpu_baseline_ref(a, b, c, d)
+        kind = "reference"
+        sample = "full 256^3 cube, solvedim 0,1,2 once each, best of 2 after one warm-up"
+    else:
+        sec = None
+        kind = "port"
+        sample = "reference CPU build missing"
+    return {"value": round(3 * BYTES_PER_SOLVE / sec / 1e9, 3) if sec else None, "unit": "GB/s",
+            "cores": threads, "kind": kind, "sample": sample,
+            "ms_per_step": round(sec * 1e3, 2) if sec else None}
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    from oracle import oracle
+
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+        return
+    import ctypes
+
+    a, b, c, d = make_inputs(1234)
+    lib = oracle.ref_lib()
+    f = lib.tridDmtsvStridedBatch
+    f.restype = ctypes.c_int
+    dims = (ctypes.c_int * 3)(*DIMS)
+    placed = {al: [oracle._placed(x, al) for x in (a, b, c, d)] for al in (False, True)}
+
+    def step():
+        for sd in range(3):
+            arrs = placed[sd > 0]
+            f(*[x.ctypes.data_as(ctypes.c_void_p) for x in arrs], None, 3, sd, dims, dims)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    sec = (time.perf_counter() - t0) / args.steps
+    value = 3 * BYTES_PER_SOLVE / sec / 1e9
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "dims": DIMS, "solves_per_step": 3,
+                   "implementation": "reference scalar/src/cpu/trid_cpu.cpp (OpenMP), "
+                                     "solvedim 0 via its scalar path"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads,
+                         "kind": "reference", "sample": "full 256^3 cube per step"},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        os.environ.setdefault("OMP_STACKSIZE", "64M")
+        os.environ.setdefault("OMP_PROC_BIND", "close")
+        run_reference(args)
+    else:
+        os.environ.setdefault("OMP_STACKSIZE", "64M")
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,131 @@
+/*
+ * tridsolver_b200 -- public C ABI of the scalar batched tridiagonal solver
+ * (libtridb200.so).
+ *
+ * Drop-in for the reference's strided-batch API:
+ *   scalar/include/trid_cpu.h:53-82   (9-argument form; declared here over
+ *                                      DEVICE pointers, one B200 GPU)
+ *   scalar/include/trid_cuda.h:44-80  (the 11-argument GPU form with
+ *                                      `int *opts, int sync` is exported under
+ *                                      the same names by the companion library
+ *                                      libtridb200_cudacompat.so, see
+ *                                      include/trid_b200_cudacompat.h)
+ *   scalar/include/trid_common.h:65-76 (tridStatus_t, same values)
+ *
+ * Semantics (same as the reference):
+ *   - a, b, c, d, u are arrays of shape dims[0..ndim-1] (dims[0] fastest),
+ *     padded to pads[0..ndim-1]: element (i0,i1,...) is at
+ *     i0 + pads[0]*(i1 + pads[1]*(i2 + ...)).
+ *   - One independent system per line along axis `solvedim`:
+ *       a_i x_{i-1} + b_i x_i + c_i x_{i+1} = d_i.
+ *     a[0] and c[n-1] of every system are never read.
+ *   - Non-Inc: the solution overwrites d; u is not used (may be NULL).
+ *     Inc:     u += solution; d is left unmodified.
+ *   - dims/pads are HOST arrays; a..u are DEVICE pointers (cudaMalloc or
+ *     managed memory) aligned to their element size.
+ *   - Work is enqueued on the calling thread's stream (tridSetStream, default
+ *     the legacy default stream) and the call returns without synchronising.
+ *
+ * Differences from the reference, all on error paths: invalid arguments
+ * return TRID_STATUS_INVALID_VALUE instead of printing and calling exit()
+ * (trid_cuda.cu:209-219); a failed launch returns
+ * TRID_STATUS_EXECUTION_FAILED instead of aborting; ndim may be 1..8 on
+ * every axis (the reference CPU path assumes 3, its GPU x-path needs
+ * pads[i>=1] == dims[i]).
+ */
+#ifndef TRID_B200_H
+#define TRID_B200_H
+
+#ifdef __cplusplus
+#define TRID_EXTERN_C extern "C"
+#else
+#define TRID_EXTERN_C
+#endif
+
+#define TRID_B200_MAXDIM 8
+
+/* scalar/include/trid_common.h:65-76 -- same names and values. */
+typedef enum {
+  TRID_STATUS_SUCCESS = 0,
+  TRID_STATUS_NOT_INITIALIZED = 1,
+  TRID_STATUS_ALLOC_FAILED = 2,
+  TRID_STATUS_INVALID_VALUE = 3,
+  TRID_STATUS_ARCH_MISMATCH = 4,
+  TRID_STATUS_MAPPING_ERROR = 5,
+  TRID_STATUS_EXECUTION_FAILED = 6,
+  TRID_STATUS_INTERNAL_ERROR = 7,
+  TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED = 8,
+  TRID_STATUS_ZERO_PIVOT = 9
+} tridStatus_t;
+
+/* ---- strided batch: replaces trid_cpu.h:53-60 (tridS/DmtsvStridedBatch) ---- */
+TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatch(const float *a, const float *b, const float *c,
+                                                 float *d, float *u, int ndim, int solvedim,
+                                                 int *dims, int *pads);
+TRID_EXTERN_C tridStatus_t tridDmtsvStridedBatch(const double *a, const double *b,
+                                                 const double *c, double *d, double *u, int ndim,
+                                                 int solvedim, int *dims, int *pads);
+
+/* ---- Inc variants: replace trid_cpu.h:74-82 (tridS/DmtsvStridedBatchInc) ---- */
+TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchInc(const float *a, const float *b,
+                                                    const float *c, float *d, float *u, int ndim,
+                                                    int solvedim, int *dims, int *pads);
+TRID_EXTERN_C tridStatus_t tridDmtsvStridedBatchInc(const double *a, const double *b,
+                                                    const double *c, double *d, double *u,
+                                                    int ndim, int solvedim, int *dims, int *pads);
+
+/* ---- per-array pads: replace trid_cuda.h:61-67 / :79-85
+ *      (tridDmtsvStridedBatchPadded[Inc]); float forms are additions.
+ *      opts is an optional algorithm hint (may be NULL); sync=1 waits for the
+ *      solve to finish before returning. ---- */
+TRID_EXTERN_C tridStatus_t tridDmtsvStridedBatchPadded(
+    const double *a, const int *a_pads, const double *b, const int *b_pads, const double *c,
+    const int *c_pads, double *d, const int *d_pads, double *u, const int *u_pads, int ndim,
+    int solvedim, int *dims, int *opts, int sync);
+TRID_EXTERN_C tridStatus_t tridDmtsvStridedBatchPaddedInc(
+    const double *a, const int *a_pads, const double *b, const int *b_pads, const double *c,
+    const int *c_pads, double *d, const int *d_pads, double *u, const int *u_pads, int ndim,
+    int solvedim, int *dims, int *opts, int sync);
+TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchPadded(
+    const float *a, const int *a_pads, const float *b, const int *b_pads, const float *c,
+    const int *c_pads, float *d, const int *d_pads, float *u, const int *u_pads, int ndim,
+    int solvedim, int *dims, int *opts, int sync);
+TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchPaddedInc(
+    const float *a, const int *a_pads, const float *b, const int *b_pads, const float *c,
+    const int *c_pads, float *d, const int *d_pads, float *u, const int *u_pads, int ndim,
+    int solvedim, int *dims, int *opts, int sync);
+
+/* ---- replaces trid_cuda.h:44 (a no-op in the reference, trid_cuda.cu:612) ---- */
+TRID_EXTERN_C void initTridMultiDimBatchSolve(int ndim, int *dims, int *pads);
+
+/* ---- extensions (no reference counterpart) -------------------------------- */
+
+/* Stream used by every call made from the calling thread (a cudaStream_t;
+ * NULL = legacy default stream). */
+TRID_EXTERN_C tridStatus_t tridSetStream(void *stream);
+TRID_EXTERN_C void *tridGetStream(void);
+
+/* Human-readable name of a status code. */
+TRID_EXTERN_C const char *tridGetStatusString(tridStatus_t status);
+
+/* Algorithm selection for the scalar solves (autotuner hook).
+ *   method 0 = automatic (tuning table, then built-in heuristics)
+ *   method 1 = Thomas, one thread per system, c'/d' in library scratch
+ *   method 2 = partitioned Thomas: per-thread chunks of `chunk` rows reduced to
+ *              a 64-row interface system solved by warp shuffles (PCR)
+ *   chunk      : rows per thread for method 2 (2, 4, 8 or 16; 0 = automatic)
+ *   sys_per_cta: systems per CTA for method 2 on strided axes (4, 8, 16; 0 = auto)
+ * Applies to calls from the calling thread. */
+TRID_EXTERN_C tridStatus_t tridSetMethod(int method, int chunk, int sys_per_cta);
+
+/* Load an autotuning table written by tridsolver_b200.autotune (text lines
+ * "<dtype> <axis> <nmax> <method> <chunk> <sys_per_cta>"); NULL clears it.
+ * Process-wide. */
+TRID_EXTERN_C tridStatus_t tridLoadTuningTable(const char *path);
+
+/* The method/chunk/sys_per_cta the dispatcher would use for a problem
+ * (dtype_bytes 4 or 8, axis 0 = contiguous solve, 1 = strided). */
+TRID_EXTERN_C tridStatus_t tridQueryMethod(int dtype_bytes, int axis, int n, int *method,
+                                           int *chunk, int *sys_per_cta);
+
+#endif /* TRID_B200_H */

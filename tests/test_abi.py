@@ -1,0 +1,135 @@
+"""C-ABI boundary checks that need no GPU.
+
+* both shared libraries load and export every function include/*.h declares;
+* argument validation happens on the host, before any CUDA call, and returns
+  TRID_STATUS_INVALID_VALUE instead of exiting the process as the reference
+  does (scalar/src/cuda/trid_cuda.cu:209-219).
+"""
+
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+import tridsolver_b200 as tb
+from tridsolver_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INCLUDE = os.path.join(ROOT, "include")
+
+INVALID = 3
+
+
+def declared_c_functions(header):
+    text = open(os.path.join(INCLUDE, header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"TRID_EXTERN_C[^;(]*?\b(\w+)\s*\(", text)))
+
+
+def exported(path):
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True,
+                         check=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if " T " in line}
+
+
+@pytest.mark.parametrize("header,lib", [
+    ("trid_b200.h", _lib.LIB_MAIN),
+    ("trid_b200_cudacompat.h", _lib.LIB_COMPAT),
+])
+def test_library_exports_every_declared_symbol(header, lib):
+    names = declared_c_functions(header)
+    assert names, header
+    syms = exported(lib)
+    missing = [n for n in names if n not in syms]
+    assert not missing, missing
+
+
+def test_extension_headers_exported_by_main_library():
+    syms = exported(_lib.LIB_MAIN)
+    for header in sorted(os.listdir(INCLUDE)):
+        if header in ("trid_b200_cudacompat.h",):
+            continue
+        for name in declared_c_functions(header):
+            assert name in syms, (header, name)
+
+
+def test_libraries_load_and_bind():
+    assert tb.lib() is not None
+    assert tb.compat_lib() is not None
+    assert tb.lib().tridGetStatusString(3) == b"TRID_STATUS_INVALID_VALUE"
+
+
+def _fake(n=64):
+    # host buffers only stand in for aligned device pointers: every call below
+    # is rejected during host-side validation, before any CUDA call.
+    buf = (ctypes.c_double * n)()
+    return ctypes.addressof(buf), buf
+
+
+@pytest.mark.parametrize("ndim,solvedim,dims,pads", [
+    (0, 0, [4], [4]),            # ndim < 1
+    (9, 0, [1] * 9, [1] * 9),    # ndim > 8
+    (2, 2, [4, 4], [4, 4]),      # solvedim out of range
+    (2, -1, [4, 4], [4, 4]),
+    (2, 0, [4, -1], [4, 4]),     # negative extent
+    (2, 0, [4, 4], [3, 4]),      # pads < dims
+])
+def test_invalid_geometry_rejected(ndim, solvedim, dims, pads):
+    p, _keep = _fake()
+    st = tb.tridDmtsvStridedBatch(p, p, p, p, None, ndim, solvedim, dims, pads)
+    assert st == INVALID
+    st = tb.tridSmtsvStridedBatchInc(p, p, p, p, p, ndim, solvedim, dims, pads)
+    assert st == INVALID
+
+
+def test_null_and_misaligned_pointers_rejected():
+    p, _keep = _fake()
+    assert tb.tridDmtsvStridedBatch(p, p, p, None, None, 1, 0, [8], [8]) == INVALID
+    assert tb.tridDmtsvStridedBatchInc(p, p, p, p, None, 1, 0, [8], [8]) == INVALID
+    assert tb.tridDmtsvStridedBatch(p + 4, p, p, p, None, 1, 0, [8], [8]) == INVALID
+    assert tb.tridSmtsvStridedBatch(p + 2, p, p, p, None, 1, 0, [8], [8]) == INVALID
+
+
+def test_bad_opts_rejected_by_padded_and_compat():
+    p, _keep = _fake()
+    st = tb.tridDmtsvStridedBatchPadded(p, [8], p, [8], p, [8], p, [8], None, [8], 1, 0, [8],
+                                        opts=[7], sync=0)
+    assert st == INVALID
+    L = tb.compat_lib()
+    opts = _lib.int_array([9, 0, 0])
+    st = L.tridDmtsvStridedBatch(p, p, p, p, None, 1, 0, _lib.int_array([8]),
+                                 _lib.int_array([8]), opts, 0)
+    assert st == INVALID
+
+
+def test_method_override_and_query():
+    L = tb.lib()
+    m, ch, spc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    assert L.tridQueryMethod(8, 0, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+    assert (m.value, ch.value) == (2, 8)
+    assert L.tridQueryMethod(8, 1, 5000, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+    assert m.value == 1
+    tb.set_method(1)
+    assert L.tridQueryMethod(8, 0, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+    assert m.value == 1
+    tb.set_method(0)
+    with pytest.raises(tb.TridError):
+        tb.set_method(2, chunk=3)
+
+
+def test_tuning_table_roundtrip(tmp_path):
+    L = tb.lib()
+    path = tmp_path / "tune.txt"
+    path.write_text("# dtype axis nmax method chunk spc\nf64 1 300 2 16 4\nf32 0 100 1 0 0\n")
+    assert L.tridLoadTuningTable(str(path).encode()) == 0
+    m, ch, spc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    L.tridQueryMethod(8, 1, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc))
+    assert (m.value, ch.value, spc.value) == (2, 16, 4)
+    L.tridQueryMethod(4, 0, 64, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc))
+    assert m.value == 1
+    bad = tmp_path / "bad.txt"
+    bad.write_text("f16 0 1 1 0 0\n")
+    assert L.tridLoadTuningTable(str(bad).encode()) == INVALID
+    assert L.tridLoadTuningTable(None) == 0

@@ -1,0 +1,323 @@
+// Scalar strided-batch C ABI (9-argument form over device pointers) and the
+// library's host runtime: per-thread stream and method override, per-device
+// scratch, tuning table, argument validation and dispatch.
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "dispatch.cuh"
+
+namespace tridb200 {
+
+// ------------------------------------------------------------------ state --
+static thread_local cudaStream_t tl_stream = nullptr;
+static thread_local MethodChoice tl_force = {0, 0, 0};
+
+cudaStream_t current_stream() { return tl_stream; }
+
+struct ScratchBuf {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+};
+static std::mutex g_scratch_mu;
+static std::vector<ScratchBuf> g_scratch;  // indexed by device
+
+void *scratch(size_t bytes) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if ((int)g_scratch.size() <= dev) g_scratch.resize(dev + 1);
+  ScratchBuf &s = g_scratch[dev];
+  if (s.bytes >= bytes) return s.ptr;
+  if (s.ptr) {
+    // kernels already queued may still read the old buffer
+    cudaDeviceSynchronize();
+    cudaFree(s.ptr);
+    s.ptr = nullptr;
+    s.bytes = 0;
+  }
+  void *p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  s.ptr = p;
+  s.bytes = bytes;
+  return p;
+}
+
+struct TuneEntry {
+  int dtype_bytes, axis, nmax, method, chunk, spc;
+};
+static std::mutex g_tune_mu;
+static std::vector<TuneEntry> g_tune;
+
+// ------------------------------------------------------- method selection --
+static int chunk_for(int n, int dtype_bytes) {
+  (void)dtype_bytes;
+  if (n <= 64) return 2;
+  if (n <= 128) return 4;
+  if (n <= 256) return 8;
+  if (n <= 512) return 16;
+  return 0;  // too long for a register-resident partition
+}
+
+MethodChoice choose_method(int dtype_bytes, int axis, int n, int opt_hint) {
+  MethodChoice m = tl_force;
+  if (m.method == 0 && opt_hint != 0) {
+    // reference opts: 1/2 = plain Thomas kernels, 3/4 = Thomas-PCR hybrid
+    if (opt_hint == 1 || opt_hint == 2) m.method = 1;
+    if (opt_hint == 3 || opt_hint == 4) m.method = 2;
+  }
+  if (m.method == 0) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (const TuneEntry &e : g_tune) {
+      if (e.dtype_bytes == dtype_bytes && e.axis == axis && n <= e.nmax) {
+        m = {e.method, e.chunk, e.spc};
+        break;
+      }
+    }
+  }
+  if (m.method == 0) m.method = chunk_for(n, dtype_bytes) ? 2 : 1;
+  if (m.method == 2) {
+    const int need = chunk_for(n, dtype_bytes);
+    if (need == 0) {
+      m.method = 1;  // longer than any register-resident partition
+    } else if (m.chunk < need) {
+      m.chunk = need;
+    }
+    if (m.spc == 0) m.spc = (dtype_bytes == 8) ? 8 : 16;
+  }
+  return m;
+}
+
+// ------------------------------------------------------------- validation --
+tridStatus_t make_geom(int ndim, int solvedim, const int *dims, const int *const pads[5],
+                       bool inc, Geom &g) {
+  if (ndim < 1 || ndim > kMaxDim || solvedim < 0 || solvedim >= ndim || dims == nullptr)
+    return TRID_STATUS_INVALID_VALUE;
+  for (int q = 0; q < 5; ++q)
+    if (pads[q] == nullptr && (q < 4 || inc)) return TRID_STATUS_INVALID_VALUE;
+  int64_t total = 1;
+  for (int k = 0; k < ndim; ++k) {
+    if (dims[k] < 0) return TRID_STATUS_INVALID_VALUE;
+    for (int q = 0; q < 5; ++q)
+      if (pads[q] && (q < 4 || inc) && pads[q][k] < dims[k]) return TRID_STATUS_INVALID_VALUE;
+    total *= (dims[k] > 0 ? dims[k] : 1);
+    if (total > ((int64_t)1 << 46)) return TRID_STATUS_INVALID_VALUE;
+  }
+  memset(&g, 0, sizeof(g));
+  g.n = dims[solvedim];
+  g.nod = 0;
+  g.nsys = 1;
+  for (int k = 0; k < ndim; ++k) {
+    if (k == solvedim) continue;
+    g.odims[g.nod] = dims[k];
+    g.nsys *= dims[k];
+    g.nod++;
+  }
+  for (int q = 0; q < 5; ++q) {
+    if (!pads[q] || (q == 4 && !inc)) continue;
+    int64_t cum = 1;
+    int o = 0;
+    for (int k = 0; k < ndim; ++k) {
+      if (k == solvedim)
+        g.stride[q] = cum;
+      else
+        g.ocum[q][o++] = cum;
+      cum *= pads[q][k];
+    }
+  }
+  return TRID_STATUS_SUCCESS;
+}
+
+template <typename T>
+static bool aligned_ptr(const T *p) {
+  return p != nullptr && ((uintptr_t)p % sizeof(T)) == 0;
+}
+
+template <typename T, int INC>
+tridStatus_t solve_strided_batch(const T *a, const T *b, const T *c, T *d, T *u, int ndim,
+                                 int solvedim, const int *dims, const int *const pads[5],
+                                 const int *opts, int sync) {
+  Geom g;
+  const tridStatus_t st = make_geom(ndim, solvedim, dims, pads, INC != 0, g);
+  if (st != TRID_STATUS_SUCCESS) return st;
+  if (!aligned_ptr(a) || !aligned_ptr(b) || !aligned_ptr(c) || !aligned_ptr(d))
+    return TRID_STATUS_INVALID_VALUE;
+  if (INC && !aligned_ptr(u)) return TRID_STATUS_INVALID_VALUE;
+  const int opt = opts ? opts[solvedim] : 0;
+  if (opt < 0 || opt > 5) return TRID_STATUS_INVALID_VALUE;
+  if (g.n == 0 || g.nsys == 0) return TRID_STATUS_SUCCESS;
+
+  const cudaStream_t stream = current_stream();
+  const int axis = (solvedim == 0) ? 0 : 1;
+  const MethodChoice m = choose_method((int)sizeof(T), axis, g.n, opt);
+  cudaError_t e = cudaSuccess;
+  if (m.method == 2) {
+    if (axis == 0)
+      e = launch_xsolve<T, INC>(g, a, b, c, d, u, m.chunk, stream);
+    else
+      e = launch_strided<T, INC>(g, a, b, c, d, u, m.chunk, m.spc, stream);
+  } else {
+    // Thomas with c'/d' in scratch, in batches of systems bounded to ~1 GiB
+    const size_t per_sys = (size_t)2 * g.n * sizeof(T);
+    int64_t ws = (int64_t)(((size_t)1 << 30) / per_sys);
+    ws = std::max<int64_t>(1, std::min<int64_t>(ws, g.nsys));
+    T *work = (T *)scratch(per_sys * (size_t)ws);
+    if (!work) return TRID_STATUS_ALLOC_FAILED;
+    e = launch_generic<T, INC>(g, a, b, c, d, u, work, ws, stream);
+  }
+  if (e != cudaSuccess) return TRID_STATUS_EXECUTION_FAILED;
+  if (sync == 1 && cudaStreamSynchronize(stream) != cudaSuccess) return TRID_STATUS_EXECUTION_FAILED;
+  return TRID_STATUS_SUCCESS;
+}
+
+template tridStatus_t solve_strided_batch<float, 0>(const float *, const float *, const float *,
+                                                    float *, float *, int, int, const int *,
+                                                    const int *const[5], const int *, int);
+template tridStatus_t solve_strided_batch<float, 1>(const float *, const float *, const float *,
+                                                    float *, float *, int, int, const int *,
+                                                    const int *const[5], const int *, int);
+template tridStatus_t solve_strided_batch<double, 0>(const double *, const double *,
+                                                     const double *, double *, double *, int, int,
+                                                     const int *, const int *const[5],
+                                                     const int *, int);
+template tridStatus_t solve_strided_batch<double, 1>(const double *, const double *,
+                                                     const double *, double *, double *, int, int,
+                                                     const int *, const int *const[5],
+                                                     const int *, int);
+
+}  // namespace tridb200
+
+using namespace tridb200;
+
+// ---------------------------------------------------------------- C ABI --
+#ifndef TRID_CUDACOMPAT
+extern "C" tridStatus_t tridSmtsvStridedBatch(const float *a, const float *b, const float *c,
+                                              float *d, float *u, int ndim, int solvedim,
+                                              int *dims, int *pads) {
+  (void)u;
+  const int *p[5] = {pads, pads, pads, pads, pads};
+  return solve_strided_batch<float, 0>(a, b, c, d, nullptr, ndim, solvedim, dims, p, nullptr, 0);
+}
+extern "C" tridStatus_t tridDmtsvStridedBatch(const double *a, const double *b, const double *c,
+                                              double *d, double *u, int ndim, int solvedim,
+                                              int *dims, int *pads) {
+  (void)u;
+  const int *p[5] = {pads, pads, pads, pads, pads};
+  return solve_strided_batch<double, 0>(a, b, c, d, nullptr, ndim, solvedim, dims, p, nullptr, 0);
+}
+extern "C" tridStatus_t tridSmtsvStridedBatchInc(const float *a, const float *b, const float *c,
+                                                 float *d, float *u, int ndim, int solvedim,
+                                                 int *dims, int *pads) {
+  const int *p[5] = {pads, pads, pads, pads, pads};
+  return solve_strided_batch<float, 1>(a, b, c, d, u, ndim, solvedim, dims, p, nullptr, 0);
+}
+extern "C" tridStatus_t tridDmtsvStridedBatchInc(const double *a, const double *b,
+                                                 const double *c, double *d, double *u, int ndim,
+                                                 int solvedim, int *dims, int *pads) {
+  const int *p[5] = {pads, pads, pads, pads, pads};
+  return solve_strided_batch<double, 1>(a, b, c, d, u, ndim, solvedim, dims, p, nullptr, 0);
+}
+#endif
+
+#define TRID_PADDED(NAME, T, INC)                                                              \
+  extern "C" tridStatus_t NAME(const T *a, const int *a_pads, const T *b, const int *b_pads,   \
+                               const T *c, const int *c_pads, T *d, const int *d_pads, T *u,   \
+                               const int *u_pads, int ndim, int solvedim, int *dims,           \
+                               int *opts, int sync) {                                          \
+    const int *p[5] = {a_pads, b_pads, c_pads, d_pads, INC ? u_pads : d_pads};                 \
+    return solve_strided_batch<T, INC>(a, b, c, d, INC ? u : nullptr, ndim, solvedim, dims, p, \
+                                       opts, sync);                                            \
+  }
+TRID_PADDED(tridDmtsvStridedBatchPadded, double, 0)
+TRID_PADDED(tridDmtsvStridedBatchPaddedInc, double, 1)
+TRID_PADDED(tridSmtsvStridedBatchPadded, float, 0)
+TRID_PADDED(tridSmtsvStridedBatchPaddedInc, float, 1)
+
+extern "C" void initTridMultiDimBatchSolve(int ndim, int *dims, int *pads) {
+  (void)ndim;
+  (void)dims;
+  (void)pads;
+}
+
+extern "C" tridStatus_t tridSetStream(void *stream) {
+  tl_stream = (cudaStream_t)stream;
+  return TRID_STATUS_SUCCESS;
+}
+
+extern "C" void *tridGetStream(void) { return (void *)tl_stream; }
+
+extern "C" const char *tridGetStatusString(tridStatus_t s) {
+  switch (s) {
+    case TRID_STATUS_SUCCESS: return "TRID_STATUS_SUCCESS";
+    case TRID_STATUS_NOT_INITIALIZED: return "TRID_STATUS_NOT_INITIALIZED";
+    case TRID_STATUS_ALLOC_FAILED: return "TRID_STATUS_ALLOC_FAILED";
+    case TRID_STATUS_INVALID_VALUE: return "TRID_STATUS_INVALID_VALUE";
+    case TRID_STATUS_ARCH_MISMATCH: return "TRID_STATUS_ARCH_MISMATCH";
+    case TRID_STATUS_MAPPING_ERROR: return "TRID_STATUS_MAPPING_ERROR";
+    case TRID_STATUS_EXECUTION_FAILED: return "TRID_STATUS_EXECUTION_FAILED";
+    case TRID_STATUS_INTERNAL_ERROR: return "TRID_STATUS_INTERNAL_ERROR";
+    case TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED: return "TRID_STATUS_MATRIX_TYPE_NOT_SUPPORTED";
+    case TRID_STATUS_ZERO_PIVOT: return "TRID_STATUS_ZERO_PIVOT";
+  }
+  return "unknown tridStatus_t";
+}
+
+extern "C" tridStatus_t tridSetMethod(int method, int chunk, int sys_per_cta) {
+  if (method < 0 || method > 2) return TRID_STATUS_INVALID_VALUE;
+  if (chunk != 0 && chunk != 2 && chunk != 4 && chunk != 8 && chunk != 16)
+    return TRID_STATUS_INVALID_VALUE;
+  if (sys_per_cta != 0 && sys_per_cta != 4 && sys_per_cta != 8 && sys_per_cta != 16)
+    return TRID_STATUS_INVALID_VALUE;
+  tl_force = {method, chunk, sys_per_cta};
+  return TRID_STATUS_SUCCESS;
+}
+
+extern "C" tridStatus_t tridLoadTuningTable(const char *path) {
+  std::vector<TuneEntry> table;
+  if (path) {
+    FILE *f = fopen(path, "r");
+    if (!f) return TRID_STATUS_INVALID_VALUE;
+    char line[256];
+    while (fgets(line, sizeof(line), f)) {
+      if (line[0] == '#' || line[0] == '\n') continue;
+      char dt[16];
+      TuneEntry e;
+      if (sscanf(line, "%15s %d %d %d %d %d", dt, &e.axis, &e.nmax, &e.method, &e.chunk,
+                 &e.spc) != 6) {
+        fclose(f);
+        return TRID_STATUS_INVALID_VALUE;
+      }
+      e.dtype_bytes = (strcmp(dt, "f64") == 0) ? 8 : (strcmp(dt, "f32") == 0 ? 4 : 0);
+      if (e.dtype_bytes == 0 || e.method < 1 || e.method > 2) {
+        fclose(f);
+        return TRID_STATUS_INVALID_VALUE;
+      }
+      table.push_back(e);
+    }
+    fclose(f);
+    std::stable_sort(table.begin(), table.end(),
+                     [](const TuneEntry &x, const TuneEntry &y) { return x.nmax < y.nmax; });
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune.swap(table);
+  return TRID_STATUS_SUCCESS;
+}
+
+extern "C" tridStatus_t tridQueryMethod(int dtype_bytes, int axis, int n, int *method, int *chunk,
+                                        int *sys_per_cta) {
+  if ((dtype_bytes != 4 && dtype_bytes != 8) || (axis != 0 && axis != 1) || n < 0 || !method ||
+      !chunk || !sys_per_cta)
+    return TRID_STATUS_INVALID_VALUE;
+  const MethodChoice m = choose_method(dtype_bytes, axis, n, 0);
+  *method = m.method;
+  *chunk = m.chunk;
+  *sys_per_cta = m.spc;
+  return TRID_STATUS_SUCCESS;
+}

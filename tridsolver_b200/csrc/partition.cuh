@@ -1,0 +1,142 @@
+// Partitioned Thomas ("hybrid Thomas-PCR") building blocks, sm_100a.
+//
+// A system of n rows is cut into 32 contiguous chunks of M rows (rows past n
+// are identity rows a=c=d=0, b=1).  Each thread owns one chunk in registers:
+//
+//  1. chunk_reduce: eliminate the chunk's interior rows j=1..M-2 with its first
+//     unknown F=x_0 kept as a parameter (downward sweep), then fold the
+//     interior back (upward recursion, FMAs only) into two interface rows
+//        F row:  fa*L_{t-1} + fb*F_t + fc*L_t     = fd
+//        L row:  la*F_t     + lb*L_t + lc*F_{t+1} = ld
+//     where L_t = x_{M-1} is the chunk's last unknown.  The interior keeps
+//     x_j = d'_j - a'_j*F_t - c'_j*x_{j+1}.
+//  2. warp_interface_solve: the 64 interface rows of the 32 chunks form a
+//     tridiagonal system [F_0, L_0, F_1, L_1, ...].  One step of odd-even
+//     elimination removes the F unknowns (one shuffle), parallel cyclic
+//     reduction (5 shuffle steps) solves the 32-row L system, and F_t follows
+//     from its own row.
+//  3. chunk_backsub: interior unknowns from F_t and L_t (FMAs only).
+//
+// This is the published partition / hybrid Thomas-PCR method; the reference
+// implements its own variant in scalar/src/cuda/trid_thomaspcr.hpp:198-318
+// (per-thread modified Thomas, trid_thomaspcr_small.h PCR).  Everything is
+// register-resident: no shared or global scratch.
+#pragma once
+
+#include "trid_internal.cuh"
+
+namespace tridb200 {
+
+template <typename T>
+struct Row {
+  T a, b, c, d;
+};
+
+// Interface rows of one chunk.  On return al/ga/de[j] (1 <= j <= M-2) hold
+// a'_j, c'_j, d'_j of  x_j + c'_j x_{j+1} = d'_j - a'_j x_0.
+template <typename T, int M>
+__device__ __forceinline__ void chunk_reduce(T (&al)[M], const T (&be)[M], T (&ga)[M],
+                                             T (&de)[M], Row<T> &F, Row<T> &L) {
+  static_assert(M >= 2, "chunks need at least two rows");
+  if constexpr (M == 2) {
+    F = {al[0], be[0], ga[0], de[0]};
+    L = {al[1], be[1], ga[1], de[1]};
+  } else {
+    // downward sweep, x_0 as parameter
+    T r = rcp(be[1]);
+    ga[1] *= r;
+    de[1] *= r;
+    al[1] *= r;
+#pragma unroll
+    for (int j = 2; j <= M - 2; ++j) {
+      r = rcp(be[j] - al[j] * ga[j - 1]);
+      de[j] = (de[j] - al[j] * de[j - 1]) * r;
+      al[j] = -(al[j] * al[j - 1]) * r;
+      ga[j] = ga[j] * r;
+    }
+    // x_{M-2} = D - A x_0 - C x_{M-1}  ->  L row
+    T D = de[M - 2], A = al[M - 2], C = ga[M - 2];
+    L.a = -al[M - 1] * A;
+    L.b = be[M - 1] - al[M - 1] * C;
+    L.c = ga[M - 1];
+    L.d = de[M - 1] - al[M - 1] * D;
+    // fold upward to x_1 = D - A x_0 - C x_{M-1}  ->  F row
+#pragma unroll
+    for (int j = M - 3; j >= 1; --j) {
+      D = de[j] - ga[j] * D;
+      A = al[j] - ga[j] * A;
+      C = -ga[j] * C;
+    }
+    F.a = al[0];
+    F.b = be[0] - ga[0] * A;
+    F.c = -ga[0] * C;
+    F.d = de[0] - ga[0] * D;
+  }
+}
+
+// Interior unknowns; the solution overwrites de[0..M-1].
+template <typename T, int M>
+__device__ __forceinline__ void chunk_backsub(const T (&al)[M], const T (&ga)[M], T (&de)[M],
+                                              T xF, T xL) {
+  if constexpr (M > 2) {
+    T x = xL;
+#pragma unroll
+    for (int j = M - 2; j >= 1; --j) {
+      x = de[j] - al[j] * xF - ga[j] * x;
+      de[j] = x;
+    }
+  }
+  de[0] = xF;
+  de[M - 1] = xL;
+}
+
+// Solve the 64-row interface system held two rows per lane (all 32 lanes of
+// the warp must call this).  Lane 0's F row must not couple to the left
+// (fa = 0) and lane 31's L row not to the right (lc = 0).
+template <typename T>
+__device__ __forceinline__ void warp_interface_solve(const Row<T> &F, const Row<T> &L, T &xF,
+                                                     T &xL, int lane) {
+  constexpr unsigned kFull = 0xffffffffu;
+  // F row of the next chunk
+  T nfa = __shfl_down_sync(kFull, F.a, 1);
+  T nfb = __shfl_down_sync(kFull, F.b, 1);
+  T nfc = __shfl_down_sync(kFull, F.c, 1);
+  T nfd = __shfl_down_sync(kFull, F.d, 1);
+  if (lane == kWarp - 1) {
+    nfa = T(0);
+    nfb = T(1);
+    nfc = T(0);
+    nfd = T(0);
+  }
+  // eliminate F_t and F_{t+1} from the L row -> tridiagonal in L only
+  const T p = L.a * rcp(F.b);
+  const T q = L.c * rcp(nfb);
+  T ra = -p * F.a;
+  T rb = L.b - p * F.c - q * nfa;
+  T rc = -q * nfc;
+  T rd = L.d - p * F.d - q * nfd;
+  // parallel cyclic reduction over the 32 lanes
+#pragma unroll
+  for (int s = 1; s < kWarp; s <<= 1) {
+    const T ib = rcp(rb);
+    const T ua = __shfl_up_sync(kFull, ra, s);
+    const T uc = __shfl_up_sync(kFull, rc, s);
+    const T ud = __shfl_up_sync(kFull, rd, s);
+    const T ui = __shfl_up_sync(kFull, ib, s);
+    const T da = __shfl_down_sync(kFull, ra, s);
+    const T dc = __shfl_down_sync(kFull, rc, s);
+    const T dd = __shfl_down_sync(kFull, rd, s);
+    const T di = __shfl_down_sync(kFull, ib, s);
+    const T k1 = (lane >= s) ? ra * ui : T(0);
+    const T k2 = (lane + s < kWarp) ? rc * di : T(0);
+    ra = -k1 * ua;
+    rc = -k2 * dc;
+    rb = rb - k1 * uc - k2 * da;
+    rd = rd - k1 * ud - k2 * dd;
+  }
+  xL = rd / rb;
+  const T lprev = __shfl_up_sync(kFull, xL, 1);
+  xF = (F.d - (lane > 0 ? F.a * lprev : T(0)) - F.c * xL) / F.b;
+}
+
+}  // namespace tridb200

@@ -1,0 +1,114 @@
+"""Scalar strided-batch solves: the reference's API names over the C ABI.
+
+Each ``trid?mtsvStridedBatch*`` function takes the reference's arguments
+(scalar/include/trid_cpu.h:53-82; Padded forms trid_cuda.h:61-84) with CUDA
+tensors (or integer device pointers) for the arrays and Python sequences for
+dims/pads, and returns the tridStatus_t the C ABI returned -- the same
+contract as the reference, whose callers check the status.  ``solve`` is the
+torch-facing convenience that raises ``TridError`` instead.
+"""
+
+import ctypes
+
+from ._lib import TridError, int_array, lib
+
+try:  # torch is only needed for tensor arguments and the current stream
+    import torch
+except ImportError:  # pragma: no cover
+    torch = None
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return ctypes.c_void_p(x)
+    if torch is not None and isinstance(x, torch.Tensor):
+        if not x.is_cuda:
+            raise ValueError("tridsolver_b200 works on CUDA tensors (device pointers)")
+        return ctypes.c_void_p(x.data_ptr())
+    raise TypeError(f"expected a CUDA tensor or a device pointer, got {type(x)}")
+
+
+def _bind_stream(L):
+    if torch is not None and torch.cuda.is_available() and torch.cuda.is_initialized():
+        L.tridSetStream(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+
+
+def _scalar9(name):
+    def f(a, b, c, d, u, ndim, solvedim, dims, pads):
+        L = lib()
+        _bind_stream(L)
+        return getattr(L, name)(_ptr(a), _ptr(b), _ptr(c), _ptr(d), _ptr(u), int(ndim),
+                                int(solvedim), int_array(dims), int_array(pads))
+    f.__name__ = name
+    f.__doc__ = f"{name}(a, b, c, d, u, ndim, solvedim, dims, pads) -> tridStatus_t"
+    return f
+
+
+def _padded(name):
+    def f(a, a_pads, b, b_pads, c, c_pads, d, d_pads, u, u_pads, ndim, solvedim, dims,
+          opts=None, sync=0):
+        L = lib()
+        _bind_stream(L)
+        return getattr(L, name)(_ptr(a), int_array(a_pads), _ptr(b), int_array(b_pads), _ptr(c),
+                                int_array(c_pads), _ptr(d), int_array(d_pads), _ptr(u),
+                                int_array(u_pads if u_pads is not None else d_pads), int(ndim),
+                                int(solvedim), int_array(dims),
+                                int_array(opts) if opts is not None else None, int(sync))
+    f.__name__ = name
+    return f
+
+
+tridSmtsvStridedBatch = _scalar9("tridSmtsvStridedBatch")
+tridDmtsvStridedBatch = _scalar9("tridDmtsvStridedBatch")
+tridSmtsvStridedBatchInc = _scalar9("tridSmtsvStridedBatchInc")
+tridDmtsvStridedBatchInc = _scalar9("tridDmtsvStridedBatchInc")
+tridSmtsvStridedBatchPadded = _padded("tridSmtsvStridedBatchPadded")
+tridDmtsvStridedBatchPadded = _padded("tridDmtsvStridedBatchPadded")
+tridSmtsvStridedBatchPaddedInc = _padded("tridSmtsvStridedBatchPaddedInc")
+tridDmtsvStridedBatchPaddedInc = _padded("tridDmtsvStridedBatchPaddedInc")
+
+
+def initTridMultiDimBatchSolve(ndim, dims, pads):
+    lib().initTridMultiDimBatchSolve(int(ndim), int_array(dims), int_array(pads))
+
+
+def set_method(method=0, chunk=0, sys_per_cta=0):
+    """Force the algorithm for calls from this thread (0 = automatic)."""
+    st = lib().tridSetMethod(int(method), int(chunk), int(sys_per_cta))
+    if st != 0:
+        raise TridError(st, "tridSetMethod")
+
+
+def solve(a, b, c, d, dim=-1, u=None, inc=False):
+    """Solve the tridiagonal systems along torch dimension ``dim``.
+
+    a, b, c, d (and u for ``inc``) are contiguous CUDA tensors of one shape
+    and dtype (float32 or float64).  Without ``inc`` the solution overwrites
+    ``d`` (returned); with ``inc`` it is added to ``u`` (returned) and ``d``
+    is left unchanged.  Torch's dimension k is the library's axis ndim-1-k
+    (the last torch dimension is the unit-stride axis 0).
+    """
+    shape = tuple(d.shape)
+    for t in (a, b, c, d) + ((u,) if inc else ()):
+        if tuple(t.shape) != shape or t.dtype != d.dtype or not t.is_contiguous():
+            raise ValueError("a, b, c, d (and u) must be contiguous tensors of one shape/dtype")
+    if inc and u is None:
+        raise ValueError("inc=True needs u")
+    ndim = len(shape)
+    if ndim == 0:
+        raise ValueError("need at least one dimension")
+    dim = dim % ndim
+    dims = list(reversed(shape))
+    solvedim = ndim - 1 - dim
+    if d.dtype == torch.float64:
+        fn = tridDmtsvStridedBatchInc if inc else tridDmtsvStridedBatch
+    elif d.dtype == torch.float32:
+        fn = tridSmtsvStridedBatchInc if inc else tridSmtsvStridedBatch
+    else:
+        raise TypeError("float32 or float64 only")
+    st = fn(a, b, c, d, u, ndim, solvedim, dims, dims)
+    if st != 0:
+        raise TridError(st, fn.__name__)
+    return u if inc else d
