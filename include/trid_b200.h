@@ -74,7 +74,7 @@ TRID_EXTERN_C tridStatus_t tridDmtsvStridedBatchInc(const double *a, const doubl
                                                     const double *c, double *d, double *u,
                                                     int ndim, int solvedim, int *dims, int *pads);
 
-/* ---- per-array pads: replace trid_cuda.h:61-67 / :79-85
+/* ---- per-array pads: replace trid_cuda.h:61-67 / :78-84
  *      (tridDmtsvStridedBatchPadded[Inc]); float forms are additions.
  *      opts is an optional algorithm hint (may be NULL); sync=1 waits for the
  *      solve to finish before returning. ---- */
@@ -112,11 +112,21 @@ TRID_EXTERN_C const char *tridGetStatusString(tridStatus_t status);
  *   method 0 = automatic (tuning table, then built-in heuristics)
  *   method 1 = Thomas, one thread per system, c'/d' in library scratch
  *   method 2 = partitioned Thomas: per-thread chunks of `chunk` rows reduced to
- *              a 64-row interface system solved by warp shuffles (PCR)
- *   chunk      : rows per thread for method 2 (2, 4, 8 or 16; 0 = automatic)
- *   sys_per_cta: systems per CTA for method 2 on strided axes (4, 8, 16; 0 = auto)
+ *              a 64-row interface system solved by warp shuffles (PCR); on
+ *              axis 0 the rows are staged by TMA when the layout allows
+ *   method 3 = method 2 with plain loads only
+ *   method 4 = strided axes: two-sided (twisted) Thomas, rows staged by TMA,
+ *              c'/d' in shared memory (falls back to method 2 where the
+ *              layout or length does not allow it; axis 0 uses method 2)
+ *   chunk      : rows per thread for methods 2/3 (2, 4, 8 or 16; 0 = automatic)
+ *   sys_per_cta: systems per CTA for methods 2/3 on strided axes (4, 8, 16; 0 = auto)
  * Applies to calls from the calling thread. */
 TRID_EXTERN_C tridStatus_t tridSetMethod(int method, int chunk, int sys_per_cta);
+
+/* Error bits recorded on the current device by kernels whose bounded waits
+ * gave up (1 = a TMA/mbarrier wait timed out); reading clears them.  Blocks
+ * until the device is idle. */
+TRID_EXTERN_C tridStatus_t tridGetDeviceErrors(unsigned *flags);
 
 /* Load an autotuning table written by tridsolver_b200.autotune (text lines
  * "<dtype> <axis> <nmax> <method> <chunk> <sys_per_cta>"); NULL clears it.

@@ -147,10 +147,42 @@ def test_8d(solvedim):
 
 
 @pytest.mark.parametrize("method", [(1, 0, 0), (2, 2, 4), (2, 4, 8), (2, 8, 16), (2, 16, 4),
-                                    (2, 16, 8)])
+                                    (2, 16, 8), (3, 8, 8), (4, 0, 0)])
 @pytest.mark.parametrize("solvedim", [0, 1, 2])
 def test_forced_methods(method, solvedim):
     run_case(np.random.default_rng(3), np.float64, [30, 29, 28], solvedim, method=method)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("dims,solvedim,pads", [
+    ([64, 256, 3], 1, None),          # TMA two-sided Thomas, full tiles
+    ([40, 33, 5], 1, [44, 33, 5]),    # partial x tile, odd n, padded
+    ([48, 6, 7], 2, None),            # n=7 < stage rows: falls back
+    ([32, 5, 300], 2, None),          # odd n, z
+    ([16, 1, 2], 2, None),            # n = 2
+    ([16, 4, 4, 9, 2], 3, None),      # rank 5
+])
+@pytest.mark.parametrize("inc", [False, True])
+def test_method4_twisted_thomas(dtype, dims, solvedim, pads, inc):
+    run_case(np.random.default_rng(sum(dims)), dtype, dims, solvedim, pads=pads, inc=inc,
+             method=(4, 0, 0))
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("n", [16, 48, 64, 200, 256, 512])
+@pytest.mark.parametrize("inc", [False, True])
+def test_x_tma_staged(dtype, n, inc):
+    """Axis 0 with pads[0] a multiple of the 128-byte row: TMA-staged loads,
+    and a TMA store when n fills whole rows."""
+    pads0 = ((n + 31) // 32) * 32
+    run_case(np.random.default_rng(n + inc), dtype, [n, 21, 3], 0, pads=[pads0, 21, 3], inc=inc)
+
+
+def test_no_device_errors_recorded():
+    import ctypes
+    flags = ctypes.c_uint(123)
+    assert tb.lib().tridGetDeviceErrors(ctypes.byref(flags)) == 0
+    assert flags.value == 0
 
 
 def test_padded_per_array_pads():

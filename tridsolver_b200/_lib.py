@@ -47,6 +47,7 @@ _COMMON = {
     "tridGetStream": (vp, []),
     "tridGetStatusString": (ctypes.c_char_p, [c_int]),
     "tridSetMethod": (c_int, [c_int, c_int, c_int]),
+    "tridGetDeviceErrors": (c_int, [ctypes.POINTER(ctypes.c_uint)]),
     "tridLoadTuningTable": (c_int, [ctypes.c_char_p]),
     "tridQueryMethod": (c_int, [c_int, c_int, c_int, ip, ip, ip]),
 }

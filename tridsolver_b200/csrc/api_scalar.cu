@@ -50,6 +50,25 @@ void *scratch(size_t bytes) {
   return p;
 }
 
+static std::mutex g_err_mu;
+static std::vector<unsigned *> g_err;  // indexed by device
+
+unsigned *device_error_flags() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  if ((int)g_err.size() <= dev) g_err.resize(dev + 1, nullptr);
+  if (!g_err[dev]) {
+    unsigned *p = nullptr;
+    if (cudaMalloc(&p, sizeof(unsigned)) != cudaSuccess || cudaMemset(p, 0, sizeof(unsigned)) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    g_err[dev] = p;
+  }
+  return g_err[dev];
+}
+
 struct TuneEntry {
   int dtype_bytes, axis, nmax, method, chunk, spc;
 };
@@ -83,7 +102,7 @@ MethodChoice choose_method(int dtype_bytes, int axis, int n, int opt_hint) {
     }
   }
   if (m.method == 0) m.method = chunk_for(n, dtype_bytes) ? 2 : 1;
-  if (m.method == 2) {
+  if (m.method >= 2) {
     const int need = chunk_for(n, dtype_bytes);
     if (need == 0) {
       m.method = 1;  // longer than any register-resident partition
@@ -120,6 +139,8 @@ tridStatus_t make_geom(int ndim, int solvedim, const int *dims, const int *const
     g.nsys *= dims[k];
     g.nod++;
   }
+  g.fastdiv = g.nsys < ((int64_t)1 << 32);
+  for (int k = 0; k < g.nod; ++k) fastdiv_setup((uint32_t)g.odims[k], g.dmul[k], g.dshift[k]);
   for (int q = 0; q < 5; ++q) {
     if (!pads[q] || (q == 4 && !inc)) continue;
     int64_t cum = 1;
@@ -157,12 +178,26 @@ tridStatus_t solve_strided_batch(const T *a, const T *b, const T *c, T *d, T *u,
   const cudaStream_t stream = current_stream();
   const int axis = (solvedim == 0) ? 0 : 1;
   const MethodChoice m = choose_method((int)sizeof(T), axis, g.n, opt);
-  cudaError_t e = cudaSuccess;
-  if (m.method == 2) {
-    if (axis == 0)
-      e = launch_xsolve<T, INC>(g, a, b, c, d, u, m.chunk, stream);
-    else
+  cudaError_t e = cudaErrorNotSupported;
+  if (m.method == 4 && axis == 1) {
+    unsigned *err = device_error_flags();
+    if (!err) return TRID_STATUS_ALLOC_FAILED;
+    e = launch_strided_tma<T, INC>(g, dims, pads, ndim, solvedim, a, b, c, d, u, err, stream);
+  }
+  if (e != cudaErrorNotSupported) {
+    // done (or failed) by the method-4 kernel
+  } else if (m.method == 2 || m.method == 3 || m.method == 4) {
+    if (axis == 0) {
+      e = cudaErrorNotSupported;
+      if (m.method == 2) {
+        unsigned *err = device_error_flags();
+        if (!err) return TRID_STATUS_ALLOC_FAILED;
+        e = launch_xsolve_tma<T, INC>(g, pads, ndim, a, b, c, d, u, m.chunk, err, stream);
+      }
+      if (e == cudaErrorNotSupported) e = launch_xsolve<T, INC>(g, a, b, c, d, u, m.chunk, stream);
+    } else {
       e = launch_strided<T, INC>(g, a, b, c, d, u, m.chunk, m.spc, stream);
+    }
   } else {
     // Thomas with c'/d' in scratch, in batches of systems bounded to ~1 GiB
     const size_t per_sys = (size_t)2 * g.n * sizeof(T);
@@ -270,12 +305,22 @@ extern "C" const char *tridGetStatusString(tridStatus_t s) {
 }
 
 extern "C" tridStatus_t tridSetMethod(int method, int chunk, int sys_per_cta) {
-  if (method < 0 || method > 2) return TRID_STATUS_INVALID_VALUE;
+  if (method < 0 || method > 4) return TRID_STATUS_INVALID_VALUE;
   if (chunk != 0 && chunk != 2 && chunk != 4 && chunk != 8 && chunk != 16)
     return TRID_STATUS_INVALID_VALUE;
   if (sys_per_cta != 0 && sys_per_cta != 4 && sys_per_cta != 8 && sys_per_cta != 16)
     return TRID_STATUS_INVALID_VALUE;
   tl_force = {method, chunk, sys_per_cta};
+  return TRID_STATUS_SUCCESS;
+}
+
+extern "C" tridStatus_t tridGetDeviceErrors(unsigned *flags) {
+  if (!flags) return TRID_STATUS_INVALID_VALUE;
+  unsigned *p = device_error_flags();
+  if (!p) return TRID_STATUS_ALLOC_FAILED;
+  if (cudaMemcpy(flags, p, sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemset(p, 0, sizeof(unsigned)) != cudaSuccess)
+    return TRID_STATUS_EXECUTION_FAILED;
   return TRID_STATUS_SUCCESS;
 }
 
@@ -295,7 +340,7 @@ extern "C" tridStatus_t tridLoadTuningTable(const char *path) {
         return TRID_STATUS_INVALID_VALUE;
       }
       e.dtype_bytes = (strcmp(dt, "f64") == 0) ? 8 : (strcmp(dt, "f32") == 0 ? 4 : 0);
-      if (e.dtype_bytes == 0 || e.method < 1 || e.method > 2) {
+      if (e.dtype_bytes == 0 || e.method < 1 || e.method > 4) {
         fclose(f);
         return TRID_STATUS_INVALID_VALUE;
       }

@@ -97,46 +97,47 @@ template <typename T>
 __device__ __forceinline__ void warp_interface_solve(const Row<T> &F, const Row<T> &L, T &xF,
                                                      T &xL, int lane) {
   constexpr unsigned kFull = 0xffffffffu;
-  // F row of the next chunk
+  const T ifb = rcp(F.b);
+  // F row of the next chunk (its pivot as a reciprocal)
   T nfa = __shfl_down_sync(kFull, F.a, 1);
-  T nfb = __shfl_down_sync(kFull, F.b, 1);
+  T nfi = __shfl_down_sync(kFull, ifb, 1);
   T nfc = __shfl_down_sync(kFull, F.c, 1);
   T nfd = __shfl_down_sync(kFull, F.d, 1);
   if (lane == kWarp - 1) {
     nfa = T(0);
-    nfb = T(1);
+    nfi = T(1);
     nfc = T(0);
     nfd = T(0);
   }
   // eliminate F_t and F_{t+1} from the L row -> tridiagonal in L only
-  const T p = L.a * rcp(F.b);
-  const T q = L.c * rcp(nfb);
+  const T p = L.a * ifb;
+  const T q = L.c * nfi;
   T ra = -p * F.a;
   T rb = L.b - p * F.c - q * nfa;
   T rc = -q * nfc;
   T rd = L.d - p * F.d - q * nfd;
-  // parallel cyclic reduction over the 32 lanes
+  // parallel cyclic reduction over the 32 lanes; each row sends its
+  // coefficients pre-divided by its pivot, so a neighbour needs 3 values
 #pragma unroll
   for (int s = 1; s < kWarp; s <<= 1) {
     const T ib = rcp(rb);
-    const T ua = __shfl_up_sync(kFull, ra, s);
-    const T uc = __shfl_up_sync(kFull, rc, s);
-    const T ud = __shfl_up_sync(kFull, rd, s);
-    const T ui = __shfl_up_sync(kFull, ib, s);
-    const T da = __shfl_down_sync(kFull, ra, s);
-    const T dc = __shfl_down_sync(kFull, rc, s);
-    const T dd = __shfl_down_sync(kFull, rd, s);
-    const T di = __shfl_down_sync(kFull, ib, s);
-    const T k1 = (lane >= s) ? ra * ui : T(0);
-    const T k2 = (lane + s < kWarp) ? rc * di : T(0);
+    const T sa = ra * ib, sc = rc * ib, sd = rd * ib;
+    const T ua = __shfl_up_sync(kFull, sa, s);
+    const T uc = __shfl_up_sync(kFull, sc, s);
+    const T ud = __shfl_up_sync(kFull, sd, s);
+    const T da = __shfl_down_sync(kFull, sa, s);
+    const T dc = __shfl_down_sync(kFull, sc, s);
+    const T dd = __shfl_down_sync(kFull, sd, s);
+    const T k1 = (lane >= s) ? ra : T(0);
+    const T k2 = (lane + s < kWarp) ? rc : T(0);
     ra = -k1 * ua;
     rc = -k2 * dc;
     rb = rb - k1 * uc - k2 * da;
     rd = rd - k1 * ud - k2 * dd;
   }
-  xL = rd / rb;
+  xL = rd * rcp(rb);
   const T lprev = __shfl_up_sync(kFull, xL, 1);
-  xF = (F.d - (lane > 0 ? F.a * lprev : T(0)) - F.c * xL) / F.b;
+  xF = (F.d - (lane > 0 ? F.a * lprev : T(0)) - F.c * xL) * ifb;
 }
 
 }  // namespace tridb200
