@@ -185,27 +185,29 @@ def run_ours(args):
     ta, tb_, tc, td = (torch.from_numpy(x).cuda() for x in (a, b, c, d0))
     stream = torch.cuda.current_stream()
 
-    def step(ev=None):
+    def step():
         for sd in range(3):
-            if ev is not None:
-                ev[sd][0].record(stream)
             st = tb.tridDmtsvStridedBatch(ta, tb_, tc, td, None, 3, sd, DIMS, DIMS)
             if st != 0:
                 raise tb.TridError(st, "tridDmtsvStridedBatch")
-            if ev is not None:
-                ev[sd][1].record(stream)
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    # per-launch timing of each axis on the launching stream
+    # per-launch timing of each axis on the launching stream: K launches of
+    # one axis back to back between two events (671 MB per launch > L2)
     per_axis = [0.0, 0.0, 0.0]
-    for _ in range(args.steps):
-        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(3)]
-        step(ev)
+    for sd in range(3):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            st = tb.tridDmtsvStridedBatch(ta, tb_, tc, td, None, 3, sd, DIMS, DIMS)
+            if st != 0:
+                raise tb.TridError(st, "tridDmtsvStridedBatch")
+        e1.record(stream)
         torch.cuda.synchronize()
-        for sd in range(3):
-            per_axis[sd] += ev[sd][0].elapsed_time(ev[sd][1]) / args.steps
+        per_axis[sd] = e0.elapsed_time(e1) / args.steps
     # whole-step timing (the reported value)
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)

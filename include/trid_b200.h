@@ -112,8 +112,9 @@ TRID_EXTERN_C const char *tridGetStatusString(tridStatus_t status);
  *   method 0 = automatic (tuning table, then built-in heuristics)
  *   method 1 = Thomas, one thread per system, c'/d' in library scratch
  *   method 2 = partitioned Thomas: per-thread chunks of `chunk` rows reduced to
- *              a 64-row interface system solved by warp shuffles (PCR); on
- *              axis 0 the rows are staged by TMA when the layout allows
+ *              a 64-row interface system solved by warp shuffles (PCR); the
+ *              rows are staged by TMA (bulk tensor copies) when the layout
+ *              allows
  *   method 3 = method 2 with plain loads only
  *   method 4 = strided axes: two-sided (twisted) Thomas, rows staged by TMA,
  *              c'/d' in shared memory (falls back to method 2 where the
@@ -124,17 +125,21 @@ TRID_EXTERN_C const char *tridGetStatusString(tridStatus_t status);
 TRID_EXTERN_C tridStatus_t tridSetMethod(int method, int chunk, int sys_per_cta);
 
 /* Error bits recorded on the current device by kernels whose bounded waits
- * gave up (1 = a TMA/mbarrier wait timed out); reading clears them.  Blocks
+ * gave up (1 = a TMA/mbarrier wait timed out; 2 = a bulk-copy shared-memory
+ * operand was misaligned and the copy was skipped); reading clears them.  Blocks
  * until the device is idle. */
 TRID_EXTERN_C tridStatus_t tridGetDeviceErrors(unsigned *flags);
 
 /* Load an autotuning table written by tridsolver_b200.autotune (text lines
- * "<dtype> <axis> <nmax> <method> <chunk> <sys_per_cta>"); NULL clears it.
- * Process-wide. */
+ * "<dtype> <axis class> <nmax> <method> <chunk> <sys_per_cta>", dtype f32 or
+ * f64, axis class as in tridQueryMethod); NULL clears it.  Process-wide.
+ * The first solve of a process also loads the file named by the environment
+ * variable TRID_B200_TUNING, when set. */
 TRID_EXTERN_C tridStatus_t tridLoadTuningTable(const char *path);
 
-/* The method/chunk/sys_per_cta the dispatcher would use for a problem
- * (dtype_bytes 4 or 8, axis 0 = contiguous solve, 1 = strided). */
+/* The method/chunk/sys_per_cta the dispatcher would use for a problem:
+ * dtype_bytes 4 or 8; axis class 0 = solve along axis 0 (unit stride),
+ * 1 = strided solve with a row stride of at most 64 KiB, 2 = larger stride. */
 TRID_EXTERN_C tridStatus_t tridQueryMethod(int dtype_bytes, int axis, int n, int *method,
                                            int *chunk, int *sys_per_cta);
 

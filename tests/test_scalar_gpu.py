@@ -178,6 +178,28 @@ def test_x_tma_staged(dtype, n, inc):
     run_case(np.random.default_rng(n + inc), dtype, [n, 21, 3], 0, pads=[pads0, 21, 3], inc=inc)
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("n", [2, 5, 33, 64, 100, 128, 255, 256, 300, 512])
+@pytest.mark.parametrize("solvedim", [1, 2])
+def test_strided_tma_staged(dtype, n, solvedim):
+    """Strided axes with pads[0]*sizeof a multiple of 16: TMA-staged tiles."""
+    dims = [40, n, 3] if solvedim == 1 else [40, 3, n]
+    run_case(np.random.default_rng(n + 7 * solvedim), dtype, dims, solvedim)
+
+
+@pytest.mark.parametrize("spc", [4, 8, 16])
+@pytest.mark.parametrize("inc", [False, True])
+@pytest.mark.parametrize("dims,solvedim,pads", [
+    ([36, 70, 6], 1, [36, 72, 6]),
+    ([36, 6, 70], 2, [40, 6, 70]),
+    ([20, 3, 50, 4], 2, [24, 3, 50, 4]),
+    ([16, 2, 3, 41, 2], 3, None),
+])
+def test_strided_tma_spc_inc_padded(spc, inc, dims, solvedim, pads):
+    run_case(np.random.default_rng(spc + inc), np.float64, dims, solvedim, pads=pads, inc=inc,
+             method=(2, 0, spc))
+
+
 def test_no_device_errors_recorded():
     import ctypes
     flags = ctypes.c_uint(123)

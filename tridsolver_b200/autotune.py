@@ -1,0 +1,154 @@
+"""Autotuner for the scalar strided-batch solves.
+
+Sweeps, on the current GPU, every algorithm the dispatcher offers for each
+(dtype, axis class, system length) bucket and writes the winners as a tuning
+table that the C ABI reads (``tridLoadTuningTable`` or the environment
+variable ``TRID_B200_TUNING``).
+
+    python -m tridsolver_b200.autotune --out tuning_b200.txt [--dtypes f64,f32]
+                                       [--lengths 32,64,128,256,512] [--elems 16777216]
+
+Candidates (see tridSetMethod in include/trid_b200.h):
+    method 1            Thomas, one thread per system, c'/d' in scratch
+    method 2/3, chunk   partitioned Thomas with warp PCR (2 = TMA staging on
+                        axis 0 when possible, 3 = plain loads), with every
+                        rows-per-thread chunk that covers n and, on strided
+                        axes, 4/8/16 systems per CTA
+    method 4            strided axes: two-sided Thomas with a TMA stage ring
+
+Axis classes: 0 = solve along axis 0 (unit stride); 1 = strided, row stride
+<= 64 KiB; 2 = larger strides.  The timing problem of each bucket holds about
+``--elems`` unknowns (16.7 M by default, > L2 for FP64 and FP32) shaped as
+[n, S] (class 0), [256, n, S] (class 1) or [256, S, n] (class 2).
+"""
+
+import argparse
+import ctypes
+import json
+import sys
+
+import numpy as np
+
+from ._lib import TridError, lib
+
+CHUNKS = (2, 4, 8, 16)
+
+
+def need_chunk(n):
+    for ch in CHUNKS:
+        if n <= 32 * ch:
+            return ch
+    return 0
+
+
+def candidates(axis, n):
+    out = [(1, 0, 0)]
+    ch0 = need_chunk(n)
+    if ch0:
+        for ch in CHUNKS:
+            if ch < ch0:
+                continue
+            if axis == 0:
+                out.append((2, ch, 0))
+                out.append((3, ch, 0))
+            else:
+                for spc in (4, 8, 16):
+                    out.append((2, ch, spc))
+    if axis > 0:
+        out.append((4, 0, 0))
+    return out
+
+
+def problem_dims(axis, n, elems):
+    if axis == 0:
+        return [n, max(1, elems // n)], 0
+    rest = max(1, elems // (256 * n))
+    if axis == 1:
+        return [256, n, rest], 1
+    return [256, rest, n], 2
+
+
+def time_candidate(torch, dtype, dims, solvedim, method, reps=10):
+    L = lib()
+    size = int(np.prod(dims))
+    g = torch.Generator(device="cuda").manual_seed(7)
+    a = torch.rand(size, device="cuda", dtype=dtype, generator=g) * 2 - 1
+    c = torch.rand(size, device="cuda", dtype=dtype, generator=g) * 2 - 1
+    b = a.abs() + c.abs() + 1 + torch.rand(size, device="cuda", dtype=dtype, generator=g)
+    d = torch.randn(size, device="cuda", dtype=dtype, generator=g)
+    fn = L.tridDmtsvStridedBatch if dtype == torch.float64 else L.tridSmtsvStridedBatch
+    dims_c = (ctypes.c_int * len(dims))(*dims)
+    st = L.tridSetMethod(*method)
+    if st != 0:
+        raise TridError(st, "tridSetMethod")
+    L.tridSetStream(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    args = [ctypes.c_void_p(t.data_ptr()) for t in (a, b, c, d)] + [None, len(dims), solvedim,
+                                                                     dims_c, dims_c]
+    try:
+        for _ in range(3):
+            st = fn(*args)
+            if st != 0:
+                raise TridError(st, "solve")
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn(*args)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+    finally:
+        L.tridSetMethod(0, 0, 0)
+
+
+def tune(dtypes=("f64", "f32"), lengths=(32, 64, 128, 256, 512), elems=1 << 24, verbose=True):
+    import torch
+
+    table, report = [], []
+    for dt in dtypes:
+        tdtype = torch.float64 if dt == "f64" else torch.float32
+        for axis in (0, 1, 2):
+            for n in lengths:
+                dims, sd = problem_dims(axis, n, elems)
+                best = None
+                for m in candidates(axis, n):
+                    ms = time_candidate(torch, tdtype, dims, sd, m)
+                    gbs = 5 * tdtype.itemsize * int(np.prod(dims)) / (ms * 1e-3) / 1e9
+                    report.append({"dtype": dt, "axis": axis, "n": n, "method": m, "ms": ms,
+                                   "GBs": round(gbs, 1)})
+                    if verbose:
+                        print(f"{dt} axis{axis} n={n:5d} method={m}: {ms:.4f} ms {gbs:8.1f} GB/s",
+                              file=sys.stderr)
+                    if best is None or ms < best[0]:
+                        best = (ms, m)
+                table.append((dt, axis, n, best[1]))
+    return table, report
+
+
+def write_table(table, path):
+    with open(path, "w") as f:
+        f.write("# dtype axis_class nmax method chunk sys_per_cta (tridsolver_b200.autotune)\n")
+        for dt, axis, n, (m, ch, spc) in table:
+            f.write(f"{dt} {axis} {n} {m} {ch} {spc}\n")
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--out", default="tuning_b200.txt")
+    ap.add_argument("--dtypes", default="f64,f32")
+    ap.add_argument("--lengths", default="32,64,128,256,512")
+    ap.add_argument("--elems", type=int, default=1 << 24)
+    ap.add_argument("--report", default=None, help="also write every timing as JSON")
+    args = ap.parse_args()
+    table, report = tune(args.dtypes.split(","), [int(v) for v in args.lengths.split(",")],
+                         args.elems)
+    write_table(table, args.out)
+    if args.report:
+        with open(args.report, "w") as f:
+            json.dump(report, f, indent=1)
+    print(open(args.out).read())
+
+
+if __name__ == "__main__":
+    main()

@@ -75,6 +75,43 @@ struct TuneEntry {
 static std::mutex g_tune_mu;
 static std::vector<TuneEntry> g_tune;
 
+static tridStatus_t parse_tuning_table(const char *path, std::vector<TuneEntry> &table) {
+  FILE *f = fopen(path, "r");
+  if (!f) return TRID_STATUS_INVALID_VALUE;
+  char line[256];
+  while (fgets(line, sizeof(line), f)) {
+    if (line[0] == '#' || line[0] == '\n') continue;
+    char dt[16];
+    TuneEntry e;
+    if (sscanf(line, "%15s %d %d %d %d %d", dt, &e.axis, &e.nmax, &e.method, &e.chunk, &e.spc) !=
+        6) {
+      fclose(f);
+      return TRID_STATUS_INVALID_VALUE;
+    }
+    e.dtype_bytes = (strcmp(dt, "f64") == 0) ? 8 : (strcmp(dt, "f32") == 0 ? 4 : 0);
+    if (e.dtype_bytes == 0 || e.method < 1 || e.method > 4 || e.axis < 0 || e.axis > 2) {
+      fclose(f);
+      return TRID_STATUS_INVALID_VALUE;
+    }
+    table.push_back(e);
+  }
+  fclose(f);
+  std::stable_sort(table.begin(), table.end(),
+                   [](const TuneEntry &x, const TuneEntry &y) { return x.nmax < y.nmax; });
+  return TRID_STATUS_SUCCESS;
+}
+
+static std::once_flag g_env_tune_once;
+static void load_env_tuning() {
+  const char *p = getenv("TRID_B200_TUNING");
+  if (!p || !*p) return;
+  std::vector<TuneEntry> table;
+  if (parse_tuning_table(p, table) == TRID_STATUS_SUCCESS) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.swap(table);
+  }
+}
+
 // ------------------------------------------------------- method selection --
 static int chunk_for(int n, int dtype_bytes) {
   (void)dtype_bytes;
@@ -86,6 +123,7 @@ static int chunk_for(int n, int dtype_bytes) {
 }
 
 MethodChoice choose_method(int dtype_bytes, int axis, int n, int opt_hint) {
+  std::call_once(g_env_tune_once, load_env_tuning);
   MethodChoice m = tl_force;
   if (m.method == 0 && opt_hint != 0) {
     // reference opts: 1/2 = plain Thomas kernels, 3/4 = Thomas-PCR hybrid
@@ -176,10 +214,13 @@ tridStatus_t solve_strided_batch(const T *a, const T *b, const T *c, T *d, T *u,
   if (g.n == 0 || g.nsys == 0) return TRID_STATUS_SUCCESS;
 
   const cudaStream_t stream = current_stream();
-  const int axis = (solvedim == 0) ? 0 : 1;
+  // axis class: 0 = unit stride inside a system, 1 = strided with a row
+  // stride of at most 64 KiB, 2 = larger strides (e.g. the outermost axis of a
+  // big cube, where DRAM-page and TLB locality differ)
+  const int axis = (solvedim == 0) ? 0 : (g.stride[kD] * (int64_t)sizeof(T) <= 65536 ? 1 : 2);
   const MethodChoice m = choose_method((int)sizeof(T), axis, g.n, opt);
   cudaError_t e = cudaErrorNotSupported;
-  if (m.method == 4 && axis == 1) {
+  if (m.method == 4 && axis >= 1) {
     unsigned *err = device_error_flags();
     if (!err) return TRID_STATUS_ALLOC_FAILED;
     e = launch_strided_tma<T, INC>(g, dims, pads, ndim, solvedim, a, b, c, d, u, err, stream);
@@ -196,7 +237,15 @@ tridStatus_t solve_strided_batch(const T *a, const T *b, const T *c, T *d, T *u,
       }
       if (e == cudaErrorNotSupported) e = launch_xsolve<T, INC>(g, a, b, c, d, u, m.chunk, stream);
     } else {
-      e = launch_strided<T, INC>(g, a, b, c, d, u, m.chunk, m.spc, stream);
+      e = cudaErrorNotSupported;
+      if (m.method == 2) {
+        unsigned *err = device_error_flags();
+        if (!err) return TRID_STATUS_ALLOC_FAILED;
+        e = launch_strided_part_tma<T, INC>(g, dims, pads, ndim, solvedim, a, b, c, d, u, m.chunk,
+                                            m.spc, err, stream);
+      }
+      if (e == cudaErrorNotSupported)
+        e = launch_strided<T, INC>(g, a, b, c, d, u, m.chunk, m.spc, stream);
     }
   } else {
     // Thomas with c'/d' in scratch, in batches of systems bounded to ~1 GiB
@@ -325,30 +374,11 @@ extern "C" tridStatus_t tridGetDeviceErrors(unsigned *flags) {
 }
 
 extern "C" tridStatus_t tridLoadTuningTable(const char *path) {
+  std::call_once(g_env_tune_once, load_env_tuning);  // an explicit table wins
   std::vector<TuneEntry> table;
   if (path) {
-    FILE *f = fopen(path, "r");
-    if (!f) return TRID_STATUS_INVALID_VALUE;
-    char line[256];
-    while (fgets(line, sizeof(line), f)) {
-      if (line[0] == '#' || line[0] == '\n') continue;
-      char dt[16];
-      TuneEntry e;
-      if (sscanf(line, "%15s %d %d %d %d %d", dt, &e.axis, &e.nmax, &e.method, &e.chunk,
-                 &e.spc) != 6) {
-        fclose(f);
-        return TRID_STATUS_INVALID_VALUE;
-      }
-      e.dtype_bytes = (strcmp(dt, "f64") == 0) ? 8 : (strcmp(dt, "f32") == 0 ? 4 : 0);
-      if (e.dtype_bytes == 0 || e.method < 1 || e.method > 4) {
-        fclose(f);
-        return TRID_STATUS_INVALID_VALUE;
-      }
-      table.push_back(e);
-    }
-    fclose(f);
-    std::stable_sort(table.begin(), table.end(),
-                     [](const TuneEntry &x, const TuneEntry &y) { return x.nmax < y.nmax; });
+    const tridStatus_t st = parse_tuning_table(path, table);
+    if (st != TRID_STATUS_SUCCESS) return st;
   }
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune.swap(table);
@@ -357,7 +387,7 @@ extern "C" tridStatus_t tridLoadTuningTable(const char *path) {
 
 extern "C" tridStatus_t tridQueryMethod(int dtype_bytes, int axis, int n, int *method, int *chunk,
                                         int *sys_per_cta) {
-  if ((dtype_bytes != 4 && dtype_bytes != 8) || (axis != 0 && axis != 1) || n < 0 || !method ||
+  if ((dtype_bytes != 4 && dtype_bytes != 8) || axis < 0 || axis > 2 || n < 0 || !method ||
       !chunk || !sys_per_cta)
     return TRID_STATUS_INVALID_VALUE;
   const MethodChoice m = choose_method(dtype_bytes, axis, n, 0);

@@ -1,0 +1,252 @@
+// Strided-axis partitioned Thomas with TMA-staged tiles (sm_100a).
+//
+// Same algorithm and thread mapping as strided_kernel (kern_scalar.cu): a CTA
+// owns SB adjacent systems, thread (system sl, chunk t) reduces rows
+// [t*M, t*M+M) of system sl, SB warps solve the interface systems (lane =
+// chunk), every thread back-substitutes its chunk.  The difference is data
+// movement: the CTA's whole tile (SB systems x n rows of a, b, c, d and, for
+// Inc, u) arrives by bulk tensor copies into shared memory (one or two boxes
+// per array, completion on one mbarrier) and the solution leaves by bulk
+// tensor stores, so every byte of the tile is in flight at once without
+// occupying registers, and the loads of one CTA overlap the arithmetic of
+// the others on the SM.  The tensor maps use the logical extents, so rows
+// past n and systems past dims[0] are never written.
+//
+// Preconditions (launch_strided_part_tma returns cudaErrorNotSupported
+// otherwise): solvedim >= 1, ndim <= 5, 16-byte aligned base pointers,
+// pads[0]*sizeof(T) a multiple of 16 for every array, dims[0] >= SB,
+// n <= 32*M and the tile fitting in shared memory.
+#include "partition.cuh"
+#include "tma.cuh"
+
+namespace tridb200 {
+
+template <typename T, int M, int SB, int INC>
+__global__ void __launch_bounds__(SB * kWarp) strided_part_tma_kernel(
+    const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mb,
+    const __grid_constant__ CUtensorMap mc, const __grid_constant__ CUtensorMap md,
+    const __grid_constant__ CUtensorMap mu, Geom g, int solvedim, int box_rows, int nbox,
+    int red_off, unsigned *err) {
+  constexpr int NA = INC ? 5 : 4;
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ uint64_t bar;
+  const int rows_cap = box_rows * nbox;                       // tile rows in smem
+  // [NA][tsz]: each array tile starts on a 128-byte boundary
+  T *tile = reinterpret_cast<T *>(smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127));
+  constexpr int kAlignElems = 128 / (int)sizeof(T);
+  const size_t tsz = (((size_t)rows_cap * SB + kAlignElems - 1) / kAlignElems) * kAlignElems;
+  // interface rows / solutions alias the a, b, c tiles once they are consumed
+  // (red_off = 0), or follow the tiles when those are too small
+  T *red = tile + red_off;                                    // [8][32][SB+1]
+  T *sol = red + 8 * kWarp * (SB + 1);                        // [2][32][SB+1]
+
+  const int tid = threadIdx.x;
+  const int sl = tid % SB;
+  const int t = tid / SB;
+  const int n = g.n;
+
+  // tile -> coordinates (x0 on axis 0, the other non-solve axes)
+  const int ntx = (g.odims[0] + SB - 1) / SB;
+  int coord[5] = {(int)(blockIdx.x % ntx) * SB, 0, 0, 0, 0};
+  {
+    uint32_t rest = blockIdx.x / ntx;
+    int o = 1;
+    for (int k = 1; k < 5; ++k) {
+      if (k == solvedim || o >= g.nod) continue;
+      const uint32_t e = (uint32_t)g.odims[o++];
+      coord[k] = (int)(rest % e);
+      rest /= e;
+    }
+  }
+  const CUtensorMap *maps[5] = {&ma, &mb, &mc, &md, &mu};
+  // every copy destination (tile starts, second boxes) must be 128-byte aligned
+  if (!tma_smem_aligned(tile) || (nbox > 1 && ((size_t)box_rows * SB * sizeof(T)) % 128 != 0)) {
+    if (tid == 0) atomicOr(err, kErrMisaligned);
+    return;
+  }
+
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    mbar_arrive_expect_tx(&bar, (uint32_t)(NA * nbox * box_rows * SB * sizeof(T)));
+    for (int q = 0; q < NA; ++q)
+      for (int bx = 0; bx < nbox; ++bx) {
+        int c[5] = {coord[0], coord[1], coord[2], coord[3], coord[4]};
+        c[solvedim] = bx * box_rows;
+        tma_load_5d(tile + q * tsz + (size_t)bx * box_rows * SB, maps[q], &bar, c[0], c[1], c[2],
+                    c[3], c[4]);
+      }
+  }
+  if (!mbar_wait(&bar, 0, err)) {
+    mbar_wait(&bar, 0, nullptr);
+    return;
+  }
+
+  const int r0 = t * M;
+  const bool valid = coord[0] + sl < g.odims[0];
+  T al[M], be[M], ga[M], de[M];
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int r = r0 + j;
+    if (valid && r < n) {
+      const size_t o = (size_t)r * SB + sl;
+      al[j] = (r == 0) ? T(0) : tile[0 * tsz + o];
+      be[j] = tile[1 * tsz + o];
+      ga[j] = (r == n - 1) ? T(0) : tile[2 * tsz + o];
+      de[j] = tile[3 * tsz + o];
+    } else {
+      al[j] = T(0);
+      be[j] = T(1);
+      ga[j] = T(0);
+      de[j] = T(0);
+    }
+  }
+  Row<T> F, L;
+  chunk_reduce<T, M>(al, be, ga, de, F, L);
+  __syncthreads();  // every thread holds its rows: the a/b/c tiles become scratch
+  auto R = [&](int comp, int chunk, int s) -> T & {
+    return red[((size_t)comp * kWarp + chunk) * (SB + 1) + s];
+  };
+  R(0, t, sl) = F.a;
+  R(1, t, sl) = F.b;
+  R(2, t, sl) = F.c;
+  R(3, t, sl) = F.d;
+  R(4, t, sl) = L.a;
+  R(5, t, sl) = L.b;
+  R(6, t, sl) = L.c;
+  R(7, t, sl) = L.d;
+  __syncthreads();
+  {
+    const int w = tid / kWarp;
+    const int lane = tid & (kWarp - 1);
+    const Row<T> F2{R(0, lane, w), R(1, lane, w), R(2, lane, w), R(3, lane, w)};
+    const Row<T> L2{R(4, lane, w), R(5, lane, w), R(6, lane, w), R(7, lane, w)};
+    T xF, xL;
+    warp_interface_solve(F2, L2, xF, xL, lane);
+    sol[(0 * kWarp + lane) * (SB + 1) + w] = xF;
+    sol[(1 * kWarp + lane) * (SB + 1) + w] = xL;
+  }
+  __syncthreads();
+  chunk_backsub<T, M>(al, ga, de, sol[(0 * kWarp + t) * (SB + 1) + sl],
+                      sol[(1 * kWarp + t) * (SB + 1) + sl]);
+
+  // solution into the d (or u) tile, then bulk tensor stores
+  T *out = tile + (INC ? 4 : 3) * tsz;
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int r = r0 + j;
+    if (r < rows_cap) {
+      const size_t o = (size_t)r * SB + sl;
+      if (INC)
+        out[o] += de[j];
+      else
+        out[o] = de[j];
+    }
+  }
+  fence_proxy_async();
+  __syncthreads();
+  if (tid == 0) {
+    for (int bx = 0; bx < nbox; ++bx) {
+      int c[5] = {coord[0], coord[1], coord[2], coord[3], coord[4]};
+      c[solvedim] = bx * box_rows;
+      const T *src = out + (size_t)bx * box_rows * SB;
+      asm volatile(
+          "cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4, %5, %6}],"
+          " [%1];" ::"l"(maps[INC ? 4 : 3]),
+          "r"(smem_u32(src)), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4])
+          : "memory");
+    }
+    tma_store_commit();
+    tma_store_wait_read();
+  }
+}
+
+template <typename T, int M, int SB, int INC>
+static cudaError_t launch_sptma(const CUtensorMap *maps, const Geom &g, int solvedim,
+                                int box_rows, int nbox, int64_t blocks, unsigned *err,
+                                cudaStream_t st, int optin) {
+  constexpr int NA = INC ? 5 : 4;
+  constexpr int kAlignElems = 128 / (int)sizeof(T);
+  const size_t tsz = (((size_t)box_rows * nbox * SB + kAlignElems - 1) / kAlignElems) * kAlignElems;
+  const size_t tile = (size_t)NA * tsz * sizeof(T);
+  const size_t scratch = (size_t)10 * kWarp * (SB + 1) * sizeof(T);   // red + sol
+  const bool alias = scratch <= (size_t)3 * tsz * sizeof(T);
+  const int red_off = alias ? 0 : (int)(NA * tsz);
+  const size_t smem = (alias ? tile : tile + scratch) + 128;          // + base alignment
+  if (smem + 64 > (size_t)optin) return cudaErrorNotSupported;
+  auto kern = strided_part_tma_kernel<T, M, SB, INC>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<dim3((unsigned)blocks), dim3(SB * kWarp), smem, st>>>(
+      maps[0], maps[1], maps[2], maps[3], maps[4], g, solvedim, box_rows, nbox, red_off, err);
+  return cudaGetLastError();
+}
+
+template <typename T, int M, int INC>
+static cudaError_t launch_sptma_sb(const CUtensorMap *maps, const Geom &g, int solvedim,
+                                   int box_rows, int nbox, int spc, int64_t ntiles_rest,
+                                   unsigned *err, cudaStream_t st, int optin) {
+  const int64_t blocks = ((g.odims[0] + spc - 1) / spc) * ntiles_rest;
+  if (blocks > 0x7fffffff || blocks == 0) return cudaErrorNotSupported;
+  switch (spc) {
+    case 4: return launch_sptma<T, M, 4, INC>(maps, g, solvedim, box_rows, nbox, blocks, err, st, optin);
+    case 8: return launch_sptma<T, M, 8, INC>(maps, g, solvedim, box_rows, nbox, blocks, err, st, optin);
+    case 16: return launch_sptma<T, M, 16, INC>(maps, g, solvedim, box_rows, nbox, blocks, err, st, optin);
+    default: return cudaErrorNotSupported;
+  }
+}
+
+template <typename T, int INC>
+cudaError_t launch_strided_part_tma(const Geom &g, const int *dims, const int *const pads[5],
+                                    int ndim, int solvedim, const T *a, const T *b, const T *c,
+                                    T *d, T *u, int chunk, int spc, unsigned *err,
+                                    cudaStream_t st) {
+  if (solvedim < 1 || ndim > 5 || g.n > 32 * chunk || dims[0] < spc) return cudaErrorNotSupported;
+  const int box_rows = g.n < 256 ? g.n : 256;
+  const int nbox = (g.n + box_rows - 1) / box_rows;
+  const int na = INC ? 5 : 4;
+  const void *ptrs[5] = {a, b, c, d, u};
+  CUtensorMap maps[5];
+  for (int q = 0; q < 5; ++q) {
+    const int qq = q < na ? q : 3;
+    if (((uintptr_t)ptrs[qq] & 15) != 0 || (pads[qq][0] * sizeof(T)) % 16 != 0)
+      return cudaErrorNotSupported;
+    uint64_t gd[5] = {1, 1, 1, 1, 1}, gs[4];
+    uint32_t box[5] = {1, 1, 1, 1, 1};
+    uint64_t cum = sizeof(T);
+    for (int k = 0; k < 5; ++k) {
+      if (k < ndim) gd[k] = (uint64_t)dims[k];
+      if (k > 0) gs[k - 1] = cum;
+      cum *= (k < ndim) ? (uint64_t)pads[qq][k] : 1;
+    }
+    box[0] = (uint32_t)spc;
+    box[solvedim] = (uint32_t)box_rows;
+    if (!encode_tensor_map(&maps[q], ptrs[qq], (int)sizeof(T), 5, gd, gs, box, false))
+      return cudaErrorNotSupported;
+  }
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const int64_t rest = g.nsys / dims[0];
+  switch (chunk) {
+    case 2: return launch_sptma_sb<T, 2, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin);
+    case 4: return launch_sptma_sb<T, 4, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin);
+    case 8: return launch_sptma_sb<T, 8, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin);
+    case 16: return launch_sptma_sb<T, 16, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin);
+    default: return cudaErrorNotSupported;
+  }
+}
+
+#define TRID_SPTMA_INSTANTIATE(T, INC)                                                         \
+  template cudaError_t launch_strided_part_tma<T, INC>(                                        \
+      const Geom &, const int *, const int *const[5], int, int, const T *, const T *, const T *, \
+      T *, T *, int, int, unsigned *, cudaStream_t);
+TRID_SPTMA_INSTANTIATE(float, 0)
+TRID_SPTMA_INSTANTIATE(float, 1)
+TRID_SPTMA_INSTANTIATE(double, 0)
+TRID_SPTMA_INSTANTIATE(double, 1)
+
+}  // namespace tridb200

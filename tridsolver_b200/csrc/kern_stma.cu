@@ -37,9 +37,10 @@ __global__ void __launch_bounds__(kWarp) strided_tma_kernel(
     int solvedim, T *__restrict__ d, T *__restrict__ u, unsigned *err) {
   constexpr int kBox = kSRows * kSW;            // elements per box
   constexpr int kStage = 4 * 2 * kBox;          // elements per stage (4 arrays, 2 boxes)
-  extern __shared__ __align__(128) unsigned char smem_raw[];
+  extern __shared__ unsigned char smem_raw[];
   __shared__ uint64_t full[kSStages];
-  T *ring = reinterpret_cast<T *>(smem_raw);
+  // stage boxes are 1 KB (FP64) / 512 B (FP32) apart: align the ring to 128 B
+  T *ring = reinterpret_cast<T *>(smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127));
   T *cq = ring + kSStages * kStage;             // c' (top rows) / a'' (bottom rows)
   T *cd = cq + (size_t)g.n * kSW;               // d' / d''
 
@@ -91,6 +92,11 @@ __global__ void __launch_bounds__(kWarp) strided_tma_kernel(
     }
   };
 
+  static_assert((kSRows * kSW * 4) % 128 == 0, "stage boxes must stay 128-byte aligned");
+  if (!tma_smem_aligned(ring)) {
+    if (lane == 0) atomicOr(err, kErrMisaligned);
+    return;
+  }
   if (lane == 0) {
     for (int s = 0; s < kSStages; ++s) mbar_init(&full[s], 1);
     fence_barrier_init();
@@ -187,7 +193,7 @@ cudaError_t launch_strided_tma(const Geom &g, const int *dims, const int *const 
   if (solvedim < 1 || ndim > 5 || g.n < kSRows || dims[0] < kSW) return cudaErrorNotSupported;
   const size_t ring = (size_t)kSStages * 4 * 2 * kSRows * kSW * sizeof(T);
   const size_t store = (size_t)2 * g.n * kSW * sizeof(T);
-  const size_t smem = ring + store;
+  const size_t smem = ring + store + 128;  // + base alignment
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);

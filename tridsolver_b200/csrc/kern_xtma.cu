@@ -94,6 +94,10 @@ __global__ void __launch_bounds__(kXWarps * kWarp) xsolve_tma_kernel(
   const int lane = threadIdx.x & (kWarp - 1);
   const int64_t sys = (int64_t)blockIdx.x * kXWarps + w;
   if (sys >= g.nsys) return;  // whole warp
+  if (!tma_smem_aligned(smem)) {
+    if (lane == 0) atomicOr(err, kErrMisaligned);
+    return;
+  }
   int64_t off[5];
   system_offsets(g, sys, off);
   unsigned char *tile = smem + (size_t)w * NA * Tile::kBytes;

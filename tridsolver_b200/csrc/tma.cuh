@@ -56,6 +56,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 // in *err and returns false.  Every wait in this library goes through here.
 constexpr uint32_t kMaxPolls = 1u << 22;
 constexpr unsigned kErrWaitTimeout = 1u;
+constexpr unsigned kErrMisaligned = 2u;  // a TMA shared-memory operand was not 128-byte aligned
+
+// Bulk tensor copies need 128-byte aligned shared-memory operands; kernels
+// check every destination with this before issuing and record kErrMisaligned
+// instead of issuing a bad copy.
+__device__ __forceinline__ bool tma_smem_aligned(const void *p) { return (smem_u32(p) & 127u) == 0; }
 
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned *err) {
   for (uint32_t i = 0; i < kMaxPolls; ++i)

@@ -136,6 +136,11 @@ cudaError_t launch_strided_tma(const Geom &g, const int *dims, const int *const 
                                int ndim, int solvedim, const T *a, const T *b, const T *c, T *d,
                                T *u, unsigned *err, cudaStream_t st);
 template <typename T, int INC>
+cudaError_t launch_strided_part_tma(const Geom &g, const int *dims, const int *const pads[5],
+                                    int ndim, int solvedim, const T *a, const T *b, const T *c,
+                                    T *d, T *u, int chunk, int spc, unsigned *err,
+                                    cudaStream_t st);
+template <typename T, int INC>
 cudaError_t launch_generic(const Geom &g, const T *a, const T *b, const T *c, T *d, T *u,
                            T *work, int64_t work_systems, cudaStream_t st);
 
