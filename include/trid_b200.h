@@ -95,6 +95,28 @@ TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchPaddedInc(
     const int *c_pads, float *d, const int *d_pads, float *u, const int *u_pads, int ndim,
     int solvedim, int *dims, int *opts, int sync);
 
+/* ---- adjoint (no reference counterpart) ----------------------------------
+ * Reverse-mode derivative of tridXmtsvStridedBatch.  For x = A^{-1} d (the
+ * systems of the forward call) and a cotangent w = dL/dx, computes
+ *   g = A^{-T} w,  dd = g,  da_i = -g_i x_{i-1},  db_i = -g_i x_i,
+ *   dc_i = -g_i x_{i+1}   (da_0 = dc_{n-1} = 0: those entries are unused).
+ * u is the forward solution x.  Every array has the layout of dims/pads (one
+ * pads array for all).  Outputs are overwritten; any of da, db, dc, dd may be
+ * NULL.  Outputs must not alias a, b, c or u (dd may alias w).  Device
+ * pointers, enqueued on the calling thread's stream.  The transposed system
+ * (sub-diagonal c_{i-1}, super-diagonal a_{i+1}) is solved in place by the
+ * partitioned-Thomas kernels, gradients formed in the same pass. */
+TRID_EXTERN_C tridStatus_t tridDmtsvStridedBatchAdjoint(const double *a, const double *b,
+                                                        const double *c, const double *u,
+                                                        const double *w, double *da, double *db,
+                                                        double *dc, double *dd, int ndim,
+                                                        int solvedim, int *dims, int *pads);
+TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchAdjoint(const float *a, const float *b,
+                                                        const float *c, const float *u,
+                                                        const float *w, float *da, float *db,
+                                                        float *dc, float *dd, int ndim,
+                                                        int solvedim, int *dims, int *pads);
+
 /* ---- replaces trid_cuda.h:44 (a no-op in the reference, trid_cuda.cu:612) ---- */
 TRID_EXTERN_C void initTridMultiDimBatchSolve(int ndim, int *dims, int *pads);
 
@@ -111,6 +133,9 @@ TRID_EXTERN_C const char *tridGetStatusString(tridStatus_t status);
 /* Algorithm selection for the scalar solves (autotuner hook).
  *   method 0 = automatic (tuning table, then built-in heuristics)
  *   method 1 = Thomas, one thread per system, c'/d' in library scratch
+ *              (systems longer than 32*chunk rows are cut into blocks of
+ *              32*chunk rows by methods 2/3: block reduction, block system
+ *              solved recursively, block finish)
  *   method 2 = partitioned Thomas: per-thread chunks of `chunk` rows reduced to
  *              a 64-row interface system solved by warp shuffles (PCR); the
  *              rows are staged by TMA (bulk tensor copies) when the layout

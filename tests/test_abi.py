@@ -109,8 +109,15 @@ def test_method_override_and_query():
     m, ch, spc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     assert L.tridQueryMethod(8, 0, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
     assert (m.value, ch.value) == (2, 8)
+    # long systems: blocked partition with 256-row blocks
     assert L.tridQueryMethod(8, 1, 5000, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
-    assert m.value == 1
+    assert (m.value, ch.value) == (3, 8)
+    assert L.tridQueryMethod(8, 0, 65536, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+    assert (m.value, ch.value) == (2, 8)
+    assert L.tridQueryMethod(8, 1, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+    assert (m.value, ch.value, spc.value) == (3, 8, 8)
+    assert L.tridQueryMethod(8, 2, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+    assert (m.value, ch.value, spc.value) == (2, 8, 8)
     tb.set_method(1)
     assert L.tridQueryMethod(8, 0, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
     assert m.value == 1

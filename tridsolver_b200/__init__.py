@@ -23,6 +23,8 @@ from .scalar import (  # noqa: F401
     initTridMultiDimBatchSolve,
     solve,
     tridDmtsvStridedBatch,
+    tridDmtsvStridedBatchAdjoint,
+    tridSmtsvStridedBatchAdjoint,
     tridDmtsvStridedBatchInc,
     tridDmtsvStridedBatchPadded,
     tridDmtsvStridedBatchPaddedInc,
@@ -32,3 +34,4 @@ from .scalar import (  # noqa: F401
     tridSmtsvStridedBatchPaddedInc,
     set_method,
 )
+from .autograd import TridSolve, trid_solve  # noqa: F401

@@ -37,7 +37,11 @@ _SCALAR11 = _SCALAR9 + [ip, c_int]
 _PADDED = [vp, ip, vp, ip, vp, ip, vp, ip, vp, ip, c_int, c_int, ip, ip, c_int]
 
 # name -> (restype, argtypes) for the symbols every library exports
+_ADJ = [vp, vp, vp, vp, vp, vp, vp, vp, vp, c_int, c_int, ip, ip]
+
 _COMMON = {
+    "tridDmtsvStridedBatchAdjoint": (c_int, _ADJ),
+    "tridSmtsvStridedBatchAdjoint": (c_int, _ADJ),
     "tridDmtsvStridedBatchPadded": (c_int, _PADDED),
     "tridDmtsvStridedBatchPaddedInc": (c_int, _PADDED),
     "tridSmtsvStridedBatchPadded": (c_int, _PADDED),

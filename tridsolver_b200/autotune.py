@@ -54,6 +54,7 @@ def candidates(axis, n):
             else:
                 for spc in (4, 8, 16):
                     out.append((2, ch, spc))
+                    out.append((3, ch, spc))
     if axis > 0:
         out.append((4, 0, 0))
     return out

@@ -23,15 +23,18 @@ struct ScratchBuf {
   void *ptr = nullptr;
   size_t bytes = 0;
 };
+constexpr int kScratchLevels = 4;
 static std::mutex g_scratch_mu;
-static std::vector<ScratchBuf> g_scratch;  // indexed by device
+static std::vector<ScratchBuf> g_scratch;  // [device * kScratchLevels + level]
 
-void *scratch(size_t bytes) {
+void *scratch(size_t bytes, int level) {
   int dev = 0;
+  if (level < 0 || level >= kScratchLevels) return nullptr;
   if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
   std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if ((int)g_scratch.size() <= dev) g_scratch.resize(dev + 1);
-  ScratchBuf &s = g_scratch[dev];
+  const size_t slot = (size_t)dev * kScratchLevels + level;
+  if (g_scratch.size() <= slot) g_scratch.resize(slot + 1);
+  ScratchBuf &s = g_scratch[slot];
   if (s.bytes >= bytes) return s.ptr;
   if (s.ptr) {
     // kernels already queued may still read the old buffer
@@ -139,15 +142,21 @@ MethodChoice choose_method(int dtype_bytes, int axis, int n, int opt_hint) {
       }
     }
   }
-  if (m.method == 0) m.method = chunk_for(n, dtype_bytes) ? 2 : 1;
+  if (m.method == 0) {
+    // built-in defaults, from the B200 sweep of tridsolver_b200.autotune:
+    // TMA staging wins on axis 0 and on large strides, plain coalesced loads
+    // on moderate strides; systems longer than 512 rows take the blocked
+    // partition (method 2 with blocks of 32*chunk rows)
+    m.method = (axis == 1) ? 3 : 2;
+  }
   if (m.method >= 2) {
     const int need = chunk_for(n, dtype_bytes);
     if (need == 0) {
-      m.method = 1;  // longer than any register-resident partition
+      if (m.chunk == 0) m.chunk = 8;  // long system: blocks of 256 rows
     } else if (m.chunk < need) {
       m.chunk = need;
     }
-    if (m.spc == 0) m.spc = (dtype_bytes == 8) ? 8 : 16;
+    if (m.spc == 0) m.spc = 8;
   }
   return m;
 }
@@ -200,9 +209,55 @@ static bool aligned_ptr(const T *p) {
 }
 
 template <typename T, int INC>
-tridStatus_t solve_strided_batch(const T *a, const T *b, const T *c, T *d, T *u, int ndim,
-                                 int solvedim, const int *dims, const int *const pads[5],
-                                 const int *opts, int sync) {
+static tridStatus_t solve_level(const T *a, const T *b, const T *c, T *d, T *u, int ndim,
+                                int solvedim, const int *dims, const int *const pads[5],
+                                const int *opts, int sync, int level);
+
+// Blocked partition for any length (and the adjoint): block reduction ->
+// block system solved recursively at the next scratch level -> finish.
+template <typename T, int MODE>
+static tridStatus_t run_general(const Geom &g, GenArgs<T> A, int axis, int chunk, int spc,
+                                int level, cudaStream_t stream) {
+  const int B = 32 * chunk;
+  const int64_t nblk = (g.n + B - 1) / B;
+  if (nblk > 0x3fffffff || g.nsys > 0x7fffffff) return TRID_STATUS_INVALID_VALUE;
+  A.nblk = (int)nblk;
+  const int ax = axis == 0 ? 0 : 1;
+  if (nblk == 1) {
+    return launch_general_phase<T, MODE>(g, A, ax, chunk, spc, kGenSingle, stream) == cudaSuccess
+               ? TRID_STATUS_SUCCESS
+               : TRID_STATUS_EXECUTION_FAILED;
+  }
+  const int64_t len = g.nsys * 2 * nblk;
+  T *red = (T *)scratch((size_t)4 * len * sizeof(T), level);
+  if (!red) return TRID_STATUS_ALLOC_FAILED;
+  A.red = red;
+  if (launch_general_phase<T, MODE>(g, A, ax, chunk, spc, kGenReduce, stream) != cudaSuccess)
+    return TRID_STATUS_EXECUTION_FAILED;
+  // block system: nsys contiguous systems of 2*nblk rows, solution into its d
+  int bd[2] = {(int)(2 * nblk), (int)g.nsys};
+  const int *bp[5] = {bd, bd, bd, bd, bd};
+  const tridStatus_t st = solve_level<T, 0>(red, red + len, red + 2 * len, red + 3 * len, nullptr,
+                                            2, 0, bd, bp, nullptr, 0, level + 1);
+  if (st != TRID_STATUS_SUCCESS) return st;
+  A.bsol = red + 3 * len;
+  return launch_general_phase<T, MODE>(g, A, ax, chunk, spc, kGenFinish, stream) == cudaSuccess
+             ? TRID_STATUS_SUCCESS
+             : TRID_STATUS_EXECUTION_FAILED;
+}
+
+static int axis_class(const Geom &g, int solvedim, int elem_bytes) {
+  // 0 = unit stride inside a system, 1 = strided with a row stride of at most
+  // 64 KiB, 2 = larger strides (the outermost axis of a big cube, where
+  // DRAM-page and TLB locality differ)
+  if (solvedim == 0) return 0;
+  return g.stride[kD] * (int64_t)elem_bytes <= 65536 ? 1 : 2;
+}
+
+template <typename T, int INC>
+static tridStatus_t solve_level(const T *a, const T *b, const T *c, T *d, T *u, int ndim,
+                                int solvedim, const int *dims, const int *const pads[5],
+                                const int *opts, int sync, int level) {
   Geom g;
   const tridStatus_t st = make_geom(ndim, solvedim, dims, pads, INC != 0, g);
   if (st != TRID_STATUS_SUCCESS) return st;
@@ -212,13 +267,12 @@ tridStatus_t solve_strided_batch(const T *a, const T *b, const T *c, T *d, T *u,
   const int opt = opts ? opts[solvedim] : 0;
   if (opt < 0 || opt > 5) return TRID_STATUS_INVALID_VALUE;
   if (g.n == 0 || g.nsys == 0) return TRID_STATUS_SUCCESS;
+  if (level >= kScratchLevels) return TRID_STATUS_INTERNAL_ERROR;
 
   const cudaStream_t stream = current_stream();
-  // axis class: 0 = unit stride inside a system, 1 = strided with a row
-  // stride of at most 64 KiB, 2 = larger strides (e.g. the outermost axis of a
-  // big cube, where DRAM-page and TLB locality differ)
-  const int axis = (solvedim == 0) ? 0 : (g.stride[kD] * (int64_t)sizeof(T) <= 65536 ? 1 : 2);
+  const int axis = axis_class(g, solvedim, (int)sizeof(T));
   const MethodChoice m = choose_method((int)sizeof(T), axis, g.n, opt);
+  const bool fits = g.n <= 32 * m.chunk;
   cudaError_t e = cudaErrorNotSupported;
   if (m.method == 4 && axis >= 1) {
     unsigned *err = device_error_flags();
@@ -227,9 +281,19 @@ tridStatus_t solve_strided_batch(const T *a, const T *b, const T *c, T *d, T *u,
   }
   if (e != cudaErrorNotSupported) {
     // done (or failed) by the method-4 kernel
-  } else if (m.method == 2 || m.method == 3 || m.method == 4) {
+  } else if (m.method >= 2 && !fits) {
+    GenArgs<T> A = {};
+    A.a = a;
+    A.b = b;
+    A.c = c;
+    A.rhs = d;
+    A.out = INC ? u : d;
+    const tridStatus_t s2 = INC ? run_general<T, kGenFwdInc>(g, A, axis, m.chunk, m.spc, level, stream)
+                                : run_general<T, kGenFwd>(g, A, axis, m.chunk, m.spc, level, stream);
+    if (s2 != TRID_STATUS_SUCCESS) return s2;
+    e = cudaSuccess;
+  } else if (m.method >= 2) {
     if (axis == 0) {
-      e = cudaErrorNotSupported;
       if (m.method == 2) {
         unsigned *err = device_error_flags();
         if (!err) return TRID_STATUS_ALLOC_FAILED;
@@ -237,12 +301,11 @@ tridStatus_t solve_strided_batch(const T *a, const T *b, const T *c, T *d, T *u,
       }
       if (e == cudaErrorNotSupported) e = launch_xsolve<T, INC>(g, a, b, c, d, u, m.chunk, stream);
     } else {
-      e = cudaErrorNotSupported;
       if (m.method == 2) {
         unsigned *err = device_error_flags();
         if (!err) return TRID_STATUS_ALLOC_FAILED;
         e = launch_strided_part_tma<T, INC>(g, dims, pads, ndim, solvedim, a, b, c, d, u, m.chunk,
-                                            m.spc, err, stream);
+                                            m.spc, true, err, stream);
       }
       if (e == cudaErrorNotSupported)
         e = launch_strided<T, INC>(g, a, b, c, d, u, m.chunk, m.spc, stream);
@@ -252,7 +315,7 @@ tridStatus_t solve_strided_batch(const T *a, const T *b, const T *c, T *d, T *u,
     const size_t per_sys = (size_t)2 * g.n * sizeof(T);
     int64_t ws = (int64_t)(((size_t)1 << 30) / per_sys);
     ws = std::max<int64_t>(1, std::min<int64_t>(ws, g.nsys));
-    T *work = (T *)scratch(per_sys * (size_t)ws);
+    T *work = (T *)scratch(per_sys * (size_t)ws, level);
     if (!work) return TRID_STATUS_ALLOC_FAILED;
     e = launch_generic<T, INC>(g, a, b, c, d, u, work, ws, stream);
   }
@@ -260,6 +323,52 @@ tridStatus_t solve_strided_batch(const T *a, const T *b, const T *c, T *d, T *u,
   if (sync == 1 && cudaStreamSynchronize(stream) != cudaSuccess) return TRID_STATUS_EXECUTION_FAILED;
   return TRID_STATUS_SUCCESS;
 }
+
+template <typename T, int INC>
+tridStatus_t solve_strided_batch(const T *a, const T *b, const T *c, T *d, T *u, int ndim,
+                                 int solvedim, const int *dims, const int *const pads[5],
+                                 const int *opts, int sync) {
+  return solve_level<T, INC>(a, b, c, d, u, ndim, solvedim, dims, pads, opts, sync, 0);
+}
+
+// Adjoint of the strided-batch solve (one pads array for every operand).
+template <typename T>
+tridStatus_t solve_adjoint(const T *a, const T *b, const T *c, const T *u, const T *w, T *ga,
+                           T *gb, T *gc, T *gd, int ndim, int solvedim, const int *dims,
+                           const int *pads) {
+  const int *p[5] = {pads, pads, pads, pads, pads};
+  Geom g;
+  const tridStatus_t st = make_geom(ndim, solvedim, dims, p, true, g);
+  if (st != TRID_STATUS_SUCCESS) return st;
+  if (!aligned_ptr(a) || !aligned_ptr(b) || !aligned_ptr(c) || !aligned_ptr(u) || !aligned_ptr(w))
+    return TRID_STATUS_INVALID_VALUE;
+  for (const T *o : {(const T *)ga, (const T *)gb, (const T *)gc, (const T *)gd})
+    if (o && ((uintptr_t)o % sizeof(T)) != 0) return TRID_STATUS_INVALID_VALUE;
+  if (g.n == 0 || g.nsys == 0) return TRID_STATUS_SUCCESS;
+  const cudaStream_t stream = current_stream();
+  const int axis = axis_class(g, solvedim, (int)sizeof(T));
+  MethodChoice m = choose_method((int)sizeof(T), axis, g.n, 0);
+  if (m.chunk == 0) m.chunk = 8;
+  if (m.spc == 0) m.spc = 8;
+  GenArgs<T> A = {};
+  A.a = a;
+  A.b = b;
+  A.c = c;
+  A.rhs = w;
+  A.usol = u;
+  A.ga = ga;
+  A.gb = gb;
+  A.gc = gc;
+  A.gd = gd;
+  return run_general<T, kGenAdj>(g, A, axis, m.chunk, m.spc, 0, stream);
+}
+template tridStatus_t solve_adjoint<float>(const float *, const float *, const float *,
+                                           const float *, const float *, float *, float *,
+                                           float *, float *, int, int, const int *, const int *);
+template tridStatus_t solve_adjoint<double>(const double *, const double *, const double *,
+                                            const double *, const double *, double *, double *,
+                                            double *, double *, int, int, const int *,
+                                            const int *);
 
 template tridStatus_t solve_strided_batch<float, 0>(const float *, const float *, const float *,
                                                     float *, float *, int, int, const int *,
@@ -323,6 +432,22 @@ TRID_PADDED(tridDmtsvStridedBatchPadded, double, 0)
 TRID_PADDED(tridDmtsvStridedBatchPaddedInc, double, 1)
 TRID_PADDED(tridSmtsvStridedBatchPadded, float, 0)
 TRID_PADDED(tridSmtsvStridedBatchPaddedInc, float, 1)
+
+extern "C" tridStatus_t tridDmtsvStridedBatchAdjoint(const double *a, const double *b,
+                                                     const double *c, const double *u,
+                                                     const double *w, double *da, double *db,
+                                                     double *dc, double *dd, int ndim,
+                                                     int solvedim, int *dims, int *pads) {
+  return solve_adjoint<double>(a, b, c, u, w, da, db, dc, dd, ndim, solvedim, dims, pads);
+}
+
+extern "C" tridStatus_t tridSmtsvStridedBatchAdjoint(const float *a, const float *b,
+                                                     const float *c, const float *u,
+                                                     const float *w, float *da, float *db,
+                                                     float *dc, float *dd, int ndim, int solvedim,
+                                                     int *dims, int *pads) {
+  return solve_adjoint<float>(a, b, c, u, w, da, db, dc, dd, ndim, solvedim, dims, pads);
+}
 
 extern "C" void initTridMultiDimBatchSolve(int ndim, int *dims, int *pads) {
   (void)ndim;

@@ -1,0 +1,277 @@
+// General partitioned-Thomas kernels (sm_100a): any system length, the
+// forward solve and the adjoint solve.
+//
+// A system is cut into blocks of B = 32*M rows (one warp's 32 chunks).
+//  * n <= B  (phase kSingle): chunk reduction, warp interface solve,
+//    back-substitution -- the algorithm of partition.cuh.
+//  * n >  B  (three launches, see launch_general):
+//      kReduce : every block reduces to two rows in its own first/last
+//                unknowns (warp_block_basis + block_rows), written to
+//                scratch as a tridiagonal system of 2*nblk rows per system;
+//      (the block system is solved by the strided-batch dispatcher itself,
+//       recursively, as a contiguous batch);
+//      kFinish : every block recomputes its chunk reduction, takes its two
+//                boundary unknowns from the block solution and
+//                back-substitutes.
+//    The block pass re-reads a, b, c and the right-hand side, so long
+//    systems move 72 bytes per FP64 unknown instead of the 40-byte minimum.
+//
+// Row modes:
+//  * kFwd / kFwdInc: the strided-batch solve (x overwrites d / u += x),
+//    a_i x_{i-1} + b_i x_i + c_i x_{i+1} = d_i (trid_cpu.cpp:360-401).
+//  * kAdj: the adjoint of that solve for a loss L(x): with the cotangent
+//    w = dL/dx and the forward solution u, g = A^{-T} w is the solution of
+//    the transposed system c_{i-1} g_{i-1} + b_i g_i + a_{i+1} g_{i+1} = w_i,
+//    and dL/dd = g, dL/da_i = -g_i u_{i-1}, dL/db_i = -g_i u_i,
+//    dL/dc_i = -g_i u_{i+1} (zero where a_0 / c_{n-1} are unused).  The
+//    transposed coefficients are read in place (no shifted copies), and the
+//    gradients are formed in the same pass.
+//
+// Layouts: axis 0 (unit stride, one warp per system block) and strided axes
+// (SB adjacent systems per CTA, thread = (system, chunk), interface rows
+// transposed through shared memory so one warp solves one system's block).
+#include "partition.cuh"
+
+namespace tridb200 {
+
+constexpr int kFwd = kGenFwd, kFwdInc = kGenFwdInc, kAdj = kGenAdj;
+constexpr int kSingle = kGenSingle, kReduce = kGenReduce, kFinish = kGenFinish;
+
+// ---------------------------------------------------------------- rows --
+template <typename T, int M, int MODE>
+__device__ __forceinline__ void load_rows(const GenArgs<T> &A, const int64_t (&off)[5],
+                                          const Geom &g, int rbase, bool valid, T (&al)[M],
+                                          T (&be)[M], T (&ga)[M], T (&de)[M]) {
+  const int n = g.n;
+  const int64_t sa = g.stride[kA], sb = g.stride[kB], sc = g.stride[kC], sd = g.stride[kD];
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int r = rbase + j;
+    if (valid && r < n) {
+      if (MODE == kAdj) {
+        al[j] = (r == 0) ? T(0) : A.c[off[kC] + (int64_t)(r - 1) * sc];
+        ga[j] = (r == n - 1) ? T(0) : A.a[off[kA] + (int64_t)(r + 1) * sa];
+      } else {
+        al[j] = (r == 0) ? T(0) : A.a[off[kA] + (int64_t)r * sa];
+        ga[j] = (r == n - 1) ? T(0) : A.c[off[kC] + (int64_t)r * sc];
+      }
+      be[j] = A.b[off[kB] + (int64_t)r * sb];
+      de[j] = A.rhs[off[kD] + (int64_t)r * sd];
+    } else {
+      al[j] = T(0);
+      be[j] = T(1);
+      ga[j] = T(0);
+      de[j] = T(0);
+    }
+  }
+}
+
+template <typename T, int M, int MODE>
+__device__ __forceinline__ void store_rows(const GenArgs<T> &A, const int64_t (&off)[5],
+                                           const Geom &g, int rbase, const T (&x)[M]) {
+  const int n = g.n;
+  if (MODE == kFwd) {
+    const int64_t sd = g.stride[kD];
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+      if (rbase + j < n) A.out[off[kD] + (int64_t)(rbase + j) * sd] = x[j];
+  } else if (MODE == kFwdInc) {
+    const int64_t su = g.stride[kU];
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+      if (rbase + j < n) A.out[off[kU] + (int64_t)(rbase + j) * su] += x[j];
+  } else {
+    // gradients; u shares the geometry of array slot kU
+    const int64_t su = g.stride[kU];
+    const T *u = A.usol + off[kU];
+    T uprev = (rbase > 0 && rbase - 1 < n) ? u[(int64_t)(rbase - 1) * su] : T(0);
+    T ucur = (rbase < n) ? u[(int64_t)rbase * su] : T(0);
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int r = rbase + j;
+      if (r >= n) break;
+      const T unext = (r + 1 < n) ? u[(int64_t)(r + 1) * su] : T(0);
+      const T gg = x[j];
+      if (A.gd) A.gd[off[kD] + (int64_t)r * g.stride[kD]] = gg;
+      if (A.gb) A.gb[off[kB] + (int64_t)r * g.stride[kB]] = -gg * ucur;
+      if (A.ga) A.ga[off[kA] + (int64_t)r * g.stride[kA]] = (r > 0) ? -gg * uprev : T(0);
+      if (A.gc) A.gc[off[kC] + (int64_t)r * g.stride[kC]] = (r + 1 < n) ? -gg * unext : T(0);
+      uprev = ucur;
+      ucur = unext;
+    }
+  }
+}
+
+// block-level bookkeeping shared by both layouts (whole warp calls it)
+template <typename T, int PHASE>
+__device__ __forceinline__ void block_step(const GenArgs<T> &A, int64_t sys, int blk, int64_t nsys,
+                                           const Row<T> &F, const Row<T> &L, int lane, T &xF,
+                                           T &xL) {
+  if (PHASE == kSingle) {
+    warp_interface_solve(F, L, xF, xL, lane);
+    return;
+  }
+  T bF[3], bL[3];
+  warp_block_basis(F, L, lane, bF, bL);
+  const int64_t m = 2 * (int64_t)A.nblk;
+  if (PHASE == kReduce) {
+    Row<T> FB, LB;
+    block_rows(F, L, bF, bL, lane, FB, LB);
+    if (sys < nsys) {
+      const int64_t plane = nsys * m;
+      const int64_t i = sys * m + 2 * (int64_t)blk;
+      if (lane == 0) {
+        A.red[0 * plane + i] = FB.a;
+        A.red[1 * plane + i] = FB.b;
+        A.red[2 * plane + i] = FB.c;
+        A.red[3 * plane + i] = FB.d;
+        A.red[0 * plane + i + 1] = LB.a;
+        A.red[1 * plane + i + 1] = LB.b;
+        A.red[2 * plane + i + 1] = LB.c;
+        A.red[3 * plane + i + 1] = LB.d;
+      }
+    }
+    xF = xL = T(0);
+  } else {
+    T fB = T(0), lB = T(0);
+    if (sys < nsys) {
+      fB = A.bsol[sys * m + 2 * (int64_t)blk];
+      lB = A.bsol[sys * m + 2 * (int64_t)blk + 1];
+    }
+    xF = bF[0] + fB * bF[1] + lB * bF[2];
+    xL = bL[0] + fB * bL[1] + lB * bL[2];
+  }
+}
+
+// --------------------------------------------------------------- axis 0 --
+template <typename T, int M, int MODE, int PHASE>
+__global__ void __launch_bounds__(128) gen_x_kernel(Geom g, GenArgs<T> A) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int64_t item = (int64_t)blockIdx.x * (blockDim.x / kWarp) + (threadIdx.x / kWarp);
+  const int64_t sys = item / A.nblk;
+  const int blk = (int)(item % A.nblk);
+  if (sys >= g.nsys) return;  // uniform per warp
+  int64_t off[5];
+  system_offsets(g, sys, off);
+  const int rbase = blk * 32 * M + lane * M;
+  T al[M], be[M], ga[M], de[M];
+  load_rows<T, M, MODE>(A, off, g, rbase, true, al, be, ga, de);
+  Row<T> F, L;
+  chunk_reduce<T, M>(al, be, ga, de, F, L);
+  T xF, xL;
+  block_step<T, PHASE>(A, sys, blk, g.nsys, F, L, lane, xF, xL);
+  if (PHASE == kReduce) return;
+  chunk_backsub<T, M>(al, ga, de, xF, xL);
+  store_rows<T, M, MODE>(A, off, g, rbase, de);
+}
+
+// --------------------------------------------------------- strided axes --
+template <typename T, int M, int SB, int MODE, int PHASE>
+__global__ void __launch_bounds__(SB * kWarp) gen_s_kernel(Geom g, GenArgs<T> A) {
+  __shared__ T red[8][kWarp][SB + 1];
+  __shared__ T sol[2][kWarp][SB + 1];
+  const int tid = threadIdx.x;
+  const int sl = tid % SB;
+  const int t = tid / SB;
+  const int64_t ntile = (g.nsys + SB - 1) / SB;
+  const int64_t tile = (int64_t)blockIdx.x % ntile;
+  const int blk = (int)((int64_t)blockIdx.x / ntile);
+  const int64_t sys = tile * SB + sl;
+  const bool valid = sys < g.nsys;
+  int64_t off[5] = {0, 0, 0, 0, 0};
+  if (valid) system_offsets(g, sys, off);
+  const int rbase = blk * 32 * M + t * M;
+  T al[M], be[M], ga[M], de[M];
+  load_rows<T, M, MODE>(A, off, g, rbase, valid, al, be, ga, de);
+  Row<T> F, L;
+  chunk_reduce<T, M>(al, be, ga, de, F, L);
+  red[0][t][sl] = F.a;
+  red[1][t][sl] = F.b;
+  red[2][t][sl] = F.c;
+  red[3][t][sl] = F.d;
+  red[4][t][sl] = L.a;
+  red[5][t][sl] = L.b;
+  red[6][t][sl] = L.c;
+  red[7][t][sl] = L.d;
+  __syncthreads();
+  {
+    const int w = tid / kWarp;
+    const int lane = tid & (kWarp - 1);
+    const Row<T> F2{red[0][lane][w], red[1][lane][w], red[2][lane][w], red[3][lane][w]};
+    const Row<T> L2{red[4][lane][w], red[5][lane][w], red[6][lane][w], red[7][lane][w]};
+    T xF, xL;
+    block_step<T, PHASE>(A, tile * SB + w, blk, g.nsys, F2, L2, lane, xF, xL);
+    sol[0][lane][w] = xF;
+    sol[1][lane][w] = xL;
+  }
+  if (PHASE == kReduce) return;
+  __syncthreads();
+  chunk_backsub<T, M>(al, ga, de, sol[0][t][sl], sol[1][t][sl]);
+  if (valid) store_rows<T, M, MODE>(A, off, g, rbase, de);
+}
+
+// -------------------------------------------------------------- launchers --
+template <typename T, int M, int MODE, int PHASE>
+static cudaError_t go_x(const Geom &g, const GenArgs<T> &A, cudaStream_t st) {
+  constexpr int kW = 4;
+  const int64_t items = g.nsys * A.nblk;
+  const int64_t blocks = (items + kW - 1) / kW;
+  if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
+  gen_x_kernel<T, M, MODE, PHASE><<<dim3((unsigned)blocks), dim3(kW * kWarp), 0, st>>>(g, A);
+  return cudaGetLastError();
+}
+
+template <typename T, int M, int SB, int MODE, int PHASE>
+static cudaError_t go_s(const Geom &g, const GenArgs<T> &A, cudaStream_t st) {
+  const int64_t blocks = ((g.nsys + SB - 1) / SB) * A.nblk;
+  if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
+  gen_s_kernel<T, M, SB, MODE, PHASE><<<dim3((unsigned)blocks), dim3(SB * kWarp), 0, st>>>(g, A);
+  return cudaGetLastError();
+}
+
+template <typename T, int M, int MODE, int PHASE>
+static cudaError_t go(const Geom &g, const GenArgs<T> &A, int axis, int spc, cudaStream_t st) {
+  if (axis == 0) return go_x<T, M, MODE, PHASE>(g, A, st);
+  switch (spc) {
+    case 4: return go_s<T, M, 4, MODE, PHASE>(g, A, st);
+    case 8: return go_s<T, M, 8, MODE, PHASE>(g, A, st);
+    case 16: return go_s<T, M, 16, MODE, PHASE>(g, A, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T, int MODE, int PHASE>
+static cudaError_t go_m(const Geom &g, const GenArgs<T> &A, int axis, int chunk, int spc,
+                        cudaStream_t st) {
+  switch (chunk) {
+    case 2: return go<T, 2, MODE, PHASE>(g, A, axis, spc, st);
+    case 4: return go<T, 4, MODE, PHASE>(g, A, axis, spc, st);
+    case 8: return go<T, 8, MODE, PHASE>(g, A, axis, spc, st);
+    case 16: return go<T, 16, MODE, PHASE>(g, A, axis, spc, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// One launch of the general family.  axis 0 = unit stride, else strided.
+template <typename T, int MODE>
+cudaError_t launch_general_phase(const Geom &g, const GenArgs<T> &A, int axis, int chunk, int spc,
+                                 int phase, cudaStream_t st) {
+  switch (phase) {
+    case kSingle: return go_m<T, MODE, kSingle>(g, A, axis, chunk, spc, st);
+    case kReduce: return go_m<T, MODE, kReduce>(g, A, axis, chunk, spc, st);
+    case kFinish: return go_m<T, MODE, kFinish>(g, A, axis, chunk, spc, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+#define TRID_GEN_INSTANTIATE(T, MODE)                                                         \
+  template cudaError_t launch_general_phase<T, MODE>(const Geom &, const GenArgs<T> &, int, int, \
+                                                     int, int, cudaStream_t);
+TRID_GEN_INSTANTIATE(float, kFwd)
+TRID_GEN_INSTANTIATE(float, kFwdInc)
+TRID_GEN_INSTANTIATE(float, kAdj)
+TRID_GEN_INSTANTIATE(double, kFwd)
+TRID_GEN_INSTANTIATE(double, kFwdInc)
+TRID_GEN_INSTANTIATE(double, kAdj)
+
+}  // namespace tridb200

@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(SB * kWarp) strided_part_tma_kernel(
     const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mb,
     const __grid_constant__ CUtensorMap mc, const __grid_constant__ CUtensorMap md,
     const __grid_constant__ CUtensorMap mu, Geom g, int solvedim, int box_rows, int nbox,
-    int red_off, unsigned *err) {
+    int red_off, int prefetch_dist, unsigned *err) {
   constexpr int NA = INC ? 5 : 4;
   extern __shared__ unsigned char smem_raw[];
   __shared__ uint64_t bar;
@@ -46,18 +46,21 @@ __global__ void __launch_bounds__(SB * kWarp) strided_part_tma_kernel(
   const int n = g.n;
 
   // tile -> coordinates (x0 on axis 0, the other non-solve axes)
-  const int ntx = (g.odims[0] + SB - 1) / SB;
-  int coord[5] = {(int)(blockIdx.x % ntx) * SB, 0, 0, 0, 0};
-  {
-    uint32_t rest = blockIdx.x / ntx;
+  auto tile_coords = [&](uint32_t blk, int (&cc)[5]) {
+    const int ntx = (g.odims[0] + SB - 1) / SB;
+    cc[0] = (int)(blk % ntx) * SB;
+    cc[1] = cc[2] = cc[3] = cc[4] = 0;
+    uint32_t rest = blk / ntx;
     int o = 1;
     for (int k = 1; k < 5; ++k) {
       if (k == solvedim || o >= g.nod) continue;
       const uint32_t e = (uint32_t)g.odims[o++];
-      coord[k] = (int)(rest % e);
+      cc[k] = (int)(rest % e);
       rest /= e;
     }
-  }
+  };
+  int coord[5];
+  tile_coords(blockIdx.x, coord);
   const CUtensorMap *maps[5] = {&ma, &mb, &mc, &md, &mu};
   // every copy destination (tile starts, second boxes) must be 128-byte aligned
   if (!tma_smem_aligned(tile) || (nbox > 1 && ((size_t)box_rows * SB * sizeof(T)) % 128 != 0)) {
@@ -79,6 +82,19 @@ __global__ void __launch_bounds__(SB * kWarp) strided_part_tma_kernel(
         tma_load_5d(tile + q * tsz + (size_t)bx * box_rows * SB, maps[q], &bar, c[0], c[1], c[2],
                     c[3], c[4]);
       }
+    // warm L2 with the tile this CTA's successor on the SM will load: keeps
+    // more bytes in flight than the resident tiles alone
+    const uint32_t nb = blockIdx.x + (uint32_t)prefetch_dist;
+    if (prefetch_dist > 0 && nb < gridDim.x) {
+      int pc[5];
+      tile_coords(nb, pc);
+      for (int q = 0; q < NA; ++q)
+        for (int bx = 0; bx < nbox; ++bx) {
+          int c[5] = {pc[0], pc[1], pc[2], pc[3], pc[4]};
+          c[solvedim] = bx * box_rows;
+          tma_prefetch_5d(maps[q], c[0], c[1], c[2], c[3], c[4]);
+        }
+    }
   }
   if (!mbar_wait(&bar, 0, err)) {
     mbar_wait(&bar, 0, nullptr);
@@ -167,7 +183,7 @@ __global__ void __launch_bounds__(SB * kWarp) strided_part_tma_kernel(
 template <typename T, int M, int SB, int INC>
 static cudaError_t launch_sptma(const CUtensorMap *maps, const Geom &g, int solvedim,
                                 int box_rows, int nbox, int64_t blocks, unsigned *err,
-                                cudaStream_t st, int optin) {
+                                cudaStream_t st, int optin, bool prefetch_tiles) {
   constexpr int NA = INC ? 5 : 4;
   constexpr int kAlignElems = 128 / (int)sizeof(T);
   const size_t tsz = (((size_t)box_rows * nbox * SB + kAlignElems - 1) / kAlignElems) * kAlignElems;
@@ -180,21 +196,29 @@ static cudaError_t launch_sptma(const CUtensorMap *maps, const Geom &g, int solv
   auto kern = strided_part_tma_kernel<T, M, SB, INC>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  // prefetch distance = CTAs resident on the whole GPU at once
+  int per_sm = 0, dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SB * kWarp, smem) != cudaSuccess)
+    per_sm = 0;
+  const int dist = prefetch_tiles ? per_sm * sms : 0;
   kern<<<dim3((unsigned)blocks), dim3(SB * kWarp), smem, st>>>(
-      maps[0], maps[1], maps[2], maps[3], maps[4], g, solvedim, box_rows, nbox, red_off, err);
+      maps[0], maps[1], maps[2], maps[3], maps[4], g, solvedim, box_rows, nbox, red_off, dist,
+      err);
   return cudaGetLastError();
 }
 
 template <typename T, int M, int INC>
 static cudaError_t launch_sptma_sb(const CUtensorMap *maps, const Geom &g, int solvedim,
                                    int box_rows, int nbox, int spc, int64_t ntiles_rest,
-                                   unsigned *err, cudaStream_t st, int optin) {
+                                   unsigned *err, cudaStream_t st, int optin, bool prefetch) {
   const int64_t blocks = ((g.odims[0] + spc - 1) / spc) * ntiles_rest;
   if (blocks > 0x7fffffff || blocks == 0) return cudaErrorNotSupported;
   switch (spc) {
-    case 4: return launch_sptma<T, M, 4, INC>(maps, g, solvedim, box_rows, nbox, blocks, err, st, optin);
-    case 8: return launch_sptma<T, M, 8, INC>(maps, g, solvedim, box_rows, nbox, blocks, err, st, optin);
-    case 16: return launch_sptma<T, M, 16, INC>(maps, g, solvedim, box_rows, nbox, blocks, err, st, optin);
+    case 4: return launch_sptma<T, M, 4, INC>(maps, g, solvedim, box_rows, nbox, blocks, err, st, optin, prefetch);
+    case 8: return launch_sptma<T, M, 8, INC>(maps, g, solvedim, box_rows, nbox, blocks, err, st, optin, prefetch);
+    case 16: return launch_sptma<T, M, 16, INC>(maps, g, solvedim, box_rows, nbox, blocks, err, st, optin, prefetch);
     default: return cudaErrorNotSupported;
   }
 }
@@ -202,8 +226,8 @@ static cudaError_t launch_sptma_sb(const CUtensorMap *maps, const Geom &g, int s
 template <typename T, int INC>
 cudaError_t launch_strided_part_tma(const Geom &g, const int *dims, const int *const pads[5],
                                     int ndim, int solvedim, const T *a, const T *b, const T *c,
-                                    T *d, T *u, int chunk, int spc, unsigned *err,
-                                    cudaStream_t st) {
+                                    T *d, T *u, int chunk, int spc, bool prefetch,
+                                    unsigned *err, cudaStream_t st) {
   if (solvedim < 1 || ndim > 5 || g.n > 32 * chunk || dims[0] < spc) return cudaErrorNotSupported;
   const int box_rows = g.n < 256 ? g.n : 256;
   const int nbox = (g.n + box_rows - 1) / box_rows;
@@ -232,10 +256,10 @@ cudaError_t launch_strided_part_tma(const Geom &g, const int *dims, const int *c
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const int64_t rest = g.nsys / dims[0];
   switch (chunk) {
-    case 2: return launch_sptma_sb<T, 2, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin);
-    case 4: return launch_sptma_sb<T, 4, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin);
-    case 8: return launch_sptma_sb<T, 8, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin);
-    case 16: return launch_sptma_sb<T, 16, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin);
+    case 2: return launch_sptma_sb<T, 2, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin, prefetch);
+    case 4: return launch_sptma_sb<T, 4, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin, prefetch);
+    case 8: return launch_sptma_sb<T, 8, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin, prefetch);
+    case 16: return launch_sptma_sb<T, 16, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin, prefetch);
     default: return cudaErrorNotSupported;
   }
 }
@@ -243,7 +267,7 @@ cudaError_t launch_strided_part_tma(const Geom &g, const int *dims, const int *c
 #define TRID_SPTMA_INSTANTIATE(T, INC)                                                         \
   template cudaError_t launch_strided_part_tma<T, INC>(                                        \
       const Geom &, const int *, const int *const[5], int, int, const T *, const T *, const T *, \
-      T *, T *, int, int, unsigned *, cudaStream_t);
+      T *, T *, int, int, bool, unsigned *, cudaStream_t);
 TRID_SPTMA_INSTANTIATE(float, 0)
 TRID_SPTMA_INSTANTIATE(float, 1)
 TRID_SPTMA_INSTANTIATE(double, 0)

@@ -140,4 +140,131 @@ __device__ __forceinline__ void warp_interface_solve(const Row<T> &F, const Row<
   xF = (F.d - (lane > 0 ? F.a * lprev : T(0)) - F.c * xL) * ifb;
 }
 
+// The interface system of one warp with several right-hand sides: NR
+// independent RHS columns share the elimination (used to express a block's
+// interior in terms of its two boundary unknowns).  Same recurrence as
+// warp_interface_solve.
+template <typename T, int NR>
+struct RowN {
+  T a, b, c, d[NR];
+};
+
+template <typename T, int NR>
+__device__ __forceinline__ void warp_interface_solve_n(const RowN<T, NR> &F, const RowN<T, NR> &L,
+                                                       T (&xF)[NR], T (&xL)[NR], int lane) {
+  constexpr unsigned kFull = 0xffffffffu;
+  const T ifb = rcp(F.b);
+  T nfa = __shfl_down_sync(kFull, F.a, 1);
+  T nfi = __shfl_down_sync(kFull, ifb, 1);
+  T nfc = __shfl_down_sync(kFull, F.c, 1);
+  T nfd[NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) nfd[k] = __shfl_down_sync(kFull, F.d[k], 1);
+  if (lane == kWarp - 1) {
+    nfa = T(0);
+    nfi = T(1);
+    nfc = T(0);
+#pragma unroll
+    for (int k = 0; k < NR; ++k) nfd[k] = T(0);
+  }
+  const T p = L.a * ifb;
+  const T q = L.c * nfi;
+  T ra = -p * F.a;
+  T rb = L.b - p * F.c - q * nfa;
+  T rc = -q * nfc;
+  T rd[NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) rd[k] = L.d[k] - p * F.d[k] - q * nfd[k];
+#pragma unroll
+  for (int s = 1; s < kWarp; s <<= 1) {
+    const T ib = rcp(rb);
+    const T sa = ra * ib, sc = rc * ib;
+    const T ua = __shfl_up_sync(kFull, sa, s);
+    const T uc = __shfl_up_sync(kFull, sc, s);
+    const T da = __shfl_down_sync(kFull, sa, s);
+    const T dc = __shfl_down_sync(kFull, sc, s);
+    const T k1 = (lane >= s) ? ra : T(0);
+    const T k2 = (lane + s < kWarp) ? rc : T(0);
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      const T sd = rd[k] * ib;
+      const T ud = __shfl_up_sync(kFull, sd, s);
+      const T dd = __shfl_down_sync(kFull, sd, s);
+      rd[k] = rd[k] - k1 * ud - k2 * dd;
+    }
+    ra = -k1 * ua;
+    rc = -k2 * dc;
+    rb = rb - k1 * uc - k2 * da;
+  }
+  const T irb = rcp(rb);
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    xL[k] = rd[k] * irb;
+    const T lprev = __shfl_up_sync(kFull, xL[k], 1);
+    xF[k] = (F.d[k] - (lane > 0 ? F.a * lprev : T(0)) - F.c * xL[k]) * ifb;
+  }
+}
+
+// Block reduction: the 32 chunks of a warp form a block of 32*M rows whose
+// first unknown F^B (lane 0's F) and last unknown L^B (lane 31's L) are kept;
+// the 62 interface unknowns in between are expressed as
+//   x = P + F^B * UF + L^B * UL
+// by one 3-RHS solve in which lane 0's F row and lane 31's L row are replaced
+// by identity rows.  Returns, per lane, (P, UF, UL) for its F and L unknown.
+template <typename T>
+__device__ __forceinline__ void warp_block_basis(const Row<T> &F, const Row<T> &L, int lane,
+                                                 T (&bF)[3], T (&bL)[3]) {
+  RowN<T, 3> F3, L3;
+  F3.a = F.a;
+  F3.b = F.b;
+  F3.c = F.c;
+  F3.d[0] = F.d;
+  F3.d[1] = T(0);
+  F3.d[2] = T(0);
+  L3.a = L.a;
+  L3.b = L.b;
+  L3.c = L.c;
+  L3.d[0] = L.d;
+  L3.d[1] = T(0);
+  L3.d[2] = T(0);
+  if (lane == 0) {  // F_0 = F^B
+    F3.a = T(0);
+    F3.b = T(1);
+    F3.c = T(0);
+    F3.d[0] = T(0);
+    F3.d[1] = T(1);
+  }
+  if (lane == kWarp - 1) {  // L_31 = L^B
+    L3.a = T(0);
+    L3.b = T(1);
+    L3.c = T(0);
+    L3.d[0] = T(0);
+    L3.d[2] = T(1);
+  }
+  warp_interface_solve_n<T, 3>(F3, L3, bF, bL, lane);
+}
+
+// The two rows of a block's reduced equations, from the original interface
+// rows of lanes 0 and 31 and the basis of warp_block_basis:
+//   FB row: fa*L^B_{k-1} + (fb + fc*UF(L_0))*F^B + fc*UL(L_0)*L^B = fd - fc*P(L_0)
+//   LB row: la*UF(F_31)*F^B + (lb + la*UL(F_31))*L^B + lc*F^B_{k+1} = ld - la*P(F_31)
+// (lane 0 fills FB, lane 31 fills LB).
+template <typename T>
+__device__ __forceinline__ void block_rows(const Row<T> &F, const Row<T> &L, const T (&bF)[3],
+                                           const T (&bL)[3], int lane, Row<T> &FB, Row<T> &LB) {
+  const T l0P = __shfl_sync(0xffffffffu, bL[0], 0);
+  const T l0F = __shfl_sync(0xffffffffu, bL[1], 0);
+  const T l0L = __shfl_sync(0xffffffffu, bL[2], 0);
+  const T f31P = __shfl_sync(0xffffffffu, bF[0], kWarp - 1);
+  const T f31F = __shfl_sync(0xffffffffu, bF[1], kWarp - 1);
+  const T f31L = __shfl_sync(0xffffffffu, bF[2], kWarp - 1);
+  const T fa = __shfl_sync(0xffffffffu, F.a, 0), fb = __shfl_sync(0xffffffffu, F.b, 0);
+  const T fc = __shfl_sync(0xffffffffu, F.c, 0), fd = __shfl_sync(0xffffffffu, F.d, 0);
+  const T la = __shfl_sync(0xffffffffu, L.a, kWarp - 1), lb = __shfl_sync(0xffffffffu, L.b, kWarp - 1);
+  const T lc = __shfl_sync(0xffffffffu, L.c, kWarp - 1), ld = __shfl_sync(0xffffffffu, L.d, kWarp - 1);
+  (void)lane;
+  FB = {fa, fb + fc * l0F, fc * l0L, fd - fc * l0P};
+  LB = {la * f31F, lb + la * f31L, lc, ld - la * f31P};
+}
+
 }  // namespace tridb200

@@ -97,6 +97,15 @@ __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
+// bring a tile into L2 ahead of its real load (no shared memory involved)
+__device__ __forceinline__ void tma_prefetch_5d(const CUtensorMap *map, int c0, int c1, int c2,
+                                                int c3, int c4) {
+  asm volatile(
+      "cp.async.bulk.prefetch.tensor.5d.L2.global.tile [%0, {%1, %2, %3, %4, %5}];" ::"l"(map),
+      "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+      : "memory");
+}
+
 __device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, const void *src, int c0,
                                              int c1) {
   asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%2, %3}], [%1];" ::

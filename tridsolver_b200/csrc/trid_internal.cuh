@@ -112,9 +112,11 @@ __device__ __forceinline__ float rcp(float x) {
 // Per-thread library state (stream), defined in api_scalar.cu.
 cudaStream_t current_stream();
 
-// Device scratch owned by the library (grow-only, per device).  Returns
-// nullptr on allocation failure.
-void *scratch(size_t bytes);
+// Device scratch owned by the library (grow-only, per device and nesting
+// level: a long-system solve at level L solves its block system at level
+// L+1, so levels never share a buffer).  Returns nullptr on allocation
+// failure.
+void *scratch(size_t bytes, int level = 0);
 
 // Per-device word of error bits set by kernels whose bounded waits gave up
 // (read and cleared by tridGetDeviceErrors).  nullptr if it cannot be made.
@@ -138,8 +140,26 @@ cudaError_t launch_strided_tma(const Geom &g, const int *dims, const int *const 
 template <typename T, int INC>
 cudaError_t launch_strided_part_tma(const Geom &g, const int *dims, const int *const pads[5],
                                     int ndim, int solvedim, const T *a, const T *b, const T *c,
-                                    T *d, T *u, int chunk, int spc, unsigned *err,
-                                    cudaStream_t st);
+                                    T *d, T *u, int chunk, int spc, bool prefetch,
+                                    unsigned *err, cudaStream_t st);
+// general partitioned kernels (kern_general.cu)
+enum GenModeId { kGenFwd = 0, kGenFwdInc = 1, kGenAdj = 2 };
+enum GenPhaseId { kGenSingle = 0, kGenReduce = 1, kGenFinish = 2 };
+template <typename T>
+struct GenArgs {
+  const T *a, *b, *c;
+  const T *rhs;    // d (forward) or w = dL/dx (adjoint)
+  const T *usol;   // adjoint: the forward solution
+  T *out;          // forward: d (non-Inc) or u (Inc)
+  T *ga, *gb, *gc, *gd;  // adjoint outputs, each may be null
+  T *red;          // reduce phase: block rows, 4 arrays of nsys*2*nblk (a, b, c, d)
+  const T *bsol;   // finish phase: block unknowns, nsys*2*nblk
+  int nblk;        // blocks per system
+};
+template <typename T, int MODE>
+cudaError_t launch_general_phase(const Geom &g, const GenArgs<T> &A, int axis, int chunk, int spc,
+                                 int phase, cudaStream_t st);
+
 template <typename T, int INC>
 cudaError_t launch_generic(const Geom &g, const T *a, const T *b, const T *c, T *d, T *u,
                            T *work, int64_t work_systems, cudaStream_t st);

@@ -70,6 +70,23 @@ tridSmtsvStridedBatchPaddedInc = _padded("tridSmtsvStridedBatchPaddedInc")
 tridDmtsvStridedBatchPaddedInc = _padded("tridDmtsvStridedBatchPaddedInc")
 
 
+def _adjoint(name):
+    def f(a, b, c, u, w, da, db, dc, dd, ndim, solvedim, dims, pads):
+        L = lib()
+        _bind_stream(L)
+        return getattr(L, name)(_ptr(a), _ptr(b), _ptr(c), _ptr(u), _ptr(w), _ptr(da), _ptr(db),
+                                _ptr(dc), _ptr(dd), int(ndim), int(solvedim), int_array(dims),
+                                int_array(pads))
+    f.__name__ = name
+    f.__doc__ = (f"{name}(a, b, c, u, w, da, db, dc, dd, ndim, solvedim, dims, pads) -> status: "
+                 "gradients of a strided-batch solve (outputs may be None)")
+    return f
+
+
+tridDmtsvStridedBatchAdjoint = _adjoint("tridDmtsvStridedBatchAdjoint")
+tridSmtsvStridedBatchAdjoint = _adjoint("tridSmtsvStridedBatchAdjoint")
+
+
 def initTridMultiDimBatchSolve(ndim, dims, pads):
     lib().initTridMultiDimBatchSolve(int(ndim), int_array(dims), int_array(pads))
 
