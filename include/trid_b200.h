@@ -117,6 +117,22 @@ TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchAdjoint(const float *a, const fl
                                                         float *dc, float *dd, int ndim,
                                                         int solvedim, int *dims, int *pads);
 
+/* ---- variable-length packed batch (no reference counterpart) --------------
+ * nsys independent systems packed back to back: system s occupies rows
+ * [offsets[s], offsets[s+1]) of a, b, c, d (unit stride); offsets is a DEVICE
+ * array of nsys+1 int64 values and total = offsets[nsys] (the number of
+ * rows, passed so that the call needs no device-to-host read).  Each system's
+ * first a and last c are never read.  The solution overwrites d.  Systems of
+ * up to 8192 rows; one persistent launch (after a one-CTA prefix pass) with
+ * length-bucketed work items.  Malformed offsets and longer systems are
+ * skipped and reported by tridGetDeviceErrors (bits 4 and 8). */
+TRID_EXTERN_C tridStatus_t tridDmtsvVarlenBatch(const double *a, const double *b, const double *c,
+                                                double *d, const long long *offsets,
+                                                long long nsys, long long total);
+TRID_EXTERN_C tridStatus_t tridSmtsvVarlenBatch(const float *a, const float *b, const float *c,
+                                                float *d, const long long *offsets,
+                                                long long nsys, long long total);
+
 /* ---- replaces trid_cuda.h:44 (a no-op in the reference, trid_cuda.cu:612) ---- */
 TRID_EXTERN_C void initTridMultiDimBatchSolve(int ndim, int *dims, int *pads);
 
@@ -151,7 +167,8 @@ TRID_EXTERN_C tridStatus_t tridSetMethod(int method, int chunk, int sys_per_cta)
 
 /* Error bits recorded on the current device by kernels whose bounded waits
  * gave up (1 = a TMA/mbarrier wait timed out; 2 = a bulk-copy shared-memory
- * operand was misaligned and the copy was skipped); reading clears them.  Blocks
+ * operand was misaligned and the copy was skipped; 4 = malformed varlen
+ * offsets; 8 = a varlen system longer than supported); reading clears them.  Blocks
  * until the device is idle. */
 TRID_EXTERN_C tridStatus_t tridGetDeviceErrors(unsigned *flags);
 

@@ -46,6 +46,24 @@ def test_library_exports_every_declared_symbol(header, lib):
     assert not missing, missing
 
 
+def test_reference_block_entry_points_have_cxx_linkage():
+    """dbtsv_gpu/sbtsv_gpu keep the reference's C++ signatures
+    (block/include/blktrid_gpu.h:38-40)."""
+    for lib in (_lib.LIB_MAIN, _lib.LIB_COMPAT):
+        syms = exported(lib)
+        assert "_Z9dbtsv_gpuPdS_S_S_S_S_S_iii" in syms
+        assert "_Z9sbtsv_gpuPfS_S_S_S_S_S_iii" in syms
+
+
+def test_block_invalid_arguments_rejected():
+    import tridsolver_b200.block  # noqa: F401  (registers the signatures)
+    p, _keep = _fake()
+    L = tb.lib()
+    assert L.tridDbtsvBatch(p, p, p, p, p, 4, 2, 11, None, None) == INVALID   # M > 10
+    assert L.tridDbtsvBatch(p, p, p, p, p, 0, 2, 2, None, None) == INVALID    # N < 1
+    assert L.tridDbtsvBatch(None, p, p, p, p, 4, 2, 2, None, None) == INVALID
+
+
 def test_extension_headers_exported_by_main_library():
     syms = exported(_lib.LIB_MAIN)
     for header in sorted(os.listdir(INCLUDE)):
