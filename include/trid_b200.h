@@ -133,6 +133,36 @@ TRID_EXTERN_C tridStatus_t tridSmtsvVarlenBatch(const float *a, const float *b, 
                                                 float *d, const long long *offsets,
                                                 long long nsys, long long total);
 
+/* ---- ADI heat diffusion (the reference app apps/adi/src/adi_orig.c:147-240,
+ *      adi_cuda.cu:285-329, rebuilt around generated coefficients) ----------
+ * Grid nx*ny*nz (x fastest, each extent 1..512).  Interior points get the
+ * tridiagonal row (a, b, c) along every axis, face points the identity row;
+ * the step RHS is lambda*(sum of the 6 neighbours - 6u) on interior points, 0
+ * on faces (the reference app uses a = c = -lambda/2, b = 1 + lambda).
+ *
+ * tridXadiSteps: nsteps steps u <- u + Z^{-1} Y^{-1} X^{-1} rhs(u), three
+ *   launches per step (stencil fused into the x solve, u += in the z solve).
+ *   work holds 2*nx*ny*nz elements (NULL = library scratch; pass a buffer when
+ *   capturing the calls into a CUDA graph).
+ * tridXadiSolve: one axis solve out = T^{-1} rhs with T the generated
+ *   operator along `axis` (0, 1, 2); stencil=1 (axis 0 only) takes u in rhs
+ *   and solves for the step RHS; transpose=1 solves with T^T (adjoint);
+ *   inc=1 (axes 1, 2) adds the solution into out.
+ * tridDadiLaplacianT: out += lambda * L^T g (L the interior-masked
+ *   7-point Laplacian): the stencil's adjoint. */
+TRID_EXTERN_C tridStatus_t tridDadiSteps(double *u, double *work, int nx, int ny, int nz,
+                                         int nsteps, double lambda, double a, double b, double c);
+TRID_EXTERN_C tridStatus_t tridSadiSteps(float *u, float *work, int nx, int ny, int nz, int nsteps,
+                                         float lambda, float a, float b, float c);
+TRID_EXTERN_C tridStatus_t tridDadiSolve(const double *rhs, double *out, int nx, int ny, int nz,
+                                         int axis, int stencil, int transpose, int inc,
+                                         double lambda, double a, double b, double c);
+TRID_EXTERN_C tridStatus_t tridSadiSolve(const float *rhs, float *out, int nx, int ny, int nz,
+                                         int axis, int stencil, int transpose, int inc,
+                                         float lambda, float a, float b, float c);
+TRID_EXTERN_C tridStatus_t tridDadiLaplacianT(const double *g, double *out, int nx, int ny, int nz,
+                                              double lambda);
+
 /* ---- replaces trid_cuda.h:44 (a no-op in the reference, trid_cuda.cu:612) ---- */
 TRID_EXTERN_C void initTridMultiDimBatchSolve(int ndim, int *dims, int *pads);
 

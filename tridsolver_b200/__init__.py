@@ -35,4 +35,4 @@ from .scalar import (  # noqa: F401
     set_method,
 )
 from .autograd import TridSolve, trid_solve  # noqa: F401
-from . import block, varlen  # noqa: F401
+from . import adi, block, varlen  # noqa: F401

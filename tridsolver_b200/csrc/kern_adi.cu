@@ -1,0 +1,307 @@
+// ADI heat-diffusion kernels (sm_100a): the reference app's step
+// (apps/adi/src/adi_orig.c:147-240, preproc.hpp:172-214, adi_cuda.cu:285-329)
+// with the tridiagonal coefficients generated from the grid position instead
+// of stored (the reference writes 9 coefficient arrays per step).
+//
+// Grid nx*ny*nz, x fastest.  A point is interior when no index is on a face.
+// Interior rows: (a, b, c) = (ca, cb, cc); face rows: identity (0, 1, 0); the
+// RHS of a step is r = lambda*(sum of the 6 neighbours - 6u) on interior
+// points and 0 on faces.  One step:
+//     du1 = X^{-1} r     (adi_x_kernel: stencil fused into the x solve)
+//     du2 = Y^{-1} du1   (adi_s_kernel, axis 1)
+//     u  += Z^{-1} du2   (adi_s_kernel, axis 2, Inc)
+// Moved per step (FP64): 8 B read + 8 B write (x), 16 B (y), 24 B (z) per
+// point = 56 B, against 80 B of coefficient writes alone in the reference.
+//
+// TRANS = true solves the transposed systems (sub-diagonal c_{i-1},
+// super-diagonal a_{i+1}) for the adjoint of a step.
+#include "partition.cuh"
+
+namespace tridb200 {
+
+template <typename T>
+struct AdiArgs {
+  int nx, ny, nz;
+  T lam, ca, cb, cc;
+  const T *rhs;   // x pass with stencil: u; otherwise the right-hand side
+  T *out;         // solution (or += for Inc)
+};
+
+template <typename T>
+__device__ __forceinline__ bool adi_inside(const AdiArgs<T> &g, int i, int j, int k) {
+  return i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1;
+}
+
+// coefficients of row r of the line through (i,j,k) along `axis`
+template <typename T, bool TRANS>
+__device__ __forceinline__ void adi_row(const AdiArgs<T> &g, int axis, int i, int j, int k, T &al,
+                                        T &be, T &ga) {
+  auto at = [&](int d) {  // neighbour along the axis, inside?
+    int ii = i, jj = j, kk = k;
+    if (axis == 0) ii += d; else if (axis == 1) jj += d; else kk += d;
+    return adi_inside(g, ii, jj, kk);
+  };
+  const bool in = adi_inside(g, i, j, k);
+  be = in ? g.cb : T(1);
+  if (!TRANS) {
+    al = in ? g.ca : T(0);
+    ga = in ? g.cc : T(0);
+  } else {
+    al = at(-1) ? g.cc : T(0);  // c of the row above
+    ga = at(+1) ? g.ca : T(0);  // a of the row below
+  }
+}
+
+// ------------------------------------------------------------- x lines --
+template <typename T, int M, bool STENCIL, bool TRANS>
+__global__ void __launch_bounds__(128) adi_x_kernel(AdiArgs<T> g) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int64_t line = (int64_t)blockIdx.x * 4 + threadIdx.x / kWarp;
+  if (line >= (int64_t)g.ny * g.nz) return;
+  const int j = (int)(line % g.ny), k = (int)(line / g.ny);
+  const int64_t sxy = (int64_t)g.nx * g.ny;
+  const int64_t base = (int64_t)k * sxy + (int64_t)j * g.nx;
+  T al[M], be[M], ga[M], de[M];
+#pragma unroll
+  for (int q = 0; q < M; ++q) {
+    const int i = lane * M + q;
+    if (i < g.nx) {
+      adi_row<T, TRANS>(g, 0, i, j, k, al[q], be[q], ga[q]);
+      const int64_t p = base + i;
+      if (STENCIL) {
+        de[q] = adi_inside(g, i, j, k)
+                    ? g.lam * (g.rhs[p - 1] + g.rhs[p + 1] + g.rhs[p - g.nx] + g.rhs[p + g.nx] +
+                               g.rhs[p - sxy] + g.rhs[p + sxy] - T(6) * g.rhs[p])
+                    : T(0);
+      } else {
+        de[q] = g.rhs[p];
+      }
+    } else {
+      al[q] = T(0);
+      be[q] = T(1);
+      ga[q] = T(0);
+      de[q] = T(0);
+    }
+  }
+  Row<T> F, L;
+  chunk_reduce<T, M>(al, be, ga, de, F, L);
+  T xF, xL;
+  warp_interface_solve(F, L, xF, xL, lane);
+  chunk_backsub<T, M>(al, ga, de, xF, xL);
+#pragma unroll
+  for (int q = 0; q < M; ++q) {
+    const int i = lane * M + q;
+    if (i < g.nx) g.out[base + i] = de[q];
+  }
+}
+
+// ------------------------------------------------------- y and z lines --
+template <typename T, int M, int SB, int AXIS, bool TRANS, bool INC>
+__global__ void __launch_bounds__(SB * kWarp) adi_s_kernel(AdiArgs<T> g) {
+  __shared__ T red[8][kWarp][SB + 1];
+  __shared__ T sol[2][kWarp][SB + 1];
+  const int tid = threadIdx.x;
+  const int sl = tid % SB, t = tid / SB;
+  const int ntx = (g.nx + SB - 1) / SB;
+  const int other = (AXIS == 1) ? g.nz : g.ny;
+  const int64_t blk = blockIdx.x;
+  const int i = (int)(blk % ntx) * SB + sl;
+  const int o = (int)(blk / ntx);  // k for axis 1, j for axis 2
+  const bool valid = i < g.nx && o < other;
+  const int n = (AXIS == 1) ? g.ny : g.nz;
+  const int64_t sxy = (int64_t)g.nx * g.ny;
+  const int64_t stride = (AXIS == 1) ? g.nx : sxy;
+  const int64_t base = (AXIS == 1) ? (int64_t)o * sxy + i : (int64_t)o * g.nx + i;
+  T al[M], be[M], ga[M], de[M];
+#pragma unroll
+  for (int q = 0; q < M; ++q) {
+    const int r = t * M + q;
+    if (valid && r < n) {
+      const int jj = (AXIS == 1) ? r : o, kk = (AXIS == 1) ? o : r;
+      adi_row<T, TRANS>(g, AXIS, i, jj, kk, al[q], be[q], ga[q]);
+      de[q] = g.rhs[base + (int64_t)r * stride];
+    } else {
+      al[q] = T(0);
+      be[q] = T(1);
+      ga[q] = T(0);
+      de[q] = T(0);
+    }
+  }
+  Row<T> F, L;
+  chunk_reduce<T, M>(al, be, ga, de, F, L);
+  red[0][t][sl] = F.a;
+  red[1][t][sl] = F.b;
+  red[2][t][sl] = F.c;
+  red[3][t][sl] = F.d;
+  red[4][t][sl] = L.a;
+  red[5][t][sl] = L.b;
+  red[6][t][sl] = L.c;
+  red[7][t][sl] = L.d;
+  __syncthreads();
+  {
+    const int w = tid / kWarp, lane = tid & (kWarp - 1);
+    const Row<T> F2{red[0][lane][w], red[1][lane][w], red[2][lane][w], red[3][lane][w]};
+    const Row<T> L2{red[4][lane][w], red[5][lane][w], red[6][lane][w], red[7][lane][w]};
+    T xF, xL;
+    warp_interface_solve(F2, L2, xF, xL, lane);
+    sol[0][lane][w] = xF;
+    sol[1][lane][w] = xL;
+  }
+  __syncthreads();
+  chunk_backsub<T, M>(al, ga, de, sol[0][t][sl], sol[1][t][sl]);
+  if (!valid) return;
+#pragma unroll
+  for (int q = 0; q < M; ++q) {
+    const int r = t * M + q;
+    if (r < n) {
+      const int64_t p = base + (int64_t)r * stride;
+      if (INC)
+        g.out[p] += de[q];
+      else
+        g.out[p] = de[q];
+    }
+  }
+}
+
+// L^T applied to g, scaled and added: out += lam * L^T g, where L is the
+// interior-masked 7-point Laplacian (L u)_p = sum_nbr u - 6 u_p on interior
+// p, 0 on faces.  (L^T g)_q = sum over interior neighbours p of q of g_p,
+// minus 6 g_q if q is interior.
+template <typename T>
+__global__ void adi_lt_kernel(AdiArgs<T> g, const T *__restrict__ gin) {
+  const int64_t total = (int64_t)g.nx * g.ny * g.nz;
+  const int64_t sxy = (int64_t)g.nx * g.ny;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < total;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(p % g.nx), j = (int)((p / g.nx) % g.ny), k = (int)(p / sxy);
+    T acc = adi_inside(g, i, j, k) ? T(-6) * gin[p] : T(0);
+    if (i > 0 && adi_inside(g, i - 1, j, k)) acc += gin[p - 1];
+    if (i < g.nx - 1 && adi_inside(g, i + 1, j, k)) acc += gin[p + 1];
+    if (j > 0 && adi_inside(g, i, j - 1, k)) acc += gin[p - g.nx];
+    if (j < g.ny - 1 && adi_inside(g, i, j + 1, k)) acc += gin[p + g.nx];
+    if (k > 0 && adi_inside(g, i, j, k - 1)) acc += gin[p - sxy];
+    if (k < g.nz - 1 && adi_inside(g, i, j, k + 1)) acc += gin[p + sxy];
+    g.out[p] += g.lam * acc;
+  }
+}
+
+// ------------------------------------------------------------- launchers --
+template <typename T, int M>
+static cudaError_t adi_axis_m(const AdiArgs<T> &g, int axis, bool stencil, bool trans, bool inc,
+                              cudaStream_t st) {
+  if (axis == 0) {
+    const int64_t lines = (int64_t)g.ny * g.nz;
+    const dim3 grid((unsigned)((lines + 3) / 4)), block(128);
+    if (stencil && !trans && !inc) adi_x_kernel<T, M, true, false><<<grid, block, 0, st>>>(g);
+    else if (!stencil && !trans && !inc) adi_x_kernel<T, M, false, false><<<grid, block, 0, st>>>(g);
+    else if (!stencil && trans && !inc) adi_x_kernel<T, M, false, true><<<grid, block, 0, st>>>(g);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+  }
+  if (stencil) return cudaErrorInvalidValue;
+  constexpr int SB = 8;
+  const int ntx = (g.nx + SB - 1) / SB;
+  const int other = (axis == 1) ? g.nz : g.ny;
+  const dim3 grid((unsigned)((int64_t)ntx * other)), block(SB * kWarp);
+#define ADI_S(AX)                                                                          \
+  if (!trans && !inc) adi_s_kernel<T, M, SB, AX, false, false><<<grid, block, 0, st>>>(g); \
+  else if (!trans && inc) adi_s_kernel<T, M, SB, AX, false, true><<<grid, block, 0, st>>>(g); \
+  else if (trans && !inc) adi_s_kernel<T, M, SB, AX, true, false><<<grid, block, 0, st>>>(g); \
+  else return cudaErrorInvalidValue;
+  if (axis == 1) {
+    ADI_S(1)
+  } else {
+    ADI_S(2)
+  }
+#undef ADI_S
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t adi_axis(const AdiArgs<T> &g, int axis, bool stencil, bool trans, bool inc,
+                     cudaStream_t st) {
+  const int n = axis == 0 ? g.nx : (axis == 1 ? g.ny : g.nz);
+  if (n <= 64) return adi_axis_m<T, 2>(g, axis, stencil, trans, inc, st);
+  if (n <= 128) return adi_axis_m<T, 4>(g, axis, stencil, trans, inc, st);
+  if (n <= 256) return adi_axis_m<T, 8>(g, axis, stencil, trans, inc, st);
+  if (n <= 512) return adi_axis_m<T, 16>(g, axis, stencil, trans, inc, st);
+  return cudaErrorNotSupported;
+}
+
+template <typename T>
+cudaError_t adi_lt(const AdiArgs<T> &g, const T *gin, cudaStream_t st) {
+  const int64_t total = (int64_t)g.nx * g.ny * g.nz;
+  int64_t blocks = (total + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  adi_lt_kernel<T><<<dim3((unsigned)blocks), dim3(256), 0, st>>>(g, gin);
+  return cudaGetLastError();
+}
+
+}  // namespace tridb200
+
+using namespace tridb200;
+
+static bool adi_dims_ok(int nx, int ny, int nz) {
+  return nx >= 1 && ny >= 1 && nz >= 1 && nx <= 512 && ny <= 512 && nz <= 512;
+}
+
+template <typename T>
+static tridStatus_t adi_solve_entry(const T *rhs, T *out, int nx, int ny, int nz, int axis,
+                                    int stencil, int transpose, int inc, T lam, T ca, T cb, T cc) {
+  if (!adi_dims_ok(nx, ny, nz) || axis < 0 || axis > 2 || !rhs || !out) return TRID_STATUS_INVALID_VALUE;
+  if ((stencil && (axis != 0 || transpose || inc)) || (inc && (transpose || axis == 0)))
+    return TRID_STATUS_INVALID_VALUE;
+  AdiArgs<T> g = {nx, ny, nz, lam, ca, cb, cc, rhs, out};
+  return adi_axis<T>(g, axis, stencil != 0, transpose != 0, inc != 0, current_stream()) == cudaSuccess
+             ? TRID_STATUS_SUCCESS
+             : TRID_STATUS_EXECUTION_FAILED;
+}
+
+template <typename T>
+static tridStatus_t adi_steps_entry(T *u, T *work, int nx, int ny, int nz, int nsteps, T lam, T ca,
+                                    T cb, T cc) {
+  if (!adi_dims_ok(nx, ny, nz) || !u || nsteps < 0) return TRID_STATUS_INVALID_VALUE;
+  const size_t npts = (size_t)nx * ny * nz;
+  if (!work) {
+    work = (T *)scratch(2 * npts * sizeof(T), 0);
+    if (!work) return TRID_STATUS_ALLOC_FAILED;
+  }
+  T *w1 = work, *w2 = work + npts;
+  const cudaStream_t st = current_stream();
+  for (int s = 0; s < nsteps; ++s) {
+    AdiArgs<T> gx = {nx, ny, nz, lam, ca, cb, cc, u, w1};
+    AdiArgs<T> gy = {nx, ny, nz, lam, ca, cb, cc, w1, w2};
+    AdiArgs<T> gz = {nx, ny, nz, lam, ca, cb, cc, w2, u};
+    if (adi_axis<T>(gx, 0, true, false, false, st) != cudaSuccess ||
+        adi_axis<T>(gy, 1, false, false, false, st) != cudaSuccess ||
+        adi_axis<T>(gz, 2, false, false, true, st) != cudaSuccess)
+      return TRID_STATUS_EXECUTION_FAILED;
+  }
+  return TRID_STATUS_SUCCESS;
+}
+
+extern "C" tridStatus_t tridDadiSolve(const double *rhs, double *out, int nx, int ny, int nz,
+                                      int axis, int stencil, int transpose, int inc, double lambda,
+                                      double a, double b, double c) {
+  return adi_solve_entry<double>(rhs, out, nx, ny, nz, axis, stencil, transpose, inc, lambda, a, b, c);
+}
+extern "C" tridStatus_t tridSadiSolve(const float *rhs, float *out, int nx, int ny, int nz,
+                                      int axis, int stencil, int transpose, int inc, float lambda,
+                                      float a, float b, float c) {
+  return adi_solve_entry<float>(rhs, out, nx, ny, nz, axis, stencil, transpose, inc, lambda, a, b, c);
+}
+extern "C" tridStatus_t tridDadiSteps(double *u, double *work, int nx, int ny, int nz, int nsteps,
+                                      double lambda, double a, double b, double c) {
+  return adi_steps_entry<double>(u, work, nx, ny, nz, nsteps, lambda, a, b, c);
+}
+extern "C" tridStatus_t tridSadiSteps(float *u, float *work, int nx, int ny, int nz, int nsteps,
+                                      float lambda, float a, float b, float c) {
+  return adi_steps_entry<float>(u, work, nx, ny, nz, nsteps, lambda, a, b, c);
+}
+extern "C" tridStatus_t tridDadiLaplacianT(const double *g, double *out, int nx, int ny, int nz,
+                                           double lambda) {
+  if (!adi_dims_ok(nx, ny, nz) || !g || !out) return TRID_STATUS_INVALID_VALUE;
+  AdiArgs<double> a = {nx, ny, nz, lambda, 0.0, 1.0, 0.0, nullptr, out};
+  return adi_lt<double>(a, g, current_stream()) == cudaSuccess ? TRID_STATUS_SUCCESS
+                                                               : TRID_STATUS_EXECUTION_FAILED;
+}
