@@ -133,6 +133,32 @@ TRID_EXTERN_C tridStatus_t tridSmtsvVarlenBatch(const float *a, const float *b, 
                                                 float *d, const long long *offsets,
                                                 long long nsys, long long total);
 
+/* Allocation-free FP64 variant of tridDmtsvVarlenBatch; it has no
+ * counterpart in the reference.  For callers that cannot allocate device
+ * memory -- code running under another component's allocator or memory budget
+ * (a driver allocation would take memory the pool reserved, or fail) and
+ * latency-critical loops that cannot absorb the device synchronisation of
+ * cudaMalloc/cudaFree.  Same arguments and result as tridDmtsvVarlenBatch,
+ * but every scratch byte comes from one fixed 32 MiB array per device that
+ * the library holds from load to process exit; no call allocates.
+ * Limit: the work space must fit in 32 MiB, roughly
+ *   12*(nsys+1) + 64*(nsys + total/256 + 1) bytes plus alignment
+ * (e.g. 100,000 systems with up to 100 million rows in total); larger
+ * problems return TRID_STATUS_INVALID_VALUE and should use
+ * tridDmtsvVarlenBatch.
+ * The first call on each device looks up the array's device address (a
+ * runtime symbol query, no allocation) with that device current; make that
+ * first call before any stream capture.  Every call uses the same array and
+ * leaves its contents behind (the next call clears what must start at zero),
+ * so calls that overlap on the GPU -- concurrent streams or threads on one
+ * device -- race and must be serialised by the caller.  Malformed offsets
+ * and over-long systems are skipped as in tridDmtsvVarlenBatch but are not
+ * reported through tridGetDeviceErrors. */
+TRID_EXTERN_C tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const double *b,
+                                                       const double *c, double *d,
+                                                       const long long *offsets, long long nsys,
+                                                       long long total);
+
 /* ---- ADI heat diffusion (the reference app apps/adi/src/adi_orig.c:147-240,
  *      adi_cuda.cu:285-329, rebuilt around generated coefficients) ----------
  * Grid nx*ny*nz (x fastest, each extent 1..512).  Interior points get the

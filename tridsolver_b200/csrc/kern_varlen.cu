@@ -19,6 +19,8 @@
 // the queue and the per-system counters.  Malformed offsets (decreasing or
 // past `total`) and systems longer than 8192 rows are skipped and recorded in
 // the device error word (bits 4 and 8).
+#include <mutex>
+
 #include "partition.cuh"
 
 namespace tridb200 {
@@ -285,4 +287,108 @@ extern "C" tridStatus_t tridSmtsvVarlenBatch(const float *a, const float *b, con
                                              float *d, const long long *offsets, long long nsys,
                                              long long total) {
   return varlen_entry<float>(a, b, c, d, (const int64_t *)offsets, nsys, total);
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the variable-length solve.
+//
+// Some callers cannot allocate device memory: code that runs under another
+// component's allocator or memory budget, where a driver allocation would
+// steal memory the pool has reserved (or fail), and latency-critical loops
+// where the implicit device synchronisation of cudaMalloc/cudaFree is not
+// acceptable.  tridDmtsvVarlenBatchNoAlloc serves them: its work space (the
+// item prefix sums, per-system counters, work queue, block rows and an error
+// word) lives in the fixed array below, which every GPU that loads this
+// library holds until the process exits.  Nothing is allocated per call.
+// ---------------------------------------------------------------------------
+namespace tridb200 {
+
+constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;  // 32 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[64];  // device address of g_noalloc_scratch, per device
+
+// Device address of the static array on the current device.  The host-side
+// name g_noalloc_scratch is only a stand-in, never a device address, so the
+// address is looked up once per device (with that device current) and cached.
+static void *noalloc_scratch_address() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  return g_noalloc_ptr[dev];
+}
+
+// Bytes of work space a solve of nsys systems / total rows needs (0 when it
+// does not fit in the static array).
+static size_t noalloc_layout(int64_t nsys, int64_t total, size_t off[5]) {
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const int64_t max_items = nsys + total / kVLBlock + 1;
+  size_t at = 0;
+  off[0] = at;  // error word
+  at += 256;
+  off[1] = at;  // item_off, nsys+1 int64
+  at += al(sizeof(int64_t) * (size_t)(nsys + 1));
+  off[2] = at;  // sys_count, nsys+1 unsigned
+  at += al(sizeof(unsigned) * (size_t)(nsys + 1));
+  off[3] = at;  // queue
+  at += 256;
+  off[4] = at;  // block rows, 8 per item
+  at += al(sizeof(double) * 8 * (size_t)max_items);
+  return at <= kNoAllocScratchBytes ? at : 0;
+}
+
+}  // namespace tridb200
+
+extern "C" tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const double *b,
+                                                    const double *c, double *d,
+                                                    const long long *offsets, long long nsys,
+                                                    long long total) {
+  using namespace tridb200;
+  if (nsys < 0 || total < 0 || !offsets || (total > 0 && (!a || !b || !c || !d)))
+    return TRID_STATUS_INVALID_VALUE;
+  if (nsys == 0 || total == 0) return TRID_STATUS_SUCCESS;
+  if (nsys > ((int64_t)1 << 40) || total > ((int64_t)1 << 46)) return TRID_STATUS_INVALID_VALUE;
+  size_t off[5];
+  if (noalloc_layout(nsys, total, off) == 0) return TRID_STATUS_INVALID_VALUE;  // too large
+  unsigned char *w = (unsigned char *)noalloc_scratch_address();
+  if (!w) return TRID_STATUS_EXECUTION_FAILED;
+  const cudaStream_t st = current_stream();
+  VLArgs<double> A;
+  A.a = a;
+  A.b = b;
+  A.c = c;
+  A.d = d;
+  A.offsets = (const int64_t *)offsets;
+  A.nsys = nsys;
+  A.total = total;
+  A.err = (unsigned *)(w + off[0]);
+  A.item_off = (int64_t *)(w + off[1]);
+  A.sys_count = (unsigned *)(w + off[2]);
+  A.queue = (unsigned long long *)(w + off[3]);
+  A.rows = (double *)(w + off[4]);
+  // varlen_prep rewrites the prefix sums and clears the queue and counters,
+  // so whatever the previous call left in the array does not matter
+  varlen_prep<<<1, 1024, 0, st>>>(A.offsets, nsys, total, (int64_t *)A.item_off, A.sys_count,
+                                   A.queue);
+  if (cudaGetLastError() != cudaSuccess) return TRID_STATUS_EXECUTION_FAILED;
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, varlen_kernel<double>, 256, 0) !=
+          cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  varlen_kernel<double><<<dim3((unsigned)(sms * per_sm)), dim3(256), 0, st>>>(A);
+  return cudaGetLastError() == cudaSuccess ? TRID_STATUS_SUCCESS : TRID_STATUS_EXECUTION_FAILED;
 }

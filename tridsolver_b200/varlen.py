@@ -16,6 +16,7 @@ c_ll = ctypes.c_longlong
 register({
     "tridDmtsvVarlenBatch": (c_int, [vp, vp, vp, vp, vp, c_ll, c_ll]),
     "tridSmtsvVarlenBatch": (c_int, [vp, vp, vp, vp, vp, c_ll, c_ll]),
+    "tridDmtsvVarlenBatchNoAlloc": (c_int, [vp, vp, vp, vp, vp, c_ll, c_ll]),
 })
 
 
