@@ -117,6 +117,24 @@ TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchAdjoint(const float *a, const fl
                                                         float *dc, float *dd, int ndim,
                                                         int solvedim, int *dims, int *pads);
 
+/* ---- forward solve + adjoint in one call (no reference counterpart) -------
+ * x = A^{-1} d and, for the cotangent w = dL/dx, the gradients of the
+ * adjoint above at that x (dd = A^{-T} w, da, db, dc), in one call.  For
+ * solvedim 0 and n <= 4096 one kernel does both (every input read once);
+ * otherwise the forward solve and the adjoint run one after the other.  x
+ * may alias d and dd may alias w; no other output may alias an input. */
+TRID_EXTERN_C tridStatus_t tridDmtsvStridedBatchFwdAdj(const double *a, const double *b,
+                                                       const double *c, const double *d,
+                                                       const double *w, double *x, double *da,
+                                                       double *db, double *dc, double *dd,
+                                                       int ndim, int solvedim, int *dims,
+                                                       int *pads);
+TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchFwdAdj(const float *a, const float *b,
+                                                       const float *c, const float *d,
+                                                       const float *w, float *x, float *da,
+                                                       float *db, float *dc, float *dd, int ndim,
+                                                       int solvedim, int *dims, int *pads);
+
 /* ---- variable-length packed batch (no reference counterpart) --------------
  * nsys independent systems packed back to back: system s occupies rows
  * [offsets[s], offsets[s+1]) of a, b, c, d (unit stride); offsets is a DEVICE

@@ -25,6 +25,9 @@ from .scalar import (  # noqa: F401
     tridDmtsvStridedBatch,
     tridDmtsvStridedBatchAdjoint,
     tridSmtsvStridedBatchAdjoint,
+    tridDmtsvStridedBatchFwdAdj,
+    tridSmtsvStridedBatchFwdAdj,
+    solve_fwd_adj,
     tridDmtsvStridedBatchInc,
     tridDmtsvStridedBatchPadded,
     tridDmtsvStridedBatchPaddedInc,

@@ -281,6 +281,12 @@ static tridStatus_t solve_level(const T *a, const T *b, const T *c, T *d, T *u, 
   }
   if (e != cudaErrorNotSupported) {
     // done (or failed) by the method-4 kernel
+  } else if (m.method >= 2 && !fits && axis == 0 && g.n <= 4096 &&
+             (e = launch_xcta<T, INC ? kXcFwdInc : kXcFwd>(
+                  g, XArgs<T>{a, b, c, d, nullptr, nullptr, INC ? u : d, nullptr, nullptr, nullptr,
+                              nullptr},
+                  stream)) != cudaErrorNotSupported) {
+    // one CTA per system: done (or failed) above
   } else if (m.method >= 2 && !fits) {
     GenArgs<T> A = {};
     A.a = a;
@@ -350,6 +356,12 @@ tridStatus_t solve_adjoint(const T *a, const T *b, const T *c, const T *u, const
   MethodChoice m = choose_method((int)sizeof(T), axis, g.n, 0);
   if (m.chunk == 0) m.chunk = 8;
   if (m.spc == 0) m.spc = 8;
+  if (axis == 0 && g.n <= 4096) {
+    const cudaError_t e = launch_xcta<T, kXcAdj>(
+        g, XArgs<T>{a, b, c, nullptr, w, u, nullptr, ga, gb, gc, gd}, stream);
+    if (e != cudaErrorNotSupported)
+      return e == cudaSuccess ? TRID_STATUS_SUCCESS : TRID_STATUS_EXECUTION_FAILED;
+  }
   GenArgs<T> A = {};
   A.a = a;
   A.b = b;
@@ -362,6 +374,54 @@ tridStatus_t solve_adjoint(const T *a, const T *b, const T *c, const T *u, const
   A.gd = gd;
   return run_general<T, kGenAdj>(g, A, axis, m.chunk, m.spc, 0, stream);
 }
+// Forward solve and adjoint of the linear loss <w, x> in one pass where a
+// one-CTA-per-system kernel applies (axis 0, n <= 4096); otherwise the
+// forward solve followed by the adjoint.
+template <typename T>
+tridStatus_t solve_fwd_adj(const T *a, const T *b, const T *c, const T *d, const T *w, T *x,
+                           T *ga, T *gb, T *gc, T *gd, int ndim, int solvedim, const int *dims,
+                           const int *pads) {
+  const int *p[5] = {pads, pads, pads, pads, pads};
+  Geom g;
+  const tridStatus_t st = make_geom(ndim, solvedim, dims, p, true, g);
+  if (st != TRID_STATUS_SUCCESS) return st;
+  if (!aligned_ptr(a) || !aligned_ptr(b) || !aligned_ptr(c) || !aligned_ptr(d) ||
+      !aligned_ptr(w) || !aligned_ptr((const T *)x))
+    return TRID_STATUS_INVALID_VALUE;
+  for (const T *o : {(const T *)ga, (const T *)gb, (const T *)gc, (const T *)gd})
+    if (o && ((uintptr_t)o % sizeof(T)) != 0) return TRID_STATUS_INVALID_VALUE;
+  if (g.n == 0 || g.nsys == 0) return TRID_STATUS_SUCCESS;
+  const cudaStream_t stream = current_stream();
+  if (solvedim == 0 && g.n <= 4096) {
+    const cudaError_t e = launch_xcta<T, kXcFused>(
+        g, XArgs<T>{a, b, c, d, w, nullptr, x, ga, gb, gc, gd}, stream);
+    if (e != cudaErrorNotSupported)
+      return e == cudaSuccess ? TRID_STATUS_SUCCESS : TRID_STATUS_EXECUTION_FAILED;
+  }
+  // two passes: x = A^{-1} d (blocked partition, d left intact), then the
+  // adjoint at x
+  const int axis = axis_class(g, solvedim, (int)sizeof(T));
+  MethodChoice m = choose_method((int)sizeof(T), axis, g.n, 0);
+  if (m.chunk == 0) m.chunk = 8;
+  if (m.spc == 0) m.spc = 8;
+  GenArgs<T> A = {};
+  A.a = a;
+  A.b = b;
+  A.c = c;
+  A.rhs = d;
+  A.out = x;
+  const tridStatus_t s1 = run_general<T, kGenFwd>(g, A, axis, m.chunk, m.spc, 0, stream);
+  if (s1 != TRID_STATUS_SUCCESS) return s1;
+  return solve_adjoint<T>(a, b, c, x, w, ga, gb, gc, gd, ndim, solvedim, dims, pads);
+}
+template tridStatus_t solve_fwd_adj<float>(const float *, const float *, const float *,
+                                           const float *, const float *, float *, float *, float *,
+                                           float *, float *, int, int, const int *, const int *);
+template tridStatus_t solve_fwd_adj<double>(const double *, const double *, const double *,
+                                            const double *, const double *, double *, double *,
+                                            double *, double *, double *, int, int, const int *,
+                                            const int *);
+
 template tridStatus_t solve_adjoint<float>(const float *, const float *, const float *,
                                            const float *, const float *, float *, float *,
                                            float *, float *, int, int, const int *, const int *);
@@ -447,6 +507,22 @@ extern "C" tridStatus_t tridSmtsvStridedBatchAdjoint(const float *a, const float
                                                      float *dc, float *dd, int ndim, int solvedim,
                                                      int *dims, int *pads) {
   return solve_adjoint<float>(a, b, c, u, w, da, db, dc, dd, ndim, solvedim, dims, pads);
+}
+
+extern "C" tridStatus_t tridDmtsvStridedBatchFwdAdj(const double *a, const double *b,
+                                                    const double *c, const double *d,
+                                                    const double *w, double *x, double *da,
+                                                    double *db, double *dc, double *dd, int ndim,
+                                                    int solvedim, int *dims, int *pads) {
+  return solve_fwd_adj<double>(a, b, c, d, w, x, da, db, dc, dd, ndim, solvedim, dims, pads);
+}
+
+extern "C" tridStatus_t tridSmtsvStridedBatchFwdAdj(const float *a, const float *b,
+                                                    const float *c, const float *d,
+                                                    const float *w, float *x, float *da,
+                                                    float *db, float *dc, float *dd, int ndim,
+                                                    int solvedim, int *dims, int *pads) {
+  return solve_fwd_adj<float>(a, b, c, d, w, x, da, db, dc, dd, ndim, solvedim, dims, pads);
 }
 
 extern "C" void initTridMultiDimBatchSolve(int ndim, int *dims, int *pads) {

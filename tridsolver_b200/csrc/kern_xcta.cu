@@ -1,0 +1,305 @@
+// Axis-0 systems of one CTA (sm_100a): the blocked partition of
+// kern_general.cu kept inside one CTA, so systems of 513..4096 rows are solved
+// in one launch without re-reading anything.
+//
+// CTA = one system, W warps; warp w owns block w (32 chunks of M rows).
+// Every warp reduces its chunks (chunk_reduce) and its block
+// (warp_block_basis + block_rows); the 2W block rows meet in shared memory,
+// warp 0 solves the block system (one warp interface solve, lane = block),
+// and every warp finishes its block from its two boundary unknowns.
+//
+// Modes:
+//   kXFwd / kXFwdInc : x = A^{-1} d into d / added into u;
+//   kXAdj            : the adjoint for a given solution u and cotangent w
+//                      (transposed system solved in place, gradients formed
+//                      in the same pass);
+//   kXFused          : forward and adjoint of the linear loss <w, x> in one
+//                      pass: reads a, b, c, d, w once and writes x, da, db,
+//                      dc, dd (10 values per unknown instead of 5 + 9).
+#include "partition.cuh"
+
+namespace tridb200 {
+
+// XArgs (trid_internal.cuh): d = forward RHS (unused by kXAdj); w = adjoint
+// cotangent (kXAdj, kXFused); usol = forward solution (kXAdj); x = solution
+// (kXFwd, kXFused) or u (+=, kXFwdInc); ga..gd = gradients, each may be null.
+constexpr int kXFwd = kXcFwd, kXFwdInc = kXcFwdInc, kXAdj = kXcAdj, kXFused = kXcFused;
+
+// Solve the system held in (al, be, ga, de) across the CTA; the solution
+// overwrites de.  Whole CTA must call it (barriers inside).
+template <typename T, int M>
+__device__ __forceinline__ void cta_solve(T (&al)[M], const T (&be)[M], T (&ga)[M], T (&de)[M],
+                                          int w, int lane, int nw, T *sm) {
+  Row<T> F, L;
+  chunk_reduce<T, M>(al, be, ga, de, F, L);
+  T bF[3], bL[3];
+  warp_block_basis(F, L, lane, bF, bL);
+  Row<T> FB, LB;
+  block_rows(F, L, bF, bL, lane, FB, LB);
+  // sm layout: [0, 8*16) block rows, [128, 128 + 2*16) block unknowns
+  if (lane == 0) {
+    T *q = sm + 8 * w;
+    q[0] = FB.a; q[1] = FB.b; q[2] = FB.c; q[3] = FB.d;
+    q[4] = LB.a; q[5] = LB.b; q[6] = LB.c; q[7] = LB.d;
+  }
+  __syncthreads();
+  if (w == 0) {
+    Row<T> RF{T(0), T(1), T(0), T(0)}, RL{T(0), T(1), T(0), T(0)};
+    if (lane < nw) {
+      const T *q = sm + 8 * lane;
+      RF = {q[0], q[1], q[2], q[3]};
+      RL = {q[4], q[5], q[6], q[7]};
+    }
+    T f, l;
+    warp_interface_solve(RF, RL, f, l, lane);
+    if (lane < nw) {
+      sm[128 + 2 * lane] = f;
+      sm[128 + 2 * lane + 1] = l;
+    }
+  }
+  __syncthreads();
+  const T f = sm[128 + 2 * w], l = sm[128 + 2 * w + 1];
+  const T xF = bF[0] + f * bF[1] + l * bF[2];
+  const T xL = bL[0] + f * bL[1] + l * bL[2];
+  chunk_backsub<T, M>(al, ga, de, xF, xL);
+  __syncthreads();  // sm is reused by the caller's next solve
+}
+
+// Staging: every array of the system is copied into shared memory with
+// coalesced 4/8-byte cp.async (row r of a warp's 32*M rows at q + q/M, one
+// pad element per M rows, so that the transposed reads -- lane L takes rows
+// L*M .. L*M+M-1 -- hit 32 distinct banks), and results leave the same way:
+// written transposed into the warp's region, stored coalesced.
+template <int M>
+__device__ __forceinline__ int pidx(int q) {
+  return q + q / M;
+}
+
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int sz = valid ? (int)sizeof(T) : 0;  // 0: zero-fill, nothing read
+  if (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(sz)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(sz)
+                 : "memory");
+}
+
+template <typename T, int M>
+struct Stage {
+  T *base;  // dynamic shared memory
+  int nw;   // warps of the CTA
+  static constexpr int R = 32 * (M + 1);  // elements per warp region
+  __device__ T *region(int k, int w) const { return base + ((size_t)k * nw + w) * R; }
+  // element of system row r in staged array k (any warp's region)
+  __device__ T &row(int k, int r) const {
+    const int wr = r / (32 * M);
+    return region(k, wr)[pidx<M>(r - wr * 32 * M)];
+  }
+};
+
+template <typename T, int M>
+__device__ __forceinline__ void stage_in(const Stage<T, M> &S, int k, int w, int lane, const T *p,
+                                         int n) {
+  T *reg = S.region(k, w);
+  const int wb = w * 32 * M;
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int q = j * kWarp + lane;
+    const bool in = wb + q < n;
+    cp_async_elem(reg + pidx<M>(q), in ? p + wb + q : p, in);
+  }
+}
+
+// v (rows lane*M + j of warp w) -> region k -> coalesced store to p (ADD: +=)
+template <typename T, int M, bool ADD>
+__device__ __forceinline__ void stage_out(const Stage<T, M> &S, int k, int w, int lane,
+                                          const T (&v)[M], T *p, int n) {
+  T *reg = S.region(k, w);
+#pragma unroll
+  for (int j = 0; j < M; ++j) reg[lane * (M + 1) + j] = v[j];
+  __syncwarp();
+  const int wb = w * 32 * M;
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int q = j * kWarp + lane;
+    if (wb + q < n) {
+      if (ADD)
+        p[wb + q] += reg[pidx<M>(q)];
+      else
+        p[wb + q] = reg[pidx<M>(q)];
+    }
+  }
+}
+
+template <typename T, int M, int MODE>
+__global__ void __launch_bounds__(512) xcta_kernel(Geom g, XArgs<T> A) {
+  extern __shared__ __align__(16) unsigned char xcta_dyn[];
+  __shared__ T sm[128 + 32 + 2 * 16];
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int w = threadIdx.x / kWarp;
+  const int nw = blockDim.x / kWarp;
+  const int64_t sys = blockIdx.x;
+  int64_t off[5];
+  system_offsets(g, sys, off);
+  const int n = g.n;
+  const int r0 = w * kWarp * M + lane * M;
+  const Stage<T, M> S{reinterpret_cast<T *>(xcta_dyn), nw};
+  // staged arrays: 0 a, 1 b, 2 c, 3 d (forward modes) or the solution
+  // (kXAdj), 4 w (kXAdj, kXFused)
+  constexpr bool kHasW = (MODE == kXAdj || MODE == kXFused);
+  stage_in<T, M>(S, 0, w, lane, A.a + off[kA], n);
+  stage_in<T, M>(S, 1, w, lane, A.b + off[kB], n);
+  stage_in<T, M>(S, 2, w, lane, A.c + off[kC], n);
+  if (MODE == kXAdj)
+    stage_in<T, M>(S, 3, w, lane, A.usol + off[kU], n);
+  else
+    stage_in<T, M>(S, 3, w, lane, A.d + off[kD], n);
+  if (kHasW) stage_in<T, M>(S, 4, w, lane, A.w + off[kD], n);
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();  // neighbouring rows are read across warp regions
+
+  const T *ra = S.region(0, w) + lane * (M + 1);
+  const T *rb = S.region(1, w) + lane * (M + 1);
+  const T *rc = S.region(2, w) + lane * (M + 1);
+  const T *rd = S.region(3, w) + lane * (M + 1);
+
+  T gsol[M];  // adjoint solution (kXAdj / kXFused), reloaded for the gradients
+  if (kHasW) {
+    // transposed rows: sub-diagonal c_{r-1}, super-diagonal a_{r+1}
+    const T *rw = S.region(4, w) + lane * (M + 1);
+    T ta[M], be[M], tg[M], tw[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int r = r0 + j;
+      const bool in = r < n;
+      ta[j] = (in && r > 0) ? (j > 0 ? rc[j - 1] : S.row(2, r - 1)) : T(0);
+      tg[j] = (r + 1 < n) ? (j < M - 1 ? ra[j + 1] : S.row(0, r + 1)) : T(0);
+      be[j] = in ? rb[j] : T(1);
+      tw[j] = rw[j];  // zero-filled past n
+    }
+    cta_solve<T, M>(ta, be, tg, tw, w, lane, nw, sm);
+    // parked in this thread's own slots of region 4 (read only by this
+    // thread above) for the forward solve's registers
+    T *pw = S.region(4, w) + lane * (M + 1);
+#pragma unroll
+    for (int j = 0; j < M; ++j) pw[j] = tw[j];
+  }
+
+  // the forward solution: solved here, or the staged one (kXAdj)
+  T xs[M];
+  if (MODE == kXAdj) {
+#pragma unroll
+    for (int j = 0; j < M; ++j) xs[j] = rd[j];
+  } else {
+    T al[M], be[M], ga[M], de[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int r = r0 + j;
+      const bool in = r < n;
+      al[j] = (in && r > 0) ? ra[j] : T(0);
+      be[j] = in ? rb[j] : T(1);
+      ga[j] = (r < n - 1) ? rc[j] : T(0);
+      de[j] = rd[j];  // zero-filled past n
+    }
+    cta_solve<T, M>(al, be, ga, de, w, lane, nw, sm);
+#pragma unroll
+    for (int j = 0; j < M; ++j) xs[j] = de[j];
+  }
+
+  if (MODE == kXFwd) {
+    stage_out<T, M, false>(S, 3, w, lane, xs, A.x + off[kD], n);
+    return;
+  }
+  if (MODE == kXFwdInc) {
+    stage_out<T, M, true>(S, 3, w, lane, xs, A.x + off[kU], n);
+    return;
+  }
+  // gradients: x_{r-1} and x_{r+1} from the staged solution (region 3)
+  if (MODE == kXFused) {
+    T *rx = S.region(3, w) + lane * (M + 1);
+#pragma unroll
+    for (int j = 0; j < M; ++j) rx[j] = xs[j];
+  }
+  __syncthreads();
+  {
+    const T *pw = S.region(4, w) + lane * (M + 1);
+#pragma unroll
+    for (int j = 0; j < M; ++j) gsol[j] = pw[j];
+  }
+  const T xprev = (r0 > 0 && r0 - 1 < n) ? S.row(3, r0 - 1) : T(0);
+  const T xnext = (r0 + M < n) ? S.row(3, r0 + M) : T(0);
+  T v[M];
+  if (A.ga) {
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const T xm = (j > 0) ? xs[j - 1] : xprev;
+      v[j] = (r0 + j > 0) ? -gsol[j] * xm : T(0);
+    }
+    stage_out<T, M, false>(S, 0, w, lane, v, A.ga + off[kA], n);
+  }
+  if (A.gb) {
+#pragma unroll
+    for (int j = 0; j < M; ++j) v[j] = -gsol[j] * xs[j];
+    stage_out<T, M, false>(S, 1, w, lane, v, A.gb + off[kB], n);
+  }
+  if (A.gc) {
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const T xp = (j < M - 1) ? xs[j + 1] : xnext;
+      v[j] = (r0 + j + 1 < n) ? -gsol[j] * xp : T(0);
+    }
+    stage_out<T, M, false>(S, 2, w, lane, v, A.gc + off[kC], n);
+  }
+  if (A.gd) stage_out<T, M, false>(S, 4, w, lane, gsol, A.gd + off[kD], n);
+  if (MODE == kXFused) {
+    // x is already in region 3 in the transposed order
+    __syncwarp();
+    const T *reg = S.region(3, w);
+    const int wb = w * 32 * M;
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int q = j * kWarp + lane;
+      if (wb + q < n) A.x[off[kD] + wb + q] = reg[pidx<M>(q)];
+    }
+  }
+}
+
+template <typename T, int M, int MODE>
+static cudaError_t launch_xcta_m(const Geom &g, const XArgs<T> &A, int warps, cudaStream_t st) {
+  constexpr int kArrays = (MODE == kXAdj || MODE == kXFused) ? 5 : 4;
+  const size_t smem = (size_t)kArrays * warps * Stage<T, M>::R * sizeof(T);
+  static bool attr_set = false;  // per instantiation; the attribute is per device function
+  if (!attr_set) {
+    const cudaError_t e = cudaFuncSetAttribute(xcta_kernel<T, M, MODE>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               kArrays * 16 * Stage<T, M>::R * (int)sizeof(T));
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  xcta_kernel<T, M, MODE><<<(unsigned)g.nsys, warps * kWarp, smem, st>>>(g, A);
+  return cudaGetLastError();
+}
+
+template <typename T, int MODE>
+cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, cudaStream_t st) {
+  // M = 4 up to 2048 rows (8..16 warps), M = 8 up to 4096
+  const int n = g.n;
+  if (n > 4096 || g.nsys > 0x7fffffff) return cudaErrorNotSupported;
+  const int M = (n <= 2048) ? 4 : 8;
+  const int warps = (n + 32 * M - 1) / (32 * M);
+  return M == 4 ? launch_xcta_m<T, 4, MODE>(g, A, warps, st)
+                : launch_xcta_m<T, 8, MODE>(g, A, warps, st);
+}
+
+#define TRID_XCTA_INSTANTIATE(T)                                                               \
+  template cudaError_t launch_xcta<T, kXFwd>(const Geom &, const XArgs<T> &, cudaStream_t);    \
+  template cudaError_t launch_xcta<T, kXFwdInc>(const Geom &, const XArgs<T> &, cudaStream_t); \
+  template cudaError_t launch_xcta<T, kXAdj>(const Geom &, const XArgs<T> &, cudaStream_t);    \
+  template cudaError_t launch_xcta<T, kXFused>(const Geom &, const XArgs<T> &, cudaStream_t);
+TRID_XCTA_INSTANTIATE(float)
+TRID_XCTA_INSTANTIATE(double)
+
+}  // namespace tridb200

@@ -160,6 +160,19 @@ template <typename T, int MODE>
 cudaError_t launch_general_phase(const Geom &g, const GenArgs<T> &A, int axis, int chunk, int spc,
                                  int phase, cudaStream_t st);
 
+// one-CTA-per-system blocked partition on axis 0 (kern_xcta.cu)
+enum XModeIdPub { kXcFwd = 0, kXcFwdInc = 1, kXcAdj = 2, kXcFused = 3 };
+template <typename T>
+struct XArgs {
+  const T *a, *b, *c, *d;
+  const T *w;
+  const T *usol;
+  T *x;
+  T *ga, *gb, *gc, *gd;
+};
+template <typename T, int MODE>
+cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, cudaStream_t st);
+
 template <typename T, int INC>
 cudaError_t launch_generic(const Geom &g, const T *a, const T *b, const T *c, T *d, T *u,
                            T *work, int64_t work_systems, cudaStream_t st);

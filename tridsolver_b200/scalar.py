@@ -87,6 +87,49 @@ tridDmtsvStridedBatchAdjoint = _adjoint("tridDmtsvStridedBatchAdjoint")
 tridSmtsvStridedBatchAdjoint = _adjoint("tridSmtsvStridedBatchAdjoint")
 
 
+def _fwdadj(name):
+    def f(a, b, c, d, w, x, da, db, dc, dd, ndim, solvedim, dims, pads):
+        L = lib()
+        _bind_stream(L)
+        return getattr(L, name)(_ptr(a), _ptr(b), _ptr(c), _ptr(d), _ptr(w), _ptr(x), _ptr(da),
+                                _ptr(db), _ptr(dc), _ptr(dd), int(ndim), int(solvedim),
+                                int_array(dims), int_array(pads))
+    f.__name__ = name
+    f.__doc__ = (f"{name}(a, b, c, d, w, x, da, db, dc, dd, ndim, solvedim, dims, pads) -> "
+                 "status: x = A^{-1} d and the gradients of <w, x> in one call")
+    return f
+
+
+tridDmtsvStridedBatchFwdAdj = _fwdadj("tridDmtsvStridedBatchFwdAdj")
+tridSmtsvStridedBatchFwdAdj = _fwdadj("tridSmtsvStridedBatchFwdAdj")
+
+
+def solve_fwd_adj(a, b, c, d, w, dim=-1):
+    """x = A^{-1} d along torch dimension ``dim`` and the gradients of the
+    linear loss sum(w * x) with respect to a, b, c, d, from one call (one
+    kernel for the unit-stride axis up to 4096 rows).  Returns
+    (x, (da, db, dc, dd)); the inputs are left unchanged."""
+    shape = tuple(d.shape)
+    for t in (a, b, c, d, w):
+        if tuple(t.shape) != shape or t.dtype != d.dtype or not t.is_contiguous():
+            raise ValueError("a, b, c, d, w must be contiguous tensors of one shape/dtype")
+    ndim = len(shape)
+    dim = dim % ndim
+    dims = list(reversed(shape))
+    if d.dtype == torch.float64:
+        fn = tridDmtsvStridedBatchFwdAdj
+    elif d.dtype == torch.float32:
+        fn = tridSmtsvStridedBatchFwdAdj
+    else:
+        raise TypeError("float32 or float64 only")
+    x = torch.empty_like(d)
+    grads = [torch.empty_like(d) for _ in range(4)]
+    st = fn(a, b, c, d, w, x, *grads, ndim, ndim - 1 - dim, dims, dims)
+    if st != 0:
+        raise TridError(st, fn.__name__)
+    return x, tuple(grads)
+
+
 def initTridMultiDimBatchSolve(ndim, dims, pads):
     lib().initTridMultiDimBatchSolve(int(ndim), int_array(dims), int_array(pads))
 
