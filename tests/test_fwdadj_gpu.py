@@ -59,6 +59,14 @@ def test_fused_one_kernel(n, dtype):
     run_fused(dtype, [n, 7], 0, seed=n)
 
 
+@pytest.mark.parametrize("method", [(5, 0), (6, 4), (6, 8), (6, 16)])
+@pytest.mark.parametrize("n", [65, 66, 100, 257, 511, 1000, 1024, 1025, 2500, 4096])
+def test_fused_forced_kernel(method, n):
+    tb.set_method(*method)
+    run_fused(np.float64, [n, 5], 0, seed=n + method[1])
+    run_fused(np.float32, [n, 3], 0, seed=n + method[1] + 1)
+
+
 @pytest.mark.parametrize("n", [1, 2, 31, 256, 512])
 def test_fused_short(n):
     run_fused(np.float64, [n, 11], 0, seed=n)
@@ -125,3 +133,21 @@ def test_one_kernel_adjoint(n):
     from test_adjoint_gpu import run_adjoint
     run_adjoint(np.float64, [n, 6], 0, seed=n + 2)
     run_adjoint(np.float32, [n, 6], 0, seed=n + 3)
+
+
+@pytest.mark.parametrize("method", [5, 6])
+@pytest.mark.parametrize("n", [65, 97, 300, 1024, 1031, 3000, 5000, 7000])
+@pytest.mark.parametrize("inc", [False, True])
+def test_forced_kernel_forward(method, n, inc):
+    """Methods 5/6 forced: where their limits exclude the system (6 past
+    4096 rows) the call still returns the solution through another kernel."""
+    from test_scalar_gpu import run_case
+    run_case(np.random.default_rng(n + method), np.float64, [n, 4], 0, inc=inc,
+             method=(method, 0, 0))
+
+
+@pytest.mark.parametrize("method", [(5, 0), (6, 4), (6, 16)])
+@pytest.mark.parametrize("n", [65, 300, 1024, 1031, 5000])
+def test_forced_kernel_adjoint(method, n):
+    from test_adjoint_gpu import run_adjoint
+    run_adjoint(np.float64, [n, 4], 0, seed=n + method[1], method=(*method, 0))

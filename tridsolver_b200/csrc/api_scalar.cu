@@ -92,7 +92,7 @@ static tridStatus_t parse_tuning_table(const char *path, std::vector<TuneEntry> 
       return TRID_STATUS_INVALID_VALUE;
     }
     e.dtype_bytes = (strcmp(dt, "f64") == 0) ? 8 : (strcmp(dt, "f32") == 0 ? 4 : 0);
-    if (e.dtype_bytes == 0 || e.method < 1 || e.method > 4 || e.axis < 0 || e.axis > 2) {
+    if (e.dtype_bytes == 0 || e.method < 1 || e.method > 6 || e.axis < 0 || e.axis > 2) {
       fclose(f);
       return TRID_STATUS_INVALID_VALUE;
     }
@@ -254,6 +254,20 @@ static int axis_class(const Geom &g, int solvedim, int elem_bytes) {
   return g.stride[kD] * (int64_t)elem_bytes <= 65536 ? 1 : 2;
 }
 
+// Axis-0 systems solved whole by one warp (method 5) or one CTA (method 6,
+// and the default up to 4096 rows) each.  cudaErrorNotSupported when neither
+// applies.
+template <typename T, int MODE>
+static cudaError_t launch_x_whole(const Geom &g, const XArgs<T> &A, const MethodChoice &m,
+                                  cudaStream_t st) {
+  if (m.method == 5) {
+    const cudaError_t e = launch_xwarp<T, MODE>(g, A, st);
+    if (e != cudaErrorNotSupported) return e;
+  }
+  if (g.n <= 4096) return launch_xcta<T, MODE>(g, A, m.method == 6 ? m.chunk : 0, st);
+  return cudaErrorNotSupported;
+}
+
 template <typename T, int INC>
 static tridStatus_t solve_level(const T *a, const T *b, const T *c, T *d, T *u, int ndim,
                                 int solvedim, const int *dims, const int *const pads[5],
@@ -281,12 +295,12 @@ static tridStatus_t solve_level(const T *a, const T *b, const T *c, T *d, T *u, 
   }
   if (e != cudaErrorNotSupported) {
     // done (or failed) by the method-4 kernel
-  } else if (m.method >= 2 && !fits && axis == 0 && g.n <= 4096 &&
-             (e = launch_xcta<T, INC ? kXcFwdInc : kXcFwd>(
+  } else if (m.method >= 2 && axis == 0 && (!fits || m.method >= 5) &&
+             (e = launch_x_whole<T, INC ? kXcFwdInc : kXcFwd>(
                   g, XArgs<T>{a, b, c, d, nullptr, nullptr, INC ? u : d, nullptr, nullptr, nullptr,
                               nullptr},
-                  stream)) != cudaErrorNotSupported) {
-    // one CTA per system: done (or failed) above
+                  m, stream)) != cudaErrorNotSupported) {
+    // one warp or one CTA per system: done (or failed) above
   } else if (m.method >= 2 && !fits) {
     GenArgs<T> A = {};
     A.a = a;
@@ -356,9 +370,9 @@ tridStatus_t solve_adjoint(const T *a, const T *b, const T *c, const T *u, const
   MethodChoice m = choose_method((int)sizeof(T), axis, g.n, 0);
   if (m.chunk == 0) m.chunk = 8;
   if (m.spc == 0) m.spc = 8;
-  if (axis == 0 && g.n <= 4096) {
-    const cudaError_t e = launch_xcta<T, kXcAdj>(
-        g, XArgs<T>{a, b, c, nullptr, w, u, nullptr, ga, gb, gc, gd}, stream);
+  if (axis == 0 && (g.n > 64 || m.method >= 5)) {
+    const cudaError_t e = launch_x_whole<T, kXcAdj>(
+        g, XArgs<T>{a, b, c, nullptr, w, u, nullptr, ga, gb, gc, gd}, m, stream);
     if (e != cudaErrorNotSupported)
       return e == cudaSuccess ? TRID_STATUS_SUCCESS : TRID_STATUS_EXECUTION_FAILED;
   }
@@ -375,7 +389,7 @@ tridStatus_t solve_adjoint(const T *a, const T *b, const T *c, const T *u, const
   return run_general<T, kGenAdj>(g, A, axis, m.chunk, m.spc, 0, stream);
 }
 // Forward solve and adjoint of the linear loss <w, x> in one pass where a
-// one-CTA-per-system kernel applies (axis 0, n <= 4096); otherwise the
+// one-warp or one-CTA-per-system kernel applies (axis 0, n <= 4096); otherwise the
 // forward solve followed by the adjoint.
 template <typename T>
 tridStatus_t solve_fwd_adj(const T *a, const T *b, const T *c, const T *d, const T *w, T *x,
@@ -392,18 +406,18 @@ tridStatus_t solve_fwd_adj(const T *a, const T *b, const T *c, const T *d, const
     if (o && ((uintptr_t)o % sizeof(T)) != 0) return TRID_STATUS_INVALID_VALUE;
   if (g.n == 0 || g.nsys == 0) return TRID_STATUS_SUCCESS;
   const cudaStream_t stream = current_stream();
-  if (solvedim == 0 && g.n <= 4096) {
-    const cudaError_t e = launch_xcta<T, kXcFused>(
-        g, XArgs<T>{a, b, c, d, w, nullptr, x, ga, gb, gc, gd}, stream);
+  const int axis = axis_class(g, solvedim, (int)sizeof(T));
+  MethodChoice m = choose_method((int)sizeof(T), axis, g.n, 0);
+  if (m.chunk == 0) m.chunk = 8;
+  if (m.spc == 0) m.spc = 8;
+  if (axis == 0) {
+    const cudaError_t e = launch_x_whole<T, kXcFused>(
+        g, XArgs<T>{a, b, c, d, w, nullptr, x, ga, gb, gc, gd}, m, stream);
     if (e != cudaErrorNotSupported)
       return e == cudaSuccess ? TRID_STATUS_SUCCESS : TRID_STATUS_EXECUTION_FAILED;
   }
   // two passes: x = A^{-1} d (blocked partition, d left intact), then the
   // adjoint at x
-  const int axis = axis_class(g, solvedim, (int)sizeof(T));
-  MethodChoice m = choose_method((int)sizeof(T), axis, g.n, 0);
-  if (m.chunk == 0) m.chunk = 8;
-  if (m.spc == 0) m.spc = 8;
   GenArgs<T> A = {};
   A.a = a;
   A.b = b;
@@ -555,7 +569,7 @@ extern "C" const char *tridGetStatusString(tridStatus_t s) {
 }
 
 extern "C" tridStatus_t tridSetMethod(int method, int chunk, int sys_per_cta) {
-  if (method < 0 || method > 4) return TRID_STATUS_INVALID_VALUE;
+  if (method < 0 || method > 6) return TRID_STATUS_INVALID_VALUE;
   if (chunk != 0 && chunk != 2 && chunk != 4 && chunk != 8 && chunk != 16)
     return TRID_STATUS_INVALID_VALUE;
   if (sys_per_cta != 0 && sys_per_cta != 4 && sys_per_cta != 8 && sys_per_cta != 16)

@@ -1,12 +1,14 @@
 // Axis-0 systems of one CTA (sm_100a): the blocked partition of
-// kern_general.cu kept inside one CTA, so systems of 513..4096 rows are solved
-// in one launch without re-reading anything.
+// kern_general.cu kept inside one CTA, so systems of up to 4096 rows are
+// solved in one launch without re-reading anything.
 //
-// CTA = one system, W warps; warp w owns block w (32 chunks of M rows).
+// CTA = one system, W <= 16 warps; warp w owns block w (32 chunks of M rows,
+// M = 4, 8 or 16).
 // Every warp reduces its chunks (chunk_reduce) and its block
 // (warp_block_basis + block_rows); the 2W block rows meet in shared memory,
 // warp 0 solves the block system (one warp interface solve, lane = block),
-// and every warp finishes its block from its two boundary unknowns.
+// and every warp finishes its block from its two boundary unknowns.  A
+// system of one block skips the block level.
 //
 // Modes:
 //   kXFwd / kXFwdInc : x = A^{-1} d into d / added into u;
@@ -32,6 +34,12 @@ __device__ __forceinline__ void cta_solve(T (&al)[M], const T (&be)[M], T (&ga)[
                                           int w, int lane, int nw, T *sm) {
   Row<T> F, L;
   chunk_reduce<T, M>(al, be, ga, de, F, L);
+  if (nw == 1) {  // one block: the warp's interface system is the whole system
+    T xF, xL;
+    warp_interface_solve(F, L, xF, xL, lane);
+    chunk_backsub<T, M>(al, ga, de, xF, xL);
+    return;
+  }
   T bF[3], bL[3];
   warp_block_basis(F, L, lane, bF, bL);
   Row<T> FB, LB;
@@ -134,8 +142,8 @@ __device__ __forceinline__ void stage_out(const Stage<T, M> &S, int k, int w, in
   }
 }
 
-template <typename T, int M, int MODE>
-__global__ void __launch_bounds__(512) xcta_kernel(Geom g, XArgs<T> A) {
+template <typename T, int M, int MODE, int MAXW>
+__global__ void __launch_bounds__(MAXW * 32) xcta_kernel(Geom g, XArgs<T> A) {
   extern __shared__ __align__(16) unsigned char xcta_dyn[];
   __shared__ T sm[128 + 32 + 2 * 16];
   const int lane = threadIdx.x & (kWarp - 1);
@@ -267,38 +275,50 @@ __global__ void __launch_bounds__(512) xcta_kernel(Geom g, XArgs<T> A) {
   }
 }
 
-template <typename T, int M, int MODE>
+template <typename T, int M, int MODE, int MAXW>
 static cudaError_t launch_xcta_m(const Geom &g, const XArgs<T> &A, int warps, cudaStream_t st) {
   constexpr int kArrays = (MODE == kXAdj || MODE == kXFused) ? 5 : 4;
   const size_t smem = (size_t)kArrays * warps * Stage<T, M>::R * sizeof(T);
-  static bool attr_set = false;  // per instantiation; the attribute is per device function
-  if (!attr_set) {
-    const cudaError_t e = cudaFuncSetAttribute(xcta_kernel<T, M, MODE>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               kArrays * 16 * Stage<T, M>::R * (int)sizeof(T));
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 64) return cudaErrorNotSupported;
+  static bool attr_set[64] = {};  // per device
+  if (!attr_set[dev]) {
+    e = cudaFuncSetAttribute(xcta_kernel<T, M, MODE, MAXW>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kArrays * MAXW * Stage<T, M>::R * (int)sizeof(T));
     if (e != cudaSuccess) return e;
-    attr_set = true;
+    attr_set[dev] = true;
   }
-  xcta_kernel<T, M, MODE><<<(unsigned)g.nsys, warps * kWarp, smem, st>>>(g, A);
+  xcta_kernel<T, M, MODE, MAXW><<<(unsigned)g.nsys, warps * kWarp, smem, st>>>(g, A);
   return cudaGetLastError();
 }
 
 template <typename T, int MODE>
-cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, cudaStream_t st) {
-  // M = 4 up to 2048 rows (8..16 warps), M = 8 up to 4096
+cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, int chunk, cudaStream_t st) {
+  // rows per thread M (chunk, or by length: 16 above 256 rows -- fewer warps
+  // per system beat shorter chains on B200 at every length measured, 512 to
+  // 4096 -- else 8 or 4); at most 16 warps, so n <= 512*M
   const int n = g.n;
   if (n > 4096 || g.nsys > 0x7fffffff) return cudaErrorNotSupported;
-  const int M = (n <= 2048) ? 4 : 8;
+  int M = chunk;
+  if (M != 4 && M != 8 && M != 16) M = (n > 256) ? 16 : (n > 128 ? 8 : 4);
+  while (n > 512 * M) M *= 2;
   const int warps = (n + 32 * M - 1) / (32 * M);
-  return M == 4 ? launch_xcta_m<T, 4, MODE>(g, A, warps, st)
-                : launch_xcta_m<T, 8, MODE>(g, A, warps, st);
+  if (M == 4) return launch_xcta_m<T, 4, MODE, 16>(g, A, warps, st);
+  if (M == 8)
+    return warps <= 8 ? launch_xcta_m<T, 8, MODE, 8>(g, A, warps, st)
+                      : launch_xcta_m<T, 8, MODE, 16>(g, A, warps, st);
+  return launch_xcta_m<T, 16, MODE, 8>(g, A, warps, st);
 }
 
 #define TRID_XCTA_INSTANTIATE(T)                                                               \
-  template cudaError_t launch_xcta<T, kXFwd>(const Geom &, const XArgs<T> &, cudaStream_t);    \
-  template cudaError_t launch_xcta<T, kXFwdInc>(const Geom &, const XArgs<T> &, cudaStream_t); \
-  template cudaError_t launch_xcta<T, kXAdj>(const Geom &, const XArgs<T> &, cudaStream_t);    \
-  template cudaError_t launch_xcta<T, kXFused>(const Geom &, const XArgs<T> &, cudaStream_t);
+  template cudaError_t launch_xcta<T, kXFwd>(const Geom &, const XArgs<T> &, int, cudaStream_t); \
+  template cudaError_t launch_xcta<T, kXFwdInc>(const Geom &, const XArgs<T> &, int,            \
+                                                cudaStream_t);                                  \
+  template cudaError_t launch_xcta<T, kXAdj>(const Geom &, const XArgs<T> &, int, cudaStream_t); \
+  template cudaError_t launch_xcta<T, kXFused>(const Geom &, const XArgs<T> &, int, cudaStream_t);
 TRID_XCTA_INSTANTIATE(float)
 TRID_XCTA_INSTANTIATE(double)
 

@@ -171,7 +171,10 @@ struct XArgs {
   T *ga, *gb, *gc, *gd;
 };
 template <typename T, int MODE>
-cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, cudaStream_t st);
+cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, int chunk, cudaStream_t st);
+// one-warp-per-system partition in shared memory on axis 0 (kern_xwarp.cu)
+template <typename T, int MODE>
+cudaError_t launch_xwarp(const Geom &g, const XArgs<T> &A, cudaStream_t st);
 
 template <typename T, int INC>
 cudaError_t launch_generic(const Geom &g, const T *a, const T *b, const T *c, T *d, T *u,
