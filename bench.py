@@ -15,7 +15,10 @@ Extra keys: roofline (dominant kernel vs the measured HBM copy bandwidth),
 cpu_baseline (the reference CPU solver compiled from the reference sources,
 all host threads, on the same cube), e2e (the same solves through the C ABI
 from pinned host buffers, host<->device copies inside the timed region),
-clocks (nvidia-smi samples during the timed region), gpu_launches.
+clocks (nvidia-smi samples during the timed region), gpu_launches,
+differentiation (16,384 x 1024 FP64: forward, forward + adjoint in one call
+and autograd forward + backward, times and their ratio to the forward solve,
+gradient error against central finite differences; rank 0 at N=1).
 
 --impl reference: times the reference's own CPU implementation of the path
 (scalar/src/cpu/trid_cpu.cpp built into oracle/_ref) on the same workload
@@ -298,12 +301,102 @@ def run_ours(args):
         "gpu_launches": 3 * args.steps,
         "clocks": clk.summary(),
     }
+    if rank == 0 and world == 1:
+        result["differentiation"] = measure_differentiation(torch, tb, max(3, min(args.steps, 20)))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline_entry(a, b, c, d0)
     if dist:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(result))
+
+
+def measure_differentiation(torch, tb, steps, seed=99):
+    """The differentiation workload: 16,384 FP64 systems of n=1024 along the
+    unit-stride axis, loss = sum(w * x) with w ~ N(0,1).  Times the plain
+    forward solve, the forward + adjoint in one call
+    (tridDmtsvStridedBatchFwdAdj: x and the gradients w.r.t. a, b, c, d) and
+    the autograd path (trid_solve forward + backward), and checks the
+    gradients against central finite differences (h = 1e-6) on 16 sampled
+    entries.  Every array is 134 MB (> L2), so no flush between launches."""
+    S, n = 16384, 1024
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    a = torch.rand(S, n, dtype=torch.float64, device="cuda", generator=gen) * 2 - 1
+    c = torch.rand(S, n, dtype=torch.float64, device="cuda", generator=gen) * 2 - 1
+    b = a.abs() + c.abs() + 1 + torch.rand(S, n, dtype=torch.float64, device="cuda", generator=gen)
+    d = torch.randn(S, n, dtype=torch.float64, device="cuda", generator=gen)
+    w = torch.randn(S, n, dtype=torch.float64, device="cuda", generator=gen)
+    dims = [n, S]
+    xs = d.clone()
+    x = torch.empty_like(d)
+    grads = [torch.empty_like(d) for _ in range(4)]
+    leaves = [t.clone().requires_grad_(True) for t in (a, b, c, d)]
+
+    def fwd():
+        st = tb.tridDmtsvStridedBatch(a, b, c, xs, None, 2, 0, dims, dims)
+        if st != 0:
+            raise tb.TridError(st, "tridDmtsvStridedBatch")
+
+    def fused():
+        st = tb.tridDmtsvStridedBatchFwdAdj(a, b, c, d, w, x, *grads, 2, 0, dims, dims)
+        if st != 0:
+            raise tb.TridError(st, "tridDmtsvStridedBatchFwdAdj")
+
+    def autograd():
+        for t in leaves:
+            t.grad = None
+        u = tb.trid_solve(*leaves)
+        u.backward(w)
+
+    stream = torch.cuda.current_stream()
+    times = {}
+    for name, fn in (("fwd", fwd), ("fused", fused), ("autograd", autograd)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times[name] = e0.elapsed_time(e1) / steps
+    fused()
+    torch.cuda.synchronize()
+    # central finite differences on one system per sample (h = 1e-6)
+    rng = np.random.default_rng(seed)
+    h = 1e-6
+    errs, gmax = [], 0.0
+    coefs = (a, b, c, d)
+    for k in range(16):
+        which, s_, i = k % 4, int(rng.integers(S)), int(rng.integers(1, n - 1))
+        rows = [t[s_:s_ + 1].clone() for t in coefs]
+        vals = []
+        for sign in (1, -1):
+            r = [t.clone() for t in rows]
+            r[which][0, i] += sign * h
+            tb.tridDmtsvStridedBatch(r[0], r[1], r[2], r[3], None, 2, 0, [n, 1], [n, 1])
+            vals.append(float((r[3][0] * w[s_]).sum()))
+        fd = (vals[0] - vals[1]) / (2 * h)
+        g = float(grads[which][s_, i])
+        errs.append(abs(fd - g))
+        gmax = max(gmax, abs(g))
+    unknowns = S * n
+    return {
+        "workload": "16,384 FP64 systems of n=1024 (unit stride), loss = sum(w*x), w ~ N(0,1)",
+        "fwd_ms": round(times["fwd"], 5),
+        "fwd_adj_ms": round(times["fused"], 5),
+        "autograd_fwd_bwd_ms": round(times["autograd"], 5),
+        "fwd_gbs": round(40 * unknowns / (times["fwd"] * 1e-3) / 1e9, 1),
+        "fwd_adj_gbs": round(80 * unknowns / (times["fused"] * 1e-3) / 1e9, 1),
+        "ratio_fwd_adj_over_fwd": round(times["fused"] / times["fwd"], 3),
+        "ratio_autograd_over_fwd": round(times["autograd"] / times["fwd"], 3),
+        "target_ratio": 2.2,
+        "grad_err_vs_fd": float(f"{max(errs) / max(1.0, gmax):.3e}"),
+        "fd": "central, h=1e-6, 16 sampled entries of a, b, c, d; error relative to max(1, max|g|)",
+        "bytes_per_unknown": {"fwd": 40, "fwd_adj": 80, "autograd": "40 + 16 (copy of d) + 72"},
+    }
 
 
 def cpu_baseline_entry(a, b, c, d):
