@@ -15,6 +15,16 @@ Candidates (see tridSetMethod in include/trid_b200.h):
                         rows-per-thread chunk that covers n and, on strided
                         axes, 4/8/16 systems per CTA
     method 4            strided axes: two-sided Thomas with a TMA stage ring
+    method 5            axis 0, longer systems: one warp per system, staged in
+                        shared memory
+    method 6, chunk     axis 0, longer systems: one CTA per system, 4/8/16
+                        rows per thread (up to 4096 rows)
+    (method 2 above 512 rows on axis 0 also means the blocked partition:
+    block reduction, recursive block solve, block finish)
+
+--stride-sweep instead times the default algorithm on FP64 problems of
+64 M unknowns whose solve axis has plane strides from 8 KiB to 2 MiB (the
+row span of one system against 2 MiB pages), with plain and TMA-staged tiles.
 
 Axis classes: 0 = solve along axis 0 (unit stride); 1 = strided, row stride
 <= 64 KiB; 2 = larger strides.  The timing problem of each bucket holds about
@@ -57,6 +67,13 @@ def candidates(axis, n):
                     out.append((3, ch, spc))
     if axis > 0:
         out.append((4, 0, 0))
+    elif n > 64:
+        out.append((5, 0, 0))
+        if n <= 4096:
+            for ch in (4, 8, 16):
+                out.append((6, ch, 0))
+        if not ch0:
+            out.append((2, 8, 0))  # blocked partition, 256-row blocks
     return out
 
 
@@ -127,6 +144,29 @@ def tune(dtypes=("f64", "f32"), lengths=(32, 64, 128, 256, 512), elems=1 << 24, 
     return table, report
 
 
+STRIDE_SHAPES = (([256, 4, 256, 256], 2), ([256, 16, 256, 64], 2), ([256, 256, 256], 1),
+                 ([256, 256, 256], 2), ([1024, 64, 256], 2), ([2048, 128, 256], 2))
+
+
+def stride_sweep(methods=((0, 0, 0), (2, 8, 8), (3, 8, 8), (3, 8, 16))):
+    """GB/s of FP64 solves of n=256 on strided axes whose plane stride grows
+    from 8 KiB to 2 MiB (the same 40 B/unknown and about 64 M unknowns each)."""
+    import torch
+
+    out = []
+    for m in methods:
+        for dims, sd in STRIDE_SHAPES:
+            ms = time_candidate(torch, torch.float64, dims, sd, m)
+            size = int(np.prod(dims))
+            row = {"dims": dims, "solvedim": sd, "method": list(m),
+                   "plane_stride_kib": int(np.prod(dims[:sd])) * 8 // 1024,
+                   "GBs": round(40 * size / (ms * 1e-3) / 1e9, 1)}
+            print(json.dumps(row), flush=True)
+            out.append(row)
+            torch.cuda.empty_cache()
+    return out
+
+
 def write_table(table, path):
     with open(path, "w") as f:
         f.write("# dtype axis_class nmax method chunk sys_per_cta (tridsolver_b200.autotune)\n")
@@ -141,7 +181,12 @@ def main():
     ap.add_argument("--lengths", default="32,64,128,256,512")
     ap.add_argument("--elems", type=int, default=1 << 24)
     ap.add_argument("--report", default=None, help="also write every timing as JSON")
+    ap.add_argument("--stride-sweep", action="store_true",
+                    help="only time strided solves against the plane stride")
     args = ap.parse_args()
+    if args.stride_sweep:
+        stride_sweep()
+        return
     table, report = tune(args.dtypes.split(","), [int(v) for v in args.lengths.split(",")],
                          args.elems)
     write_table(table, args.out)

@@ -59,7 +59,9 @@ __device__ __forceinline__ void cta_solve(T (&al)[M], const T (&be)[M], T (&ga)[
       RL = {q[4], q[5], q[6], q[7]};
     }
     T f, l;
-    warp_interface_solve(RF, RL, f, l, lane);
+    int span = 1;  // lanes with block rows, rounded up to a power of two
+    while (span < nw) span <<= 1;
+    warp_interface_solve(RF, RL, f, l, lane, span);
     if (lane < nw) {
       sm[128 + 2 * lane] = f;
       sm[128 + 2 * lane + 1] = l;
@@ -142,8 +144,19 @@ __device__ __forceinline__ void stage_out(const Stage<T, M> &S, int k, int w, in
   }
 }
 
+// Warm L2 with the system `dist` CTAs ahead (the CTA that will take this
+// one's place on the GPU): one bulk prefetch per array, so that DRAM keeps
+// streaming while the resident CTAs compute.  Needs 16-byte aligned rows of a
+// whole number of 16-byte units.
+template <typename T>
+__device__ __forceinline__ void prefetch_system_l2(const T *p, int n) {
+  const uint32_t bytes = (uint32_t)n * sizeof(T);
+  if (((uintptr_t)p & 15) == 0 && (bytes & 15) == 0)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 template <typename T, int M, int MODE, int MAXW>
-__global__ void __launch_bounds__(MAXW * 32) xcta_kernel(Geom g, XArgs<T> A) {
+__global__ void __launch_bounds__(MAXW * 32) xcta_kernel(Geom g, XArgs<T> A, int dist) {
   extern __shared__ __align__(16) unsigned char xcta_dyn[];
   __shared__ T sm[128 + 32 + 2 * 16];
   const int lane = threadIdx.x & (kWarp - 1);
@@ -166,6 +179,15 @@ __global__ void __launch_bounds__(MAXW * 32) xcta_kernel(Geom g, XArgs<T> A) {
   else
     stage_in<T, M>(S, 3, w, lane, A.d + off[kD], n);
   if (kHasW) stage_in<T, M>(S, 4, w, lane, A.w + off[kD], n);
+  if (dist > 0 && threadIdx.x == 0 && blockIdx.x + (int64_t)dist < g.nsys) {
+    int64_t po[5];
+    system_offsets(g, blockIdx.x + (int64_t)dist, po);
+    prefetch_system_l2(A.a + po[kA], n);
+    prefetch_system_l2(A.b + po[kB], n);
+    prefetch_system_l2(A.c + po[kC], n);
+    prefetch_system_l2(MODE == kXAdj ? A.usol + po[kU] : A.d + po[kD], n);
+    if (kHasW) prefetch_system_l2(A.w + po[kD], n);
+  }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();  // neighbouring rows are read across warp regions
 
@@ -291,7 +313,16 @@ static cudaError_t launch_xcta_m(const Geom &g, const XArgs<T> &A, int warps, cu
     if (e != cudaSuccess) return e;
     attr_set[dev] = true;
   }
-  xcta_kernel<T, M, MODE, MAXW><<<(unsigned)g.nsys, warps * kWarp, smem, st>>>(g, A);
+  // prefetch distance: the CTAs resident on the whole GPU at once
+  int per_sm = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xcta_kernel<T, M, MODE, MAXW>,
+                                                    warps * kWarp, smem) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    per_sm = 0;
+    cudaGetLastError();
+  }
+  xcta_kernel<T, M, MODE, MAXW><<<(unsigned)g.nsys, warps * kWarp, smem, st>>>(g, A,
+                                                                                per_sm * sms);
   return cudaGetLastError();
 }
 

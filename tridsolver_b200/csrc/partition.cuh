@@ -93,9 +93,12 @@ __device__ __forceinline__ void chunk_backsub(const T (&al)[M], const T (&ga)[M]
 // Solve the 64-row interface system held two rows per lane (all 32 lanes of
 // the warp must call this).  Lane 0's F row must not couple to the left
 // (fa = 0) and lane 31's L row not to the right (lc = 0).
+// span: a power of two >= the number of lanes holding non-identity rows
+// (lanes at or past it hold identity rows); PCR stops after log2(span)
+// steps, when every such row is decoupled.
 template <typename T>
 __device__ __forceinline__ void warp_interface_solve(const Row<T> &F, const Row<T> &L, T &xF,
-                                                     T &xL, int lane) {
+                                                     T &xL, int lane, int span = kWarp) {
   constexpr unsigned kFull = 0xffffffffu;
   const T ifb = rcp(F.b);
   // F row of the next chunk (its pivot as a reciprocal)
@@ -120,6 +123,7 @@ __device__ __forceinline__ void warp_interface_solve(const Row<T> &F, const Row<
   // coefficients pre-divided by its pivot, so a neighbour needs 3 values
 #pragma unroll
   for (int s = 1; s < kWarp; s <<= 1) {
+    if (s >= span) break;
     const T ib = rcp(rb);
     const T sa = ra * ib, sc = rc * ib, sd = rd * ib;
     const T ua = __shfl_up_sync(kFull, sa, s);
