@@ -17,7 +17,8 @@
 //                      in the same pass);
 //   kXFused          : forward and adjoint of the linear loss <w, x> in one
 //                      pass: reads a, b, c, d, w once and writes x, da, db,
-//                      dc, dd (10 values per unknown instead of 5 + 9).
+//                      dc, dd (10 values per unknown instead of 5 + 9); the
+//                      transposed chunk reductions reuse the forward pivots.
 #include "partition.cuh"
 
 namespace tridb200 {
@@ -29,11 +30,25 @@ constexpr int kXFwd = kXcFwd, kXFwdInc = kXcFwdInc, kXAdj = kXcAdj, kXFused = kX
 
 // Solve the system held in (al, be, ga, de) across the CTA; the solution
 // overwrites de.  Whole CTA must call it (barriers inside).
+// The part of cta_solve after the chunk reduction (F, L: this thread's
+// interface rows; al/ga/de: its reduced chunk).
+template <typename T, int M>
+__device__ __forceinline__ void cta_solve_rows(const Row<T> &F, const Row<T> &L, T (&al)[M],
+                                               T (&ga)[M], T (&de)[M], int w, int lane, int nw,
+                                               T *sm);
+
 template <typename T, int M>
 __device__ __forceinline__ void cta_solve(T (&al)[M], const T (&be)[M], T (&ga)[M], T (&de)[M],
                                           int w, int lane, int nw, T *sm) {
   Row<T> F, L;
   chunk_reduce<T, M>(al, be, ga, de, F, L);
+  cta_solve_rows<T, M>(F, L, al, ga, de, w, lane, nw, sm);
+}
+
+template <typename T, int M>
+__device__ __forceinline__ void cta_solve_rows(const Row<T> &F, const Row<T> &L, T (&al)[M],
+                                               T (&ga)[M], T (&de)[M], int w, int lane, int nw,
+                                               T *sm) {
   if (nw == 1) {  // one block: the warp's interface system is the whole system
     T xF, xL;
     warp_interface_solve(F, L, xF, xL, lane);
@@ -196,11 +211,12 @@ __global__ void __launch_bounds__(MAXW * 32) xcta_kernel(Geom g, XArgs<T> A, int
   const T *rc = S.region(2, w) + lane * (M + 1);
   const T *rd = S.region(3, w) + lane * (M + 1);
 
-  T gsol[M];  // adjoint solution (kXAdj / kXFused), reloaded for the gradients
-  if (kHasW) {
+  T gsol[M];  // the adjoint solution
+  T xs[M];    // the forward solution
+  if (MODE == kXAdj) {
     // transposed rows: sub-diagonal c_{r-1}, super-diagonal a_{r+1}
     const T *rw = S.region(4, w) + lane * (M + 1);
-    T ta[M], be[M], tg[M], tw[M];
+    T ta[M], be[M], tg[M];
 #pragma unroll
     for (int j = 0; j < M; ++j) {
       const int r = r0 + j;
@@ -208,23 +224,14 @@ __global__ void __launch_bounds__(MAXW * 32) xcta_kernel(Geom g, XArgs<T> A, int
       ta[j] = (in && r > 0) ? (j > 0 ? rc[j - 1] : S.row(2, r - 1)) : T(0);
       tg[j] = (r + 1 < n) ? (j < M - 1 ? ra[j + 1] : S.row(0, r + 1)) : T(0);
       be[j] = in ? rb[j] : T(1);
-      tw[j] = rw[j];  // zero-filled past n
+      gsol[j] = rw[j];  // zero-filled past n
     }
-    cta_solve<T, M>(ta, be, tg, tw, w, lane, nw, sm);
-    // parked in this thread's own slots of region 4 (read only by this
-    // thread above) for the forward solve's registers
-    T *pw = S.region(4, w) + lane * (M + 1);
-#pragma unroll
-    for (int j = 0; j < M; ++j) pw[j] = tw[j];
-  }
-
-  // the forward solution: solved here, or the staged one (kXAdj)
-  T xs[M];
-  if (MODE == kXAdj) {
+    cta_solve<T, M>(ta, be, tg, gsol, w, lane, nw, sm);
 #pragma unroll
     for (int j = 0; j < M; ++j) xs[j] = rd[j];
   } else {
-    T al[M], be[M], ga[M], de[M];
+    // forward rows
+    T al[M], be[M], ga[M], rp[M];
 #pragma unroll
     for (int j = 0; j < M; ++j) {
       const int r = r0 + j;
@@ -232,11 +239,34 @@ __global__ void __launch_bounds__(MAXW * 32) xcta_kernel(Geom g, XArgs<T> A, int
       al[j] = (in && r > 0) ? ra[j] : T(0);
       be[j] = in ? rb[j] : T(1);
       ga[j] = (r < n - 1) ? rc[j] : T(0);
-      de[j] = rd[j];  // zero-filled past n
+      xs[j] = rd[j];  // zero-filled past n
     }
-    cta_solve<T, M>(al, be, ga, de, w, lane, nw, sm);
+    if (MODE == kXFused) {
+      Row<T> F, L;
+      chunk_reduce_pivots<T, M>(al, be, ga, xs, F, L, rp);
+      cta_solve_rows<T, M>(F, L, al, ga, xs, w, lane, nw, sm);
+      // x into this thread's own slots of region 3 (d was read by this
+      // thread alone): the neighbours x_{r-1}, x_{r+1} and the outgoing x
+      T *rx = S.region(3, w) + lane * (M + 1);
 #pragma unroll
-    for (int j = 0; j < M; ++j) xs[j] = de[j];
+      for (int j = 0; j < M; ++j) rx[j] = xs[j];
+      // the transposed system: rows (c_{r-1}, b_r, a_{r+1}); its chunk
+      // interiors have the forward pivots rp
+      const T *rw = S.region(4, w) + lane * (M + 1);
+      T ta[M], tg[M];
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        const int r = r0 + j;
+        const bool in = r < n;
+        ta[j] = (in && r > 0) ? (j > 0 ? rc[j - 1] : S.row(2, r - 1)) : T(0);
+        tg[j] = (r + 1 < n) ? (j < M - 1 ? ra[j + 1] : S.row(0, r + 1)) : T(0);
+        gsol[j] = rw[j];  // zero-filled past n
+      }
+      chunk_reduce_given<T, M>(ta, be, tg, gsol, F, L, rp);
+      cta_solve_rows<T, M>(F, L, ta, tg, gsol, w, lane, nw, sm);
+    } else {
+      cta_solve<T, M>(al, be, ga, xs, w, lane, nw, sm);
+    }
   }
 
   if (MODE == kXFwd) {
@@ -248,16 +278,11 @@ __global__ void __launch_bounds__(MAXW * 32) xcta_kernel(Geom g, XArgs<T> A, int
     return;
   }
   // gradients: x_{r-1} and x_{r+1} from the staged solution (region 3)
-  if (MODE == kXFused) {
-    T *rx = S.region(3, w) + lane * (M + 1);
-#pragma unroll
-    for (int j = 0; j < M; ++j) rx[j] = xs[j];
-  }
   __syncthreads();
-  {
-    const T *pw = S.region(4, w) + lane * (M + 1);
+  if (MODE == kXFused) {
+    const T *rx = S.region(3, w) + lane * (M + 1);
 #pragma unroll
-    for (int j = 0; j < M; ++j) gsol[j] = pw[j];
+    for (int j = 0; j < M; ++j) xs[j] = rx[j];
   }
   const T xprev = (r0 > 0 && r0 - 1 < n) ? S.row(3, r0 - 1) : T(0);
   const T xnext = (r0 + M < n) ? S.row(3, r0 + M) : T(0);

@@ -74,6 +74,79 @@ __device__ __forceinline__ void chunk_reduce(T (&al)[M], const T (&be)[M], T (&g
   }
 }
 
+// chunk_reduce that also returns the reciprocal pivots rp[1..M-2] of the
+// chunk's interior block.  A chunk's interior block and its transpose have
+// the same pivots (p_j = b_j - a_j c_{j-1} / p_{j-1} either way), so the
+// transposed system can reuse them: chunk_reduce_given below.
+template <typename T, int M>
+__device__ __forceinline__ void chunk_reduce_pivots(T (&al)[M], const T (&be)[M], T (&ga)[M],
+                                                    T (&de)[M], Row<T> &F, Row<T> &L,
+                                                    T (&rp)[M]) {
+  static_assert(M >= 4, "chunks of at least four rows");
+  T r = rcp(be[1]);
+  rp[1] = r;
+  ga[1] *= r;
+  de[1] *= r;
+  al[1] *= r;
+#pragma unroll
+  for (int j = 2; j <= M - 2; ++j) {
+    r = rcp(be[j] - al[j] * ga[j - 1]);
+    rp[j] = r;
+    de[j] = (de[j] - al[j] * de[j - 1]) * r;
+    al[j] = -(al[j] * al[j - 1]) * r;
+    ga[j] = ga[j] * r;
+  }
+  T D = de[M - 2], A = al[M - 2], C = ga[M - 2];
+  L.a = -al[M - 1] * A;
+  L.b = be[M - 1] - al[M - 1] * C;
+  L.c = ga[M - 1];
+  L.d = de[M - 1] - al[M - 1] * D;
+#pragma unroll
+  for (int j = M - 3; j >= 1; --j) {
+    D = de[j] - ga[j] * D;
+    A = al[j] - ga[j] * A;
+    C = -ga[j] * C;
+  }
+  F.a = al[0];
+  F.b = be[0] - ga[0] * A;
+  F.c = -ga[0] * C;
+  F.d = de[0] - ga[0] * D;
+}
+
+// chunk_reduce with the interior's reciprocal pivots given: no divisions,
+// only multiply-add recurrences.
+template <typename T, int M>
+__device__ __forceinline__ void chunk_reduce_given(T (&al)[M], const T (&be)[M], T (&ga)[M],
+                                                   T (&de)[M], Row<T> &F, Row<T> &L,
+                                                   const T (&rp)[M]) {
+  static_assert(M >= 4, "chunks of at least four rows");
+  ga[1] *= rp[1];
+  de[1] *= rp[1];
+  al[1] *= rp[1];
+#pragma unroll
+  for (int j = 2; j <= M - 2; ++j) {
+    const T r = rp[j];
+    de[j] = (de[j] - al[j] * de[j - 1]) * r;
+    al[j] = -(al[j] * al[j - 1]) * r;
+    ga[j] = ga[j] * r;
+  }
+  T D = de[M - 2], A = al[M - 2], C = ga[M - 2];
+  L.a = -al[M - 1] * A;
+  L.b = be[M - 1] - al[M - 1] * C;
+  L.c = ga[M - 1];
+  L.d = de[M - 1] - al[M - 1] * D;
+#pragma unroll
+  for (int j = M - 3; j >= 1; --j) {
+    D = de[j] - ga[j] * D;
+    A = al[j] - ga[j] * A;
+    C = -ga[j] * C;
+  }
+  F.a = al[0];
+  F.b = be[0] - ga[0] * A;
+  F.c = -ga[0] * C;
+  F.d = de[0] - ga[0] * D;
+}
+
 // Interior unknowns; the solution overwrites de[0..M-1].
 template <typename T, int M>
 __device__ __forceinline__ void chunk_backsub(const T (&al)[M], const T (&ga)[M], T (&de)[M],
