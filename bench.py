@@ -20,6 +20,9 @@ differentiation (16,384 x 1024 FP64: forward, forward + adjoint in one call
 and autograd forward + backward, times and their ratio to the forward solve,
 gradient error against central finite differences; rank 0 at N=1).
 
+--suite: one JSON line per other workload (FP32 cube, long systems,
+variable-length batch, block systems, ADI steps and the ADI gradient).
+
 --impl reference: times the reference's own CPU implementation of the path
 (scalar/src/cpu/trid_cpu.cpp built into oracle/_ref) on the same workload
 with every host thread; with N>1 only rank 0 runs it.
@@ -462,6 +465,142 @@ def run_reference(args):
     }))
 
 
+def run_suite(args):
+    """The other workloads of the path, one JSON line each (GPU, N=1):
+    FP32 cube per axis, long systems, variable-length batch, block systems
+    (forward and adjoint), ADI steps (eager and CUDA graph) and the
+    checkpointed ADI gradient.  Algorithmic bytes per workload are stated in
+    each line; inputs are seeded synthetic data of the workload's shapes and
+    distributions; every timing is CUDA events around K launches after 2
+    warm-up launches, inputs larger than L2 unless stated."""
+    import torch
+
+    import tridsolver_b200 as tb
+    from tridsolver_b200.adi import ADI
+    from tridsolver_b200.block import btsv, btsv_adjoint
+    from tridsolver_b200.varlen import solve_varlen
+
+    peak, peak_kind = measured_peak()
+    K = max(3, min(args.steps, 10))
+    dev = torch.device("cuda")
+    gen = torch.Generator(device="cuda").manual_seed(2024)
+
+    def timed(fn, reps=K):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def emit(d):
+        d["peak_gbs_" + peak_kind] = peak
+        if "gbs" in d:
+            d["frac_of_" + peak_kind] = round(d["gbs"] / peak, 4)
+        print(json.dumps(d), flush=True)
+
+    def coeffs(shape, dtype):
+        a = torch.rand(shape, dtype=dtype, device=dev, generator=gen) * 2 - 1
+        c = torch.rand(shape, dtype=dtype, device=dev, generator=gen) * 2 - 1
+        b = a.abs() + c.abs() + 1 + torch.rand(shape, dtype=dtype, device=dev, generator=gen)
+        d = torch.randn(shape, dtype=dtype, device=dev, generator=gen)
+        return a, b, c, d
+
+    # FP32 256^3, each axis (20 B per unknown)
+    a, b, c, d = coeffs((UNKNOWNS,), torch.float32)
+    for sd in range(3):
+        ms = timed(lambda: tb.tridSmtsvStridedBatch(a, b, c, d, None, 3, sd, DIMS, DIMS))
+        emit({"workload": f"FP32 256^3 solvedim {sd}", "ms": round(ms, 5),
+              "gbs": round(20 * UNKNOWNS / (ms * 1e-3) / 1e9, 1)})
+    del a, b, c, d
+
+    # long systems: 2048 x n=65,536 FP64 along axis 0
+    n, S = 65536, 2048
+    a, b, c, d = coeffs((S * n,), torch.float64)
+    ms = timed(lambda: tb.tridDmtsvStridedBatch(a, b, c, d, None, 2, 0, [n, S], [n, S]))
+    emit({"workload": "FP64 2048 systems of n=65,536 (axis 0, blocked partition)",
+          "ms": round(ms, 4), "gbs": round(40 * n * S / (ms * 1e-3) / 1e9, 1),
+          "bytes_per_unknown": {"algorithmic": 40, "moved": "72 + block systems (a, b, c, d read "
+                                "twice: block reduction, then block finish)"}})
+    del a, b, c, d
+
+    # variable-length batch: 200,000 systems, lengths floor(exp(U(ln 8, ln 8192)))
+    rng = np.random.default_rng(7)
+    lens = np.floor(np.exp(rng.uniform(np.log(8), np.log(8192), 200000))).astype(np.int64)
+    off = torch.from_numpy(np.concatenate([[0], np.cumsum(lens)])).to(dev)
+    total = int(lens.sum())
+    a, b, c, d = coeffs((total,), torch.float64)
+    ms = timed(lambda: solve_varlen(a, b, c, d, off, total))
+    emit({"workload": "FP64 variable-length batch, 200,000 systems, n ~ logU[8, 8192]",
+          "unknowns": total, "ms": round(ms, 4),
+          "gbs": round((40 * total + 8 * (len(lens) + 1)) / (ms * 1e-3) / 1e9, 1)})
+    del a, b, c, d, off
+
+    # block tridiagonal: M in {2, 4, 8}, N=256, P=32,768 (interleaved layout)
+    for M in (2, 4, 8):
+        N, P = 256, 32768
+        A = (torch.rand((N, P, M, M), dtype=torch.float64, device=dev, generator=gen) * 2 - 1) / M
+        C = (torch.rand((N, P, M, M), dtype=torch.float64, device=dev, generator=gen) * 2 - 1) / M
+        B = (torch.rand((N, P, M, M), dtype=torch.float64, device=dev, generator=gen) * 2 - 1) / M
+        B += (2 + torch.rand((N, P, 1, 1), dtype=torch.float64, device=dev, generator=gen)) * \
+            torch.eye(M, dtype=torch.float64, device=dev)
+        dv = torch.randn((N, P, M), dtype=torch.float64, device=dev, generator=gen)
+        x = torch.empty_like(dv)
+        ms = timed(lambda: btsv(A, B, C, dv, x))
+        rows = N * P
+        fwd_b = (3 * M * M + 2 * M) * 8 * rows
+        emit({"workload": f"FP64 block tridiagonal M={M}, N=256, P=32,768: forward",
+              "ms": round(ms, 4), "gbs": round(fwd_b / (ms * 1e-3) / 1e9, 1),
+              "bytes_per_block_row": (3 * M * M + 2 * M) * 8})
+        w = torch.randn_like(dv)
+        msa = timed(lambda: btsv_adjoint(A, B, C, x, w))
+        adj_b = (6 * M * M + 3 * M) * 8 * rows
+        emit({"workload": f"FP64 block tridiagonal M={M}, N=256, P=32,768: adjoint",
+              "ms": round(msa, 4), "gbs": round(adj_b / (msa * 1e-3) / 1e9, 1),
+              "bytes_per_block_row": (6 * M * M + 3 * M) * 8})
+        del A, B, C, dv, x, w
+        torch.cuda.empty_cache()
+
+    # ADI heat diffusion: 128^3 x 100 steps, eager and CUDA graph; 64^3 x 10
+    for shape, steps in (((128, 128, 128), 100), ((64, 64, 64), 10)):
+        u = torch.rand(shape, dtype=torch.float64, device=dev, generator=gen)
+        adi = ADI(shape, 1.0)
+        ms_e = timed(lambda: adi.step(u, steps), reps=2)
+        adi.run(u, 2, graph=True)
+        ms_g = timed(lambda: adi.run(u, steps, graph=True), reps=2)
+        elems = int(np.prod(shape))
+        emit({"workload": f"FP64 ADI {shape[0]}^3 x {steps} steps (lambda=1)",
+              "ms_eager": round(ms_e, 3), "ms_graph": round(ms_g, 3),
+              "us_per_step_graph": round(1e3 * ms_g / steps, 2),
+              "gbs": round(56 * elems * steps / (ms_g * 1e-3) / 1e9, 1),
+              "bytes_per_element_step": "56: x solve with the stencil fused (read u, write "
+                                        "du1), y solve (du1 -> du2), z solve adding into u"})
+        del u, adi
+
+    # checkpointed adjoint of ||u_200|| at 128^3 w.r.t. u0 and lambda
+    shape = (128, 128, 128)
+    u0 = torch.rand(shape, dtype=torch.float64, device=dev, generator=gen)
+    adi = ADI(shape, 1.0)
+    torch.cuda.synchronize()
+    torch.cuda.reset_peak_memory_stats()
+    base = torch.cuda.memory_allocated()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    loss, du0, dlam = adi.grad_final_norm(u0, 200, 20)
+    e1.record()
+    torch.cuda.synchronize()
+    emit({"workload": "FP64 ADI 128^3 x 200 steps: d||u_200|| / d(u0, lambda), checkpoints "
+                      "every 20 steps", "ms": round(e0.elapsed_time(e1), 2),
+          "peak_extra_mib": round((torch.cuda.max_memory_allocated() - base) / 2**20, 1),
+          "loss": float(loss), "dloss_dlambda": float(dlam)})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -469,7 +608,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--suite", action="store_true",
+                    help="instead: one JSON line per other workload of the path (1 GPU)")
     args = ap.parse_args()
+    if args.suite:
+        run_suite(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -266,7 +266,8 @@ TRID_EXTERN_C tridStatus_t tridLoadTuningTable(const char *path);
 
 /* The method/chunk/sys_per_cta the dispatcher would use for a problem:
  * dtype_bytes 4 or 8; axis class 0 = solve along axis 0 (unit stride),
- * 1 = strided solve with a row stride of at most 64 KiB, 2 = larger stride. */
+ * 1 = strided solve with a row stride of at most 64 KiB, 2 = at most 1 MiB,
+ * 3 = larger stride. */
 TRID_EXTERN_C tridStatus_t tridQueryMethod(int dtype_bytes, int axis, int n, int *method,
                                            int *chunk, int *sys_per_cta);
 

@@ -136,6 +136,15 @@ def test_method_override_and_query():
     assert (m.value, ch.value, spc.value) == (3, 8, 8)
     assert L.tridQueryMethod(8, 2, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
     assert (m.value, ch.value, spc.value) == (2, 8, 8)
+    # strides past 1 MiB, and FP32 strided axes: plain loads, 16 systems per CTA
+    assert L.tridQueryMethod(8, 3, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+    assert (m.value, ch.value, spc.value) == (3, 8, 16)
+    for cls in (1, 2, 3):
+        assert L.tridQueryMethod(4, cls, 256, ctypes.byref(m), ctypes.byref(ch),
+                                 ctypes.byref(spc)) == 0
+        assert (m.value, ch.value, spc.value) == (3, 8, 16)
+    assert L.tridQueryMethod(8, 4, 256, ctypes.byref(m), ctypes.byref(ch),
+                             ctypes.byref(spc)) == INVALID
     tb.set_method(1)
     assert L.tridQueryMethod(8, 0, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
     assert m.value == 1

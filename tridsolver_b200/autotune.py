@@ -27,9 +27,11 @@ Candidates (see tridSetMethod in include/trid_b200.h):
 row span of one system against 2 MiB pages), with plain and TMA-staged tiles.
 
 Axis classes: 0 = solve along axis 0 (unit stride); 1 = strided, row stride
-<= 64 KiB; 2 = larger strides.  The timing problem of each bucket holds about
-``--elems`` unknowns (16.7 M by default, > L2 for FP64 and FP32) shaped as
-[n, S] (class 0), [256, n, S] (class 1) or [256, S, n] (class 2).
+<= 64 KiB; 2 = <= 1 MiB; 3 = larger strides (swept with --classes 0,1,2,3).
+The timing problem of each bucket holds about ``--elems`` unknowns (16.7 M by
+default, > L2 for FP64 and FP32) shaped as [n, S] (class 0), [256, n, S]
+(class 1) or [256, S, n] (class 2); class 3 uses [32, S, n] with S >= 8192
+(a 2 MiB row stride in FP64).
 """
 
 import argparse
@@ -80,6 +82,8 @@ def candidates(axis, n):
 def problem_dims(axis, n, elems):
     if axis == 0:
         return [n, max(1, elems // n)], 0
+    if axis == 3:
+        return [32, max(8192, elems // (32 * n)), n], 2
     rest = max(1, elems // (256 * n))
     if axis == 1:
         return [256, n, rest], 1
@@ -120,13 +124,14 @@ def time_candidate(torch, dtype, dims, solvedim, method, reps=10):
         L.tridSetMethod(0, 0, 0)
 
 
-def tune(dtypes=("f64", "f32"), lengths=(32, 64, 128, 256, 512), elems=1 << 24, verbose=True):
+def tune(dtypes=("f64", "f32"), lengths=(32, 64, 128, 256, 512), elems=1 << 24, verbose=True,
+         classes=(0, 1, 2)):
     import torch
 
     table, report = [], []
     for dt in dtypes:
         tdtype = torch.float64 if dt == "f64" else torch.float32
-        for axis in (0, 1, 2):
+        for axis in classes:
             for n in lengths:
                 dims, sd = problem_dims(axis, n, elems)
                 best = None
@@ -180,6 +185,7 @@ def main():
     ap.add_argument("--dtypes", default="f64,f32")
     ap.add_argument("--lengths", default="32,64,128,256,512")
     ap.add_argument("--elems", type=int, default=1 << 24)
+    ap.add_argument("--classes", default="0,1,2", help="axis classes to sweep (0-3)")
     ap.add_argument("--report", default=None, help="also write every timing as JSON")
     ap.add_argument("--stride-sweep", action="store_true",
                     help="only time strided solves against the plane stride")
@@ -188,7 +194,7 @@ def main():
         stride_sweep()
         return
     table, report = tune(args.dtypes.split(","), [int(v) for v in args.lengths.split(",")],
-                         args.elems)
+                         args.elems, classes=[int(v) for v in args.classes.split(",")])
     write_table(table, args.out)
     if args.report:
         with open(args.report, "w") as f:

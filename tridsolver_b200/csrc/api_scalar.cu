@@ -92,7 +92,7 @@ static tridStatus_t parse_tuning_table(const char *path, std::vector<TuneEntry> 
       return TRID_STATUS_INVALID_VALUE;
     }
     e.dtype_bytes = (strcmp(dt, "f64") == 0) ? 8 : (strcmp(dt, "f32") == 0 ? 4 : 0);
-    if (e.dtype_bytes == 0 || e.method < 1 || e.method > 6 || e.axis < 0 || e.axis > 2) {
+    if (e.dtype_bytes == 0 || e.method < 1 || e.method > 6 || e.axis < 0 || e.axis > 3) {
       fclose(f);
       return TRID_STATUS_INVALID_VALUE;
     }
@@ -143,11 +143,21 @@ MethodChoice choose_method(int dtype_bytes, int axis, int n, int opt_hint) {
     }
   }
   if (m.method == 0) {
-    // built-in defaults, from the B200 sweep of tridsolver_b200.autotune:
-    // TMA staging wins on axis 0 and on large strides, plain coalesced loads
-    // on moderate strides; systems longer than 512 rows take the blocked
-    // partition (method 2 with blocks of 32*chunk rows)
-    m.method = (axis == 1) ? 3 : 2;
+    // built-in defaults, from the B200 sweeps of tridsolver_b200.autotune:
+    // TMA staging wins on axis 0 and, in FP64, on strides of 64 KiB..1 MiB;
+    // plain coalesced loads elsewhere on strided axes, with 16 systems per
+    // CTA (64-byte row segments) in FP32 and beyond 1 MiB in FP64 (where a
+    // tile's rows fall in different 2 MiB pages and the TMA tiles slow
+    // down); long axis-0 systems take one CTA each, longer ones the blocked
+    // partition (blocks of 32*chunk rows)
+    if (axis == 0) {
+      m.method = 2;
+    } else if (dtype_bytes == 4 || axis == 3) {
+      m.method = 3;
+      m.spc = 16;
+    } else {
+      m.method = (axis == 1) ? 3 : 2;
+    }
   }
   if (m.method >= 2) {
     const int need = chunk_for(n, dtype_bytes);
@@ -248,10 +258,11 @@ static tridStatus_t run_general(const Geom &g, GenArgs<T> A, int axis, int chunk
 
 static int axis_class(const Geom &g, int solvedim, int elem_bytes) {
   // 0 = unit stride inside a system, 1 = strided with a row stride of at most
-  // 64 KiB, 2 = larger strides (the outermost axis of a big cube, where
-  // DRAM-page and TLB locality differ)
+  // 64 KiB, 2 = up to 1 MiB (the outermost axis of a big cube, where DRAM-page
+  // and TLB locality differ), 3 = larger (every row in its own 2 MiB page)
   if (solvedim == 0) return 0;
-  return g.stride[kD] * (int64_t)elem_bytes <= 65536 ? 1 : 2;
+  const int64_t bytes = g.stride[kD] * (int64_t)elem_bytes;
+  return bytes <= 65536 ? 1 : (bytes <= (1 << 20) ? 2 : 3);
 }
 
 // Axis-0 systems solved whole by one warp (method 5) or one CTA (method 6,
@@ -602,7 +613,7 @@ extern "C" tridStatus_t tridLoadTuningTable(const char *path) {
 
 extern "C" tridStatus_t tridQueryMethod(int dtype_bytes, int axis, int n, int *method, int *chunk,
                                         int *sys_per_cta) {
-  if ((dtype_bytes != 4 && dtype_bytes != 8) || axis < 0 || axis > 2 || n < 0 || !method ||
+  if ((dtype_bytes != 4 && dtype_bytes != 8) || axis < 0 || axis > 3 || n < 0 || !method ||
       !chunk || !sys_per_cta)
     return TRID_STATUS_INVALID_VALUE;
   const MethodChoice m = choose_method(dtype_bytes, axis, n, 0);
