@@ -21,7 +21,8 @@ and autograd forward + backward, times and their ratio to the forward solve,
 gradient error against central finite differences; rank 0 at N=1).
 
 --suite: one JSON line per other workload (FP32 cube, long systems,
-variable-length batch, block systems, ADI steps and the ADI gradient).
+variable-length batch, block systems, ADI steps and the ADI gradient);
+--scale f runs the batched workloads with a fraction f of their systems.
 
 --impl reference: times the reference's own CPU implementation of the path
 (scalar/src/cpu/trid_cpu.cpp built into oracle/_ref) on the same workload
@@ -519,11 +520,14 @@ def run_suite(args):
               "gbs": round(20 * UNKNOWNS / (ms * 1e-3) / 1e9, 1)})
     del a, b, c, d
 
+    sc = args.scale  # fraction of each workload's systems (1 = the configured sizes)
+    assert 0 < sc <= 1, "--scale in (0, 1]"
+
     # long systems: 2048 x n=65,536 FP64 along axis 0
-    n, S = 65536, 2048
+    n, S = 65536, max(1, int(2048 * sc))
     a, b, c, d = coeffs((S * n,), torch.float64)
     ms = timed(lambda: tb.tridDmtsvStridedBatch(a, b, c, d, None, 2, 0, [n, S], [n, S]))
-    emit({"workload": "FP64 2048 systems of n=65,536 (axis 0, blocked partition)",
+    emit({"workload": f"FP64 {S} systems of n=65,536 (axis 0, blocked partition)",
           "ms": round(ms, 4), "gbs": round(40 * n * S / (ms * 1e-3) / 1e9, 1),
           "bytes_per_unknown": {"algorithmic": 40, "moved": "72 + block systems (a, b, c, d read "
                                 "twice: block reduction, then block finish)"}})
@@ -531,19 +535,20 @@ def run_suite(args):
 
     # variable-length batch: 200,000 systems, lengths floor(exp(U(ln 8, ln 8192)))
     rng = np.random.default_rng(7)
-    lens = np.floor(np.exp(rng.uniform(np.log(8), np.log(8192), 200000))).astype(np.int64)
+    nvar = max(1, int(200000 * sc))
+    lens = np.floor(np.exp(rng.uniform(np.log(8), np.log(8192), nvar))).astype(np.int64)
     off = torch.from_numpy(np.concatenate([[0], np.cumsum(lens)])).to(dev)
     total = int(lens.sum())
     a, b, c, d = coeffs((total,), torch.float64)
     ms = timed(lambda: solve_varlen(a, b, c, d, off, total))
-    emit({"workload": "FP64 variable-length batch, 200,000 systems, n ~ logU[8, 8192]",
+    emit({"workload": f"FP64 variable-length batch, {nvar} systems, n ~ logU[8, 8192]",
           "unknowns": total, "ms": round(ms, 4),
           "gbs": round((40 * total + 8 * (len(lens) + 1)) / (ms * 1e-3) / 1e9, 1)})
     del a, b, c, d, off
 
     # block tridiagonal: M in {2, 4, 8}, N=256, P=32,768 (interleaved layout)
     for M in (2, 4, 8):
-        N, P = 256, 32768
+        N, P = 256, max(1, int(32768 * sc))
         A = (torch.rand((N, P, M, M), dtype=torch.float64, device=dev, generator=gen) * 2 - 1) / M
         C = (torch.rand((N, P, M, M), dtype=torch.float64, device=dev, generator=gen) * 2 - 1) / M
         B = (torch.rand((N, P, M, M), dtype=torch.float64, device=dev, generator=gen) * 2 - 1) / M
@@ -554,13 +559,13 @@ def run_suite(args):
         ms = timed(lambda: btsv(A, B, C, dv, x))
         rows = N * P
         fwd_b = (3 * M * M + 2 * M) * 8 * rows
-        emit({"workload": f"FP64 block tridiagonal M={M}, N=256, P=32,768: forward",
+        emit({"workload": f"FP64 block tridiagonal M={M}, N=256, P={P}: forward",
               "ms": round(ms, 4), "gbs": round(fwd_b / (ms * 1e-3) / 1e9, 1),
               "bytes_per_block_row": (3 * M * M + 2 * M) * 8})
         w = torch.randn_like(dv)
         msa = timed(lambda: btsv_adjoint(A, B, C, x, w))
         adj_b = (6 * M * M + 3 * M) * 8 * rows
-        emit({"workload": f"FP64 block tridiagonal M={M}, N=256, P=32,768: adjoint",
+        emit({"workload": f"FP64 block tridiagonal M={M}, N=256, P={P}: adjoint",
               "ms": round(msa, 4), "gbs": round(adj_b / (msa * 1e-3) / 1e9, 1),
               "bytes_per_block_row": (6 * M * M + 3 * M) * 8})
         del A, B, C, dv, x, w
@@ -610,6 +615,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--suite", action="store_true",
                     help="instead: one JSON line per other workload of the path (1 GPU)")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="--suite: fraction of each workload's systems (profiling runs)")
     args = ap.parse_args()
     if args.suite:
         run_suite(args)

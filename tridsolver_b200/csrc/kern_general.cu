@@ -27,7 +27,8 @@
 //    transposed coefficients are read in place (no shifted copies), and the
 //    gradients are formed in the same pass.
 //
-// Layouts: axis 0 (unit stride, one warp per system block) and strided axes
+// Layouts: axis 0 (unit stride, one warp per system block, rows staged in
+// shared memory by coalesced copies) and strided axes
 // (SB adjacent systems per CTA, thread = (system, chunk), interface rows
 // transposed through shared memory so one warp solves one system's block).
 #include "partition.cuh"
@@ -144,25 +145,154 @@ __device__ __forceinline__ void block_step(const GenArgs<T> &A, int64_t sys, int
 }
 
 // --------------------------------------------------------------- axis 0 --
+// One warp per block of 32*M rows.  The block's rows arrive in the warp's
+// own shared-memory regions by coalesced cp.async (row q of the block at
+// q + q/M: one pad element per chunk, so that lane L reading its rows
+// L*M .. L*M+M-1 hits 32 distinct banks); results leave the same way.  The
+// adjoint mode stages a, b, c, w and u; neighbours across the block edge
+// (c_{r-1} for the first row, a_{r+1} for the last, u on both sides) are
+// single global loads.
+template <typename T>
+__device__ __forceinline__ void gx_cp_async(T *dst, const T *src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int sz = valid ? (int)sizeof(T) : 0;  // 0: zero-fill, nothing read
+  if (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(sz)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(sz)
+                 : "memory");
+}
+
+template <int M>
+__device__ __forceinline__ int gx_pidx(int q) {
+  return q + q / M;
+}
+
+template <int MODE>
+constexpr int gx_regions() {
+  return MODE == kAdj ? 5 : 4;
+}
+
 template <typename T, int M, int MODE, int PHASE>
 __global__ void __launch_bounds__(128) gen_x_kernel(Geom g, GenArgs<T> A) {
+  extern __shared__ __align__(16) unsigned char gx_dyn[];
+  constexpr int R = 32 * (M + 1);  // elements per region
+  constexpr int NR = gx_regions<MODE>();
   const int lane = threadIdx.x & (kWarp - 1);
-  const int64_t item = (int64_t)blockIdx.x * (blockDim.x / kWarp) + (threadIdx.x / kWarp);
+  const int wi = threadIdx.x / kWarp;
+  const int64_t item = (int64_t)blockIdx.x * (blockDim.x / kWarp) + wi;
   const int64_t sys = item / A.nblk;
   const int blk = (int)(item % A.nblk);
-  if (sys >= g.nsys) return;  // uniform per warp
+  if (sys >= g.nsys) return;  // uniform per warp; the kernel has no CTA barriers
   int64_t off[5];
   system_offsets(g, sys, off);
-  const int rbase = blk * 32 * M + lane * M;
+  const int n = g.n;
+  const int wb = blk * 32 * M;  // first row of the block
+  T *reg = reinterpret_cast<T *>(gx_dyn) + (size_t)wi * NR * R;
+  T *sa = reg, *sb = reg + R, *sc = reg + 2 * R, *sd = reg + 3 * R, *su = reg + 4 * R;
+  const T *pa = A.a + off[kA], *pb = A.b + off[kB], *pc = A.c + off[kC];
+  const T *pd = A.rhs + off[kD];
+  const T *pu = (MODE == kAdj) ? A.usol + off[kU] : nullptr;
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int q = j * kWarp + lane;
+    const int r = wb + q;
+    const bool in = r < n;
+    const int s = gx_pidx<M>(q);
+    gx_cp_async(sa + s, in ? pa + r : pa, in);
+    gx_cp_async(sb + s, in ? pb + r : pb, in);
+    gx_cp_async(sc + s, in ? pc + r : pc, in);
+    gx_cp_async(sd + s, in ? pd + r : pd, in);
+    if (MODE == kAdj) gx_cp_async(su + s, in ? pu + r : pu, in);
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncwarp();
+
+  const int rbase = wb + lane * M;
+  const int ts = lane * (M + 1);  // this lane's rows in every region
   T al[M], be[M], ga[M], de[M];
-  load_rows<T, M, MODE>(A, off, g, rbase, true, al, be, ga, de);
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int r = rbase + j;
+    const bool in = r < n;
+    be[j] = in ? sb[ts + j] : T(1);
+    de[j] = sd[ts + j];  // zero-filled past n
+    if (MODE == kAdj) {
+      // transposed rows: sub-diagonal c_{r-1}, super-diagonal a_{r+1}
+      T cm = T(0), ap = T(0);
+      if (in && r > 0) cm = (j > 0) ? sc[ts + j - 1] : (lane > 0 ? sc[ts - 2] : pc[r - 1]);
+      if (r + 1 < n) ap = (j < M - 1) ? sa[ts + j + 1] : (lane < kWarp - 1 ? sa[ts + M + 1] : pa[r + 1]);
+      al[j] = cm;
+      ga[j] = ap;
+    } else {
+      al[j] = (in && r > 0) ? sa[ts + j] : T(0);
+      ga[j] = (r < n - 1) ? sc[ts + j] : T(0);
+    }
+  }
   Row<T> F, L;
   chunk_reduce<T, M>(al, be, ga, de, F, L);
   T xF, xL;
   block_step<T, PHASE>(A, sys, blk, g.nsys, F, L, lane, xF, xL);
   if (PHASE == kReduce) return;
   chunk_backsub<T, M>(al, ga, de, xF, xL);
-  store_rows<T, M, MODE>(A, off, g, rbase, de);
+
+  // out through this warp's regions: value v_j of this lane's rows into
+  // region k, then coalesced stores of rows wb .. wb+32M-1
+  auto put = [&](T *rg, const T(&v)[M]) {
+#pragma unroll
+    for (int j = 0; j < M; ++j) rg[ts + j] = v[j];
+  };
+  auto flush = [&](const T *rg, T *p, bool add) {
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int q = j * kWarp + lane;
+      if (wb + q < n) {
+        if (add)
+          p[wb + q] += rg[gx_pidx<M>(q)];
+        else
+          p[wb + q] = rg[gx_pidx<M>(q)];
+      }
+    }
+  };
+  if constexpr (MODE == kFwd || MODE == kFwdInc) {
+    put(sd, de);  // d was read only by this lane
+    flush(sd, A.out + (MODE == kFwd ? off[kD] : off[kU]), MODE == kFwdInc);
+  } else {
+  // gradients: g = de; u_{r-1}, u_r, u_{r+1} from the staged u
+  T uu[M];
+#pragma unroll
+  for (int j = 0; j < M; ++j) uu[j] = su[ts + j];
+  const T uprev = (rbase > 0 && rbase - 1 < n) ? (lane > 0 ? su[ts - 2] : pu[rbase - 1]) : T(0);
+  const T unext = (rbase + M < n) ? (lane < kWarp - 1 ? su[ts + M + 1] : pu[rbase + M]) : T(0);
+  __syncwarp();  // every lane has read its neighbours' a, c and u slots
+  T v[M];
+  if (A.ga) {
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+      v[j] = (rbase + j > 0) ? -de[j] * (j > 0 ? uu[j - 1] : uprev) : T(0);
+    put(sa, v);
+    flush(sa, A.ga + off[kA], false);
+  }
+  if (A.gb) {
+#pragma unroll
+    for (int j = 0; j < M; ++j) v[j] = -de[j] * uu[j];
+    put(sb, v);
+    flush(sb, A.gb + off[kB], false);
+  }
+  if (A.gc) {
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+      v[j] = (rbase + j + 1 < n) ? -de[j] * (j < M - 1 ? uu[j + 1] : unext) : T(0);
+    put(sc, v);
+    flush(sc, A.gc + off[kC], false);
+  }
+  if (A.gd) {
+    put(sd, de);
+    flush(sd, A.gd + off[kD], false);
+  }
+  }
 }
 
 // --------------------------------------------------------- strided axes --
@@ -217,7 +347,19 @@ static cudaError_t go_x(const Geom &g, const GenArgs<T> &A, cudaStream_t st) {
   const int64_t items = g.nsys * A.nblk;
   const int64_t blocks = (items + kW - 1) / kW;
   if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
-  gen_x_kernel<T, M, MODE, PHASE><<<dim3((unsigned)blocks), dim3(kW * kWarp), 0, st>>>(g, A);
+  const int smem = kW * gx_regions<MODE>() * 32 * (M + 1) * (int)sizeof(T);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 64) return cudaErrorNotSupported;
+  static bool attr_set[64] = {};  // per device
+  if (!attr_set[dev]) {
+    e = cudaFuncSetAttribute(gen_x_kernel<T, M, MODE, PHASE>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    attr_set[dev] = true;
+  }
+  gen_x_kernel<T, M, MODE, PHASE><<<dim3((unsigned)blocks), dim3(kW * kWarp), smem, st>>>(g, A);
   return cudaGetLastError();
 }
 
