@@ -161,8 +161,8 @@ TRID_EXTERN_C tridStatus_t tridSmtsvVarlenBatch(const float *a, const float *b, 
  * but every scratch byte comes from one fixed 32 MiB array per device that
  * the library holds from load to process exit; no call allocates.
  * Limit: the work space must fit in 32 MiB, roughly
- *   12*(nsys+1) + 64*(nsys + total/256 + 1) bytes plus alignment
- * (e.g. 100,000 systems with up to 100 million rows in total); larger
+ *   20*(nsys+1) + 72*(nsys + total/256 + 1) bytes plus alignment
+ * (e.g. 100,000 systems with up to 80 million rows in total); larger
  * problems return TRID_STATUS_INVALID_VALUE and should use
  * tridDmtsvVarlenBatch.
  * The first call on each device looks up the array's device address (a

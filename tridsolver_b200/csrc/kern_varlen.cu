@@ -1,78 +1,193 @@
 // Variable-length packed batch: one persistent launch (sm_100a).
 //
 // System s occupies rows [offsets[s], offsets[s+1]) of every array (unit
-// stride, int64 offsets).  Work items:
-//   * a system of at most 256 rows is one item, solved whole by one warp with
-//     the partitioned Thomas of partition.cuh; the rows-per-lane chunk M is
-//     picked per item from the length (2/4/8: the length buckets);
-//   * a longer system (up to 32 blocks of 256 rows = 8192 rows) is one item
-//     per block.  A warp reduces its block to the block's two boundary rows
-//     (warp_block_basis / block_rows), publishes them, and counts the block
-//     done on the system's atomic counter; the warp that completes the count
-//     solves the system's block system (2 rows per block, one warp interface
-//     solve) and then finishes every block of the system (back-substitution
-//     from the block's boundary unknowns).  Nothing ever waits on another
-//     warp: completion is detected by the counter, never polled.
-// Warps take items from one atomic queue in system order.
+// stride, int64 offsets).  Two work queues in system order, served by the
+// same persistent warps one after the other:
+//   * the reduce queue: a system of at most 256 rows is one item, solved
+//     whole by one warp with the partitioned Thomas of partition.cuh, the
+//     rows-per-lane chunk M picked from the length (2/4/8: the length
+//     buckets); a longer system (up to 32 blocks of 256 rows = 8192 rows)
+//     gives one item per block: the warp reduces its block to the block's two
+//     boundary rows (warp_block_basis / block_rows), publishes them and counts
+//     the block done on the system's counter; the warp that completes the
+//     count solves the system's block system (2 rows per block, one warp
+//     interface solve), publishes the block boundary unknowns and marks the
+//     system solved.  Nothing waits in this phase.
+//   * the finish queue (taken once the reduce queue is empty): one item per
+//     block of a long system; the warp reduces the block again and
+//     back-substitutes from the block's boundary unknowns.  Its system was
+//     marked solved long ago except for the last few systems, whose reduce
+//     items are held by running warps; for those the warp polls the mark a
+//     bounded number of times (a timeout is recorded in the device error
+//     word and the block skipped).
+// Items map to their system through per-item tables built beforehand.
+// Rows reach each warp's shared-memory regions by coalesced cp.async (row q
+// of the 32*M at q + q/M, conflict-free for the lane-per-chunk reads) and
+// leave by coalesced stores.  Long systems move their rows twice (reduce,
+// finish): 72 bytes per FP64 unknown, like the blocked partition of
+// kern_general.cu.
 //
-// varlen_prep (one CTA) turns offsets into the item prefix sums and clears
-// the queue and the per-system counters.  Malformed offsets (decreasing or
-// past `total`) and systems longer than 8192 rows are skipped and recorded in
-// the device error word (bits 4 and 8).
+// Three preparation launches (launch_varlen_prep) turn offsets into the
+// prefix sums and item tables of both queues and clear the queues and the
+// per-system counters.
+// Malformed offsets (decreasing or past `total`) and systems longer than
+// 8192 rows are skipped and recorded in the device error word (bits 4 and 8).
 #include <mutex>
 
 #include "partition.cuh"
+#include "tma.cuh"
 
 namespace tridb200 {
 
 constexpr int kVLBlock = 256;   // rows per block of a long system (M = 8)
 constexpr int kVLShort = 256;   // longest system solved as one item
 constexpr int kVLMaxBlocks = 32;
+constexpr int kVLWarps = 8;     // warps per CTA
+constexpr int kVLRegion = 32 * (8 + 1);  // elements per staged array and warp
 constexpr unsigned kErrBadOffsets = 4u;
 constexpr unsigned kErrTooLong = 8u;
+constexpr unsigned kVLSolved = 0x80000000u;  // sys_count flag: block solution published
+constexpr uint32_t kVLMaxIdle = 1u << 22;    // finish-queue polls after the reduce queue ran dry
 
+__device__ __forceinline__ bool vl_bad(int64_t lo, int64_t hi, int64_t total) {
+  return hi < lo || lo < 0 || hi > total;
+}
+
+// reduce items of a system of len rows
 __device__ __forceinline__ int64_t vl_items(int64_t len) {
   if (len <= kVLShort) return 1;
   return (len + kVLBlock - 1) / kVLBlock;
 }
 
-// Exclusive prefix of items per system into item_off[0..nsys]; clears queue
-// and counters.  One CTA of 1024 threads.
-__global__ void __launch_bounds__(1024) varlen_prep(const int64_t *__restrict__ offsets, int64_t nsys,
-                                                    int64_t total, int64_t *__restrict__ item_off,
-                                                    unsigned *__restrict__ sys_count,
-                                                    unsigned long long *__restrict__ queue) {
-  __shared__ int64_t part[1024];
+// finish items: one per block of a long system that can be solved
+__device__ __forceinline__ int64_t vl_fitems(int64_t len) {
+  if (len <= kVLShort) return 0;
+  const int64_t nb = (len + kVLBlock - 1) / kVLBlock;
+  return nb <= kVLMaxBlocks ? nb : 0;
+}
+
+// Preparation, three short launches over the systems (256 per CTA):
+//   count: reduce and finish items per CTA of systems -> bsum;
+//   scan : one CTA, exclusive prefix of bsum; totals; clears both queues;
+//   fill : per system, its prefixes item_off/fitem_off (CTA scan + the CTA's
+//          prefix), its counter cleared, and the system index written into
+//          the item tables item_sys/fitem_sys for each of its items.
+constexpr int kPrepThreads = 256;
+
+__device__ __forceinline__ void vl_counts(const int64_t *offsets, int64_t nsys, int64_t total,
+                                          int64_t s, int64_t &ni, int64_t &nf) {
+  ni = nf = 0;
+  if (s >= nsys) return;
+  int64_t len = offsets[s + 1] - offsets[s];
+  if (vl_bad(offsets[s], offsets[s + 1], total)) len = 0;
+  ni = vl_items(len > 0 ? len : 1);
+  nf = vl_fitems(len);
+}
+
+// inclusive sum over the CTA of v (blockDim.x == kPrepThreads); returns it
+__device__ __forceinline__ int64_t vl_cta_scan(int64_t v, int64_t *warp_tot) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t u = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += u;
+  }
+  if (lane == 31) warp_tot[w] = v;
+  __syncthreads();
+  int64_t add = 0;
+  for (int k = 0; k < w; ++k) add += warp_tot[k];
+  __syncthreads();
+  return v + add;
+}
+
+__global__ void __launch_bounds__(kPrepThreads) varlen_prep_count(const int64_t *__restrict__ offsets,
+                                                                  int64_t nsys, int64_t total,
+                                                                  int64_t *__restrict__ bsum) {
+  __shared__ int64_t wt[kPrepThreads / 32];
+  const int64_t s = (int64_t)blockIdx.x * kPrepThreads + threadIdx.x;
+  int64_t ni, nf;
+  vl_counts(offsets, nsys, total, s, ni, nf);
+  const int64_t ci = vl_cta_scan(ni, wt);
+  const int64_t cf = vl_cta_scan(nf, wt);
+  if (threadIdx.x == kPrepThreads - 1) {
+    bsum[2 * blockIdx.x] = ci;
+    bsum[2 * blockIdx.x + 1] = cf;
+  }
+}
+
+__global__ void __launch_bounds__(1024) varlen_prep_scan(int64_t *__restrict__ bsum, int64_t nblocks,
+                                                         int64_t nsys, int64_t *__restrict__ item_off,
+                                                         int64_t *__restrict__ fitem_off,
+                                                         unsigned long long *__restrict__ queue) {
+  __shared__ int64_t part[1024], fpart[1024];
   const int tid = threadIdx.x;
-  const int64_t per = (nsys + 1023) / 1024;
-  const int64_t s0 = tid * per, s1 = (s0 + per < nsys) ? s0 + per : nsys;
-  int64_t acc = 0;
-  for (int64_t s = s0; s < s1; ++s) {
-    int64_t len = offsets[s + 1] - offsets[s];
-    if (len < 0 || offsets[s] < 0 || offsets[s + 1] > total) len = 0;
-    acc += vl_items(len > 0 ? len : 1);
-    sys_count[s] = 0u;
+  const int64_t per = (nblocks + 1023) / 1024;
+  const int64_t b0 = tid * per, b1 = (b0 + per < nblocks) ? b0 + per : nblocks;
+  int64_t acc = 0, facc = 0;
+  for (int64_t b = b0; b < b1; ++b) {
+    acc += bsum[2 * b];
+    facc += bsum[2 * b + 1];
   }
   part[tid] = acc;
+  fpart[tid] = facc;
   __syncthreads();
   if (tid == 0) {
-    int64_t run = 0;
+    int64_t run = 0, frun = 0;
     for (int k = 0; k < 1024; ++k) {
-      const int64_t v = part[k];
+      const int64_t v = part[k], fv = fpart[k];
       part[k] = run;
+      fpart[k] = frun;
       run += v;
+      frun += fv;
     }
     item_off[nsys] = run;
-    *queue = 0ull;
+    fitem_off[nsys] = frun;
+    queue[0] = 0ull;
+    queue[1] = 0ull;
   }
   __syncthreads();
-  int64_t run = part[tid];
-  for (int64_t s = s0; s < s1; ++s) {
-    item_off[s] = run;
-    int64_t len = offsets[s + 1] - offsets[s];
-    if (len < 0 || offsets[s] < 0 || offsets[s + 1] > total) len = 0;
-    run += vl_items(len > 0 ? len : 1);
+  int64_t run = part[tid], frun = fpart[tid];
+  for (int64_t b = b0; b < b1; ++b) {
+    const int64_t v = bsum[2 * b], fv = bsum[2 * b + 1];
+    bsum[2 * b] = run;
+    bsum[2 * b + 1] = frun;
+    run += v;
+    frun += fv;
   }
+}
+
+__global__ void __launch_bounds__(kPrepThreads) varlen_prep_fill(
+    const int64_t *__restrict__ offsets, int64_t nsys, int64_t total,
+    const int64_t *__restrict__ bsum, int64_t *__restrict__ item_off,
+    int64_t *__restrict__ fitem_off, int *__restrict__ item_sys, int *__restrict__ fitem_sys,
+    unsigned *__restrict__ sys_count) {
+  __shared__ int64_t wt[kPrepThreads / 32];
+  const int64_t s = (int64_t)blockIdx.x * kPrepThreads + threadIdx.x;
+  int64_t ni, nf;
+  vl_counts(offsets, nsys, total, s, ni, nf);
+  const int64_t ri = bsum[2 * blockIdx.x] + vl_cta_scan(ni, wt) - ni;
+  const int64_t rf = bsum[2 * blockIdx.x + 1] + vl_cta_scan(nf, wt) - nf;
+  if (s >= nsys) return;
+  item_off[s] = ri;
+  fitem_off[s] = rf;
+  sys_count[s] = 0u;
+  for (int64_t k = 0; k < ni; ++k) item_sys[ri + k] = (int)s;
+  for (int64_t k = 0; k < nf; ++k) fitem_sys[rf + k] = (int)s;
+}
+
+// the three preparation launches; bsum holds 2*ceil(nsys/256) int64
+static cudaError_t launch_varlen_prep(const int64_t *offsets, int64_t nsys, int64_t total,
+                                      int64_t *bsum, int64_t *item_off, int64_t *fitem_off,
+                                      int *item_sys, int *fitem_sys, unsigned *sys_count,
+                                      unsigned long long *queue, cudaStream_t st) {
+  const int64_t nb = (nsys + kPrepThreads - 1) / kPrepThreads;
+  if (nb > 0x7fffffff) return cudaErrorInvalidValue;
+  varlen_prep_count<<<(unsigned)nb, kPrepThreads, 0, st>>>(offsets, nsys, total, bsum);
+  varlen_prep_scan<<<1, 1024, 0, st>>>(bsum, nb, nsys, item_off, fitem_off, queue);
+  varlen_prep_fill<<<(unsigned)nb, kPrepThreads, 0, st>>>(offsets, nsys, total, bsum, item_off,
+                                                          fitem_off, item_sys, fitem_sys,
+                                                          sys_count);
+  return cudaGetLastError();
 }
 
 template <typename T>
@@ -80,91 +195,136 @@ struct VLArgs {
   const T *a, *b, *c;
   T *d;
   const int64_t *offsets;
-  const int64_t *item_off;
+  const int64_t *item_off;   // reduce-queue prefix, nsys+1
+  const int64_t *fitem_off;  // finish-queue prefix, nsys+1
+  const int *item_sys;       // system of every reduce item
+  const int *fitem_sys;      // system of every finish item
   int64_t nsys;
   int64_t total;
   unsigned *sys_count;
-  unsigned long long *queue;
-  T *rows;       // block rows: item index * 8
+  unsigned long long *queue;  // [0] reduce queue, [1] finish queue
+  T *rows;       // per reduce item: the block's 8 row values; later its 2 unknowns
   unsigned *err;
 };
 
+__device__ __forceinline__ void vl_cp_async(void *dst, const void *src, bool valid, int bytes) {
+  const unsigned dd = (unsigned)__cvta_generic_to_shared(dst);
+  const int sz = valid ? bytes : 0;  // 0: zero-fill, nothing read
+  if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dd), "l"(src), "r"(sz)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dd), "l"(src), "r"(sz)
+                 : "memory");
+}
+
+// rows rb .. rb+32M-1 of a system (clipped to len) into the warp's four
+// regions, then this lane's rows rb+lane*M+j, transposed
 template <typename T, int M>
-__device__ __forceinline__ void vl_load(const VLArgs<T> &A, int64_t lo, int64_t len, int64_t r0,
-                                        T (&al)[M], T (&be)[M], T (&ga)[M], T (&de)[M]) {
+__device__ __forceinline__ void vl_load(const VLArgs<T> &A, T *reg, int64_t lo, int64_t rb,
+                                        int64_t len, int lane, T (&al)[M], T (&be)[M], T (&ga)[M],
+                                        T (&de)[M]) {
+  const T *src[4] = {A.a + lo, A.b + lo, A.c + lo, A.d + lo};
+  __syncwarp();  // the previous item's reads of the regions are done
 #pragma unroll
   for (int j = 0; j < M; ++j) {
-    const int64_t r = r0 + j;
-    if (r < len) {
-      al[j] = (r == 0) ? T(0) : A.a[lo + r];
-      be[j] = A.b[lo + r];
-      ga[j] = (r == len - 1) ? T(0) : A.c[lo + r];
-      de[j] = A.d[lo + r];
-    } else {
-      al[j] = T(0);
-      be[j] = T(1);
-      ga[j] = T(0);
-      de[j] = T(0);
-    }
+    const int q = j * kWarp + lane;
+    const int64_t r = rb + q;
+    const bool in = r < len;
+    const int sq = q + q / M;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      vl_cp_async(reg + k * kVLRegion + sq, in ? src[k] + r : src[k], in, (int)sizeof(T));
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncwarp();
+  const int ts = lane * (M + 1);
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int64_t r = rb + lane * M + j;
+    const bool in = r < len;
+    al[j] = (in && r > 0) ? reg[ts + j] : T(0);
+    be[j] = in ? reg[kVLRegion + ts + j] : T(1);
+    ga[j] = (r < len - 1) ? reg[2 * kVLRegion + ts + j] : T(0);
+    de[j] = reg[3 * kVLRegion + ts + j];  // zero-filled past len
   }
 }
 
+// this lane's solution rows through the d region, coalesced to d
 template <typename T, int M>
-__device__ __forceinline__ void vl_short(const VLArgs<T> &A, int64_t lo, int64_t len, int lane) {
+__device__ __forceinline__ void vl_store(const VLArgs<T> &A, T *reg, int64_t lo, int64_t rb,
+                                         int64_t len, int lane, const T (&x)[M]) {
+  T *rd = reg + 3 * kVLRegion;
+  const int ts = lane * (M + 1);
+#pragma unroll
+  for (int j = 0; j < M; ++j) rd[ts + j] = x[j];  // d slots read only by this lane
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int q = j * kWarp + lane;
+    if (rb + q < len) A.d[lo + rb + q] = rd[q + q / M];
+  }
+  __syncwarp();  // the regions are reused by the warp's next item
+}
+
+template <typename T, int M>
+__device__ __forceinline__ void vl_short(const VLArgs<T> &A, T *reg, int64_t lo, int64_t len,
+                                         int lane) {
   T al[M], be[M], ga[M], de[M];
-  const int64_t r0 = (int64_t)lane * M;
-  vl_load<T, M>(A, lo, len, r0, al, be, ga, de);
+  vl_load<T, M>(A, reg, lo, 0, len, lane, al, be, ga, de);
   Row<T> F, L;
   chunk_reduce<T, M>(al, be, ga, de, F, L);
   T xF, xL;
   warp_interface_solve(F, L, xF, xL, lane);
   chunk_backsub<T, M>(al, ga, de, xF, xL);
-#pragma unroll
-  for (int j = 0; j < M; ++j)
-    if (r0 + j < len) A.d[lo + r0 + j] = de[j];
+  vl_store<T, M>(A, reg, lo, 0, len, lane, de);
 }
 
 // one block of a long system: chunk reduction + block basis
 template <typename T>
-__device__ __forceinline__ void vl_block(const VLArgs<T> &A, int64_t lo, int64_t len, int blk,
-                                         int lane, T (&al)[8], T (&ga)[8], T (&de)[8], Row<T> &F,
-                                         Row<T> &L, T (&bF)[3], T (&bL)[3]) {
+__device__ __forceinline__ void vl_block(const VLArgs<T> &A, T *reg, int64_t lo, int64_t len,
+                                         int blk, int lane, T (&al)[8], T (&ga)[8], T (&de)[8],
+                                         Row<T> &F, Row<T> &L, T (&bF)[3], T (&bL)[3]) {
   T be[8];
-  vl_load<T, 8>(A, lo, len, (int64_t)blk * kVLBlock + lane * 8, al, be, ga, de);
+  vl_load<T, 8>(A, reg, lo, (int64_t)blk * kVLBlock, len, lane, al, be, ga, de);
   chunk_reduce<T, 8>(al, be, ga, de, F, L);
   warp_block_basis(F, L, lane, bF, bL);
 }
 
+__device__ __forceinline__ unsigned vl_load_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 template <typename T>
-__global__ void __launch_bounds__(256, 2) varlen_kernel(VLArgs<T> A) {
+__global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
+  extern __shared__ __align__(16) unsigned char vl_dyn[];
   const int lane = threadIdx.x & (kWarp - 1);
+  T *reg = reinterpret_cast<T *>(vl_dyn) + (size_t)(threadIdx.x / kWarp) * 4 * kVLRegion;
   const int64_t nitems = A.item_off[A.nsys];
+  const int64_t nf = A.fitem_off[A.nsys];
+  // ---- reduce queue ----
   for (;;) {
     unsigned long long it = 0;
-    if (lane == 0) it = atomicAdd(A.queue, 1ull);
+    if (lane == 0) it = atomicAdd(&A.queue[0], 1ull);
     it = __shfl_sync(0xffffffffu, it, 0);
     if ((int64_t)it >= nitems) break;
-    // system of this item: last s with item_off[s] <= it
-    int64_t lo_s = 0, hi_s = A.nsys;  // item_off[lo_s] <= it < item_off[hi_s]
-    while (hi_s - lo_s > 1) {
-      const int64_t mid = (lo_s + hi_s) / 2;
-      if (A.item_off[mid] <= (int64_t)it) lo_s = mid; else hi_s = mid;
-    }
-    const int64_t s = lo_s;
+    const int64_t s = A.item_sys[it];
     const int64_t lo = A.offsets[s], hi = A.offsets[s + 1];
     const int64_t len = hi - lo;
-    if (len < 0 || lo < 0 || hi > A.total) {
+    if (vl_bad(lo, hi, A.total)) {
       if (lane == 0) atomicOr(A.err, kErrBadOffsets);
       continue;
     }
     if (len == 0) continue;
     if (len <= kVLShort) {
       if (len <= 64)
-        vl_short<T, 2>(A, lo, len, lane);
+        vl_short<T, 2>(A, reg, lo, len, lane);
       else if (len <= 128)
-        vl_short<T, 4>(A, lo, len, lane);
+        vl_short<T, 4>(A, reg, lo, len, lane);
       else
-        vl_short<T, 8>(A, lo, len, lane);
+        vl_short<T, 8>(A, reg, lo, len, lane);
       continue;
     }
     const int nblk = (int)((len + kVLBlock - 1) / kVLBlock);
@@ -175,7 +335,7 @@ __global__ void __launch_bounds__(256, 2) varlen_kernel(VLArgs<T> A) {
     const int blk = (int)((int64_t)it - A.item_off[s]);
     T al[8], ga[8], de[8], bF[3], bL[3];
     Row<T> F, L, FB, LB;
-    vl_block<T>(A, lo, len, blk, lane, al, ga, de, F, L, bF, bL);
+    vl_block<T>(A, reg, lo, len, blk, lane, al, ga, de, F, L, bF, bL);
     block_rows(F, L, bF, bL, lane, FB, LB);
     T *rw = A.rows + ((int64_t)A.item_off[s] + blk) * 8;
     if (lane == 0) {
@@ -189,7 +349,7 @@ __global__ void __launch_bounds__(256, 2) varlen_kernel(VLArgs<T> A) {
     if (done != (unsigned)(nblk - 1)) continue;
     __threadfence();  // every block's rows are visible to this warp now
     // the block system of s: lane t holds block t's two rows
-    const T *rs = A.rows + (int64_t)A.item_off[s] * 8;
+    T *rs = A.rows + (int64_t)A.item_off[s] * 8;
     Row<T> RF{T(0), T(1), T(0), T(0)}, RL{T(0), T(1), T(0), T(0)};
     if (lane < nblk) {
       const T *q = rs + (int64_t)lane * 8;
@@ -197,35 +357,103 @@ __global__ void __launch_bounds__(256, 2) varlen_kernel(VLArgs<T> A) {
       RL = {__ldcg(q + 4), __ldcg(q + 5), __ldcg(q + 6), __ldcg(q + 7)};
     }
     T fB, lB;
-    warp_interface_solve(RF, RL, fB, lB, lane);
-    // finish every block of s
-    for (int t = 0; t < nblk; ++t) {
-      vl_block<T>(A, lo, len, t, lane, al, ga, de, F, L, bF, bL);
-      const T f = __shfl_sync(0xffffffffu, fB, t);
-      const T l = __shfl_sync(0xffffffffu, lB, t);
-      const T xF = bF[0] + f * bF[1] + l * bF[2];
-      const T xL = bL[0] + f * bL[1] + l * bL[2];
-      chunk_backsub<T, 8>(al, ga, de, xF, xL);
-      const int64_t r0 = (int64_t)t * kVLBlock + lane * 8;
-#pragma unroll
-      for (int j = 0; j < 8; ++j)
-        if (r0 + j < len) A.d[lo + r0 + j] = de[j];
+    int span = 1;
+    while (span < nblk) span <<= 1;
+    warp_interface_solve(RF, RL, fB, lB, lane, span);
+    __syncwarp();  // all block rows read before they are overwritten
+    if (lane < nblk) {
+      rs[(int64_t)lane * 8 + 0] = fB;  // block t's boundary unknowns
+      rs[(int64_t)lane * 8 + 1] = lB;
     }
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) atomicOr(&A.sys_count[s], kVLSolved);
   }
+  // ---- finish queue ----
+  for (;;) {
+    unsigned long long fi = 0;
+    if (lane == 0) fi = atomicAdd(&A.queue[1], 1ull);
+    fi = __shfl_sync(0xffffffffu, fi, 0);
+    if ((int64_t)fi >= nf) break;
+    const int64_t s = A.fitem_sys[fi];
+    // the system's reduce items were all taken by running warps: its mark
+    // comes; poll a bounded number of times
+    int ok = 0;
+    if (lane == 0) {
+      for (uint32_t k = 0; k < kVLMaxIdle; ++k) {
+        if (vl_load_acquire(&A.sys_count[s]) & kVLSolved) {
+          ok = 1;
+          break;
+        }
+        __nanosleep(128);
+      }
+      if (!ok) atomicOr(A.err, kErrWaitTimeout);
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    if (!ok) continue;
+    const int blk = (int)((int64_t)fi - A.fitem_off[s]);
+    const int64_t lo = A.offsets[s], len = A.offsets[s + 1] - lo;
+    T al[8], ga[8], de[8], bF[3], bL[3];
+    Row<T> F, L;
+    vl_block<T>(A, reg, lo, len, blk, lane, al, ga, de, F, L, bF, bL);
+    const T *bs = A.rows + ((int64_t)A.item_off[s] + blk) * 8;
+    const T f = __ldcg(bs), l = __ldcg(bs + 1);
+    const T xF = bF[0] + f * bF[1] + l * bF[2];
+    const T xL = bL[0] + f * bL[1] + l * bL[2];
+    chunk_backsub<T, 8>(al, ga, de, xF, xL);
+    vl_store<T, 8>(A, reg, lo, (int64_t)blk * kVLBlock, len, lane, de);
+  }
+}
+
+template <typename T>
+static int varlen_smem_bytes() {
+  return kVLWarps * 4 * kVLRegion * (int)sizeof(T);
+}
+
+// Residency of the persistent kernel on the current device (sets the
+// shared-memory attribute once per device).
+template <typename T>
+static cudaError_t varlen_grid(int &grid) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  static bool attr_set[64] = {};
+  if (!attr_set[dev]) {
+    e = cudaFuncSetAttribute(varlen_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             varlen_smem_bytes<T>());
+    if (e != cudaSuccess) return e;
+    attr_set[dev] = true;
+  }
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, varlen_kernel<T>, kVLWarps * 32,
+                                                    varlen_smem_bytes<T>()) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  grid = sms * per_sm;
+  return cudaSuccess;
 }
 
 template <typename T>
 cudaError_t launch_varlen(const T *a, const T *b, const T *c, T *d, const int64_t *offsets,
                           int64_t nsys, int64_t total, unsigned *err, cudaStream_t st) {
-  // scratch: item_off (nsys+1), sys_count (nsys), queue, block rows
+  // scratch: item_off and fitem_off (nsys+1 each), sys_count, queues, block
+  // rows (8 per item), item_sys and fitem_sys (one int per item each)
   const int64_t max_items = nsys + total / kVLBlock + 1;
   const size_t b_off = sizeof(int64_t) * (size_t)(nsys + 1);
   const size_t b_cnt = sizeof(unsigned) * (size_t)(nsys + 1);
   const size_t b_q = 64;
   const size_t b_rows = sizeof(T) * 8 * (size_t)max_items;
+  const size_t b_map = sizeof(int) * (size_t)max_items;
+  const size_t b_bsum = sizeof(int64_t) * 2 * (size_t)((nsys + kPrepThreads - 1) / kPrepThreads);
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-  unsigned char *w = (unsigned char *)scratch(al(b_off) + al(b_cnt) + al(b_q) + al(b_rows), 0);
+  unsigned char *w = (unsigned char *)scratch(
+      2 * al(b_off) + al(b_cnt) + al(b_q) + al(b_rows) + 2 * al(b_map) + al(b_bsum), 0);
   if (!w) return cudaErrorMemoryAllocation;
+  int64_t *bsum = (int64_t *)(w + 2 * al(b_off) + al(b_cnt) + al(b_q) + al(b_rows) + 2 * al(b_map));
   VLArgs<T> A;
   A.a = a;
   A.b = b;
@@ -235,20 +463,21 @@ cudaError_t launch_varlen(const T *a, const T *b, const T *c, T *d, const int64_
   A.nsys = nsys;
   A.total = total;
   A.item_off = (int64_t *)w;
-  A.sys_count = (unsigned *)(w + al(b_off));
-  A.queue = (unsigned long long *)(w + al(b_off) + al(b_cnt));
-  A.rows = (T *)(w + al(b_off) + al(b_cnt) + al(b_q));
+  A.fitem_off = (int64_t *)(w + al(b_off));
+  A.sys_count = (unsigned *)(w + 2 * al(b_off));
+  A.queue = (unsigned long long *)(w + 2 * al(b_off) + al(b_cnt));
+  A.rows = (T *)(w + 2 * al(b_off) + al(b_cnt) + al(b_q));
+  A.item_sys = (const int *)(w + 2 * al(b_off) + al(b_cnt) + al(b_q) + al(b_rows));
+  A.fitem_sys = A.item_sys + al(b_map) / sizeof(int);
   A.err = err;
-  varlen_prep<<<1, 1024, 0, st>>>(offsets, nsys, total, (int64_t *)A.item_off, A.sys_count, A.queue);
-  cudaError_t e = cudaGetLastError();
+  int grid = 0;
+  cudaError_t e = varlen_grid<T>(grid);
   if (e != cudaSuccess) return e;
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, varlen_kernel<T>, 256, 0) != cudaSuccess ||
-      per_sm < 1)
-    per_sm = 1;
-  varlen_kernel<T><<<dim3((unsigned)(sms * per_sm)), dim3(256), 0, st>>>(A);
+  e = launch_varlen_prep(offsets, nsys, total, bsum, (int64_t *)A.item_off,
+                         (int64_t *)A.fitem_off, (int *)A.item_sys, (int *)A.fitem_sys,
+                         A.sys_count, A.queue, st);
+  if (e != cudaSuccess) return e;
+  varlen_kernel<T><<<dim3((unsigned)grid), dim3(kVLWarps * 32), varlen_smem_bytes<T>(), st>>>(A);
   return cudaGetLastError();
 }
 
@@ -269,7 +498,7 @@ static tridStatus_t varlen_entry(const T *a, const T *b, const T *c, T *d, const
   if (nsys < 0 || total < 0 || !offsets || (total > 0 && (!a || !b || !c || !d)))
     return TRID_STATUS_INVALID_VALUE;
   if (nsys == 0 || total == 0) return TRID_STATUS_SUCCESS;
-  if (nsys > ((int64_t)1 << 40)) return TRID_STATUS_INVALID_VALUE;
+  if (nsys >= ((int64_t)1 << 31)) return TRID_STATUS_INVALID_VALUE;  // int item tables
   unsigned *err = device_error_flags();
   if (!err) return TRID_STATUS_ALLOC_FAILED;
   const cudaError_t e = launch_varlen<T>(a, b, c, d, offsets, nsys, total, err, current_stream());
@@ -335,14 +564,16 @@ static size_t noalloc_layout(int64_t nsys, int64_t total, size_t off[5]) {
   size_t at = 0;
   off[0] = at;  // error word
   at += 256;
-  off[1] = at;  // item_off, nsys+1 int64
-  at += al(sizeof(int64_t) * (size_t)(nsys + 1));
+  off[1] = at;  // item_off and fitem_off, nsys+1 int64 each
+  at += 2 * al(sizeof(int64_t) * (size_t)(nsys + 1));
   off[2] = at;  // sys_count, nsys+1 unsigned
   at += al(sizeof(unsigned) * (size_t)(nsys + 1));
   off[3] = at;  // queue
   at += 256;
-  off[4] = at;  // block rows, 8 per item
-  at += al(sizeof(double) * 8 * (size_t)max_items);
+  off[4] = at;  // block rows, 8 per item; then item_sys and fitem_sys; then
+                // the preparation's per-CTA sums
+  at += al(sizeof(double) * 8 * (size_t)max_items) + 2 * al(sizeof(int) * (size_t)max_items);
+  at += al(sizeof(int64_t) * 2 * (size_t)((nsys + kPrepThreads - 1) / kPrepThreads));
   return at <= kNoAllocScratchBytes ? at : 0;
 }
 
@@ -356,7 +587,7 @@ extern "C" tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const doubl
   if (nsys < 0 || total < 0 || !offsets || (total > 0 && (!a || !b || !c || !d)))
     return TRID_STATUS_INVALID_VALUE;
   if (nsys == 0 || total == 0) return TRID_STATUS_SUCCESS;
-  if (nsys > ((int64_t)1 << 40) || total > ((int64_t)1 << 46)) return TRID_STATUS_INVALID_VALUE;
+  if (nsys >= ((int64_t)1 << 31) || total > ((int64_t)1 << 46)) return TRID_STATUS_INVALID_VALUE;
   size_t off[5];
   if (noalloc_layout(nsys, total, off) == 0) return TRID_STATUS_INVALID_VALUE;  // too large
   unsigned char *w = (unsigned char *)noalloc_scratch_address();
@@ -372,23 +603,28 @@ extern "C" tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const doubl
   A.total = total;
   A.err = (unsigned *)(w + off[0]);
   A.item_off = (int64_t *)(w + off[1]);
+  A.fitem_off = (int64_t *)(w + off[1] + (off[2] - off[1]) / 2);
   A.sys_count = (unsigned *)(w + off[2]);
   A.queue = (unsigned long long *)(w + off[3]);
   A.rows = (double *)(w + off[4]);
-  // varlen_prep rewrites the prefix sums and clears the queue and counters,
-  // so whatever the previous call left in the array does not matter
-  varlen_prep<<<1, 1024, 0, st>>>(A.offsets, nsys, total, (int64_t *)A.item_off, A.sys_count,
-                                   A.queue);
-  if (cudaGetLastError() != cudaSuccess) return TRID_STATUS_EXECUTION_FAILED;
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, varlen_kernel<double>, 256, 0) !=
-          cudaSuccess ||
-      per_sm < 1) {
-    cudaGetLastError();
-    per_sm = 1;
+  int64_t *bsum = nullptr;
+  {
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const int64_t max_items = nsys + total / kVLBlock + 1;
+    A.item_sys = (const int *)(w + off[4] + al(sizeof(double) * 8 * (size_t)max_items));
+    A.fitem_sys = A.item_sys + al(sizeof(int) * (size_t)max_items) / sizeof(int);
+    bsum = (int64_t *)(w + off[4] + al(sizeof(double) * 8 * (size_t)max_items) +
+                       2 * al(sizeof(int) * (size_t)max_items));
   }
-  varlen_kernel<double><<<dim3((unsigned)(sms * per_sm)), dim3(256), 0, st>>>(A);
+  // the preparation rewrites the prefix sums and clears the queues and counters,
+  // so whatever the previous call left in the array does not matter
+  int grid = 0;
+  if (varlen_grid<double>(grid) != cudaSuccess) return TRID_STATUS_EXECUTION_FAILED;
+  if (launch_varlen_prep(A.offsets, nsys, total, bsum, (int64_t *)A.item_off,
+                         (int64_t *)A.fitem_off, (int *)A.item_sys, (int *)A.fitem_sys,
+                         A.sys_count, A.queue, st) != cudaSuccess)
+    return TRID_STATUS_EXECUTION_FAILED;
+  varlen_kernel<double><<<dim3((unsigned)grid), dim3(kVLWarps * 32), varlen_smem_bytes<double>(),
+                          st>>>(A);
   return cudaGetLastError() == cudaSuccess ? TRID_STATUS_SUCCESS : TRID_STATUS_EXECUTION_FAILED;
 }
