@@ -591,6 +591,7 @@ def run_suite(args):
     shape = (128, 128, 128)
     u0 = torch.rand(shape, dtype=torch.float64, device=dev, generator=gen)
     adi = ADI(shape, 1.0)
+    adi.grad_final_norm(u0, 4, 2)  # warm-up (library scratch, torch kernels)
     torch.cuda.synchronize()
     torch.cuda.reset_peak_memory_stats()
     base = torch.cuda.memory_allocated()
