@@ -41,7 +41,8 @@ template <typename T, int M>
 __device__ __forceinline__ void cta_solve(T (&al)[M], const T (&be)[M], T (&ga)[M], T (&de)[M],
                                           int w, int lane, int nw, T *sm) {
   Row<T> F, L;
-  chunk_reduce<T, M>(al, be, ga, de, F, L);
+  T rp[M];
+  chunk_reduce_cont<T, M>(al, be, ga, de, F, L, rp);
   cta_solve_rows<T, M>(F, L, al, ga, de, w, lane, nw, sm);
 }
 
@@ -170,8 +171,8 @@ __device__ __forceinline__ void prefetch_system_l2(const T *p, int n) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-template <typename T, int M, int MODE, int MAXW>
-__global__ void __launch_bounds__(MAXW * 32) xcta_kernel(Geom g, XArgs<T> A, int dist) {
+template <typename T, int M, int MODE>
+__device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int dist) {
   extern __shared__ __align__(16) unsigned char xcta_dyn[];
   __shared__ T sm[128 + 32 + 2 * 16];
   const int lane = threadIdx.x & (kWarp - 1);
@@ -243,7 +244,14 @@ __global__ void __launch_bounds__(MAXW * 32) xcta_kernel(Geom g, XArgs<T> A, int
     }
     if (MODE == kXFused) {
       Row<T> F, L;
-      chunk_reduce_pivots<T, M>(al, be, ga, xs, F, L, rp);
+      chunk_reduce_cont<T, M>(al, be, ga, xs, F, L, rp);
+      // the transposed reduction needs b only at the chunk's first and last
+      // rows; the interior pivots wait in this thread's own b slots (read by
+      // this thread alone), so that neither occupies registers meanwhile
+      const T b0 = be[0], bl = be[M - 1];
+      T *rbw = S.region(1, w) + lane * (M + 1);
+#pragma unroll
+      for (int j = 1; j <= M - 2; ++j) rbw[j] = rp[j];
       cta_solve_rows<T, M>(F, L, al, ga, xs, w, lane, nw, sm);
       // x into this thread's own slots of region 3 (d was read by this
       // thread alone): the neighbours x_{r-1}, x_{r+1} and the outgoing x
@@ -251,9 +259,9 @@ __global__ void __launch_bounds__(MAXW * 32) xcta_kernel(Geom g, XArgs<T> A, int
 #pragma unroll
       for (int j = 0; j < M; ++j) rx[j] = xs[j];
       // the transposed system: rows (c_{r-1}, b_r, a_{r+1}); its chunk
-      // interiors have the forward pivots rp
+      // interiors have the forward pivots
       const T *rw = S.region(4, w) + lane * (M + 1);
-      T ta[M], tg[M];
+      T ta[M], tg[M], tb[M], tp[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) {
         const int r = r0 + j;
@@ -261,8 +269,10 @@ __global__ void __launch_bounds__(MAXW * 32) xcta_kernel(Geom g, XArgs<T> A, int
         ta[j] = (in && r > 0) ? (j > 0 ? rc[j - 1] : S.row(2, r - 1)) : T(0);
         tg[j] = (r + 1 < n) ? (j < M - 1 ? ra[j + 1] : S.row(0, r + 1)) : T(0);
         gsol[j] = rw[j];  // zero-filled past n
+        tb[j] = (j == 0) ? b0 : (j == M - 1 ? bl : T(1));  // interior b unused
+        tp[j] = (j >= 1 && j <= M - 2) ? rbw[j] : T(0);
       }
-      chunk_reduce_given<T, M>(ta, be, tg, gsol, F, L, rp);
+      chunk_reduce_given<T, M>(ta, tb, tg, gsol, F, L, tp);
       cta_solve_rows<T, M>(F, L, ta, tg, gsol, w, lane, nw, sm);
     } else {
       cta_solve<T, M>(al, be, ga, xs, w, lane, nw, sm);
@@ -322,33 +332,44 @@ __global__ void __launch_bounds__(MAXW * 32) xcta_kernel(Geom g, XArgs<T> A, int
   }
 }
 
-template <typename T, int M, int MODE, int MAXW>
-static cudaError_t launch_xcta_m(const Geom &g, const XArgs<T> &A, int warps, cudaStream_t st) {
+// The kernel: register use bounded by its launch bounds (MAXW warps, MINB
+// CTAs per SM).
+template <typename T, int M, int MODE, int MAXW, int MINB>
+__global__ void __launch_bounds__(MAXW * 32, MINB) xcta_kernel(Geom g, XArgs<T> A, int dist) {
+  xcta_body<T, M, MODE>(g, A, dist);
+}
+
+template <typename T, int M, int MODE, auto kern>
+static cudaError_t launch_xcta_k(int max_warps, const Geom &g, const XArgs<T> &A, int warps,
+                                 cudaStream_t st) {
   constexpr int kArrays = (MODE == kXAdj || MODE == kXFused) ? 5 : 4;
   const size_t smem = (size_t)kArrays * warps * Stage<T, M>::R * sizeof(T);
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev >= 64) return cudaErrorNotSupported;
-  static bool attr_set[64] = {};  // per device
+  static bool attr_set[64] = {};  // per device, per kernel (one instantiation each)
   if (!attr_set[dev]) {
-    e = cudaFuncSetAttribute(xcta_kernel<T, M, MODE, MAXW>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kArrays * MAXW * Stage<T, M>::R * (int)sizeof(T));
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kArrays * max_warps * Stage<T, M>::R * (int)sizeof(T));
     if (e != cudaSuccess) return e;
     attr_set[dev] = true;
   }
   // prefetch distance: the CTAs resident on the whole GPU at once
   int per_sm = 0, sms = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xcta_kernel<T, M, MODE, MAXW>,
-                                                    warps * kWarp, smem) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * kWarp, smem) !=
+          cudaSuccess ||
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
     per_sm = 0;
     cudaGetLastError();
   }
-  xcta_kernel<T, M, MODE, MAXW><<<(unsigned)g.nsys, warps * kWarp, smem, st>>>(g, A,
-                                                                                per_sm * sms);
+  kern<<<(unsigned)g.nsys, warps * kWarp, smem, st>>>(g, A, per_sm * sms);
   return cudaGetLastError();
+}
+
+template <typename T, int M, int MODE, int MAXW, int MINB = 1>
+static cudaError_t launch_xcta_m(const Geom &g, const XArgs<T> &A, int warps, cudaStream_t st) {
+  return launch_xcta_k<T, M, MODE, xcta_kernel<T, M, MODE, MAXW, MINB>>(MAXW, g, A, warps, st);
 }
 
 template <typename T, int MODE>
@@ -366,6 +387,11 @@ cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, int chunk, cudaStream_
   if (M == 8)
     return warps <= 8 ? launch_xcta_m<T, 8, MODE, 8>(g, A, warps, st)
                       : launch_xcta_m<T, 8, MODE, 16>(g, A, warps, st);
+  // forward modes up to 1024 rows (two warps): registers capped for 6 CTAs
+  // per SM (the adjoint modes spill under such caps, and measured slower)
+  if constexpr (MODE == kXFwd || MODE == kXFwdInc) {
+    if (warps <= 2) return launch_xcta_m<T, 16, MODE, 2, 6>(g, A, warps, st);
+  }
   return launch_xcta_m<T, 16, MODE, 8>(g, A, warps, st);
 }
 

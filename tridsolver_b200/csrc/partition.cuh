@@ -113,6 +113,76 @@ __device__ __forceinline__ void chunk_reduce_pivots(T (&al)[M], const T (&be)[M]
   F.d = de[0] - ga[0] * D;
 }
 
+// 2^-e for the binary exponent e of x (x normal), else 1: multiplying by it
+// is exact and brings |x| into [1, 2)
+__device__ __forceinline__ double pow2_inv_exponent(double x) {
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(x);
+  const unsigned e = (unsigned)(bits >> 52) & 0x7ffu;
+  if (e == 0u || e >= 0x7feu) return 1.0;
+  return __longlong_as_double((long long)((unsigned long long)(2046u - e) << 52));
+}
+__device__ __forceinline__ float pow2_inv_exponent(float x) {
+  const unsigned bits = __float_as_uint(x);
+  const unsigned e = (bits >> 23) & 0xffu;
+  if (e == 0u || e >= 0xfeu) return 1.0f;
+  return __uint_as_float((254u - e) << 23);
+}
+
+// chunk_reduce_pivots with the pivots from the continuant recurrence
+//   q_1 = b_1, q_0 = 1,  q_j = b_j q_{j-1} - (a_j c_{j-1}) q_{j-2},
+//   p_j = q_j / q_{j-1}  (the leading minors of the chunk's interior block),
+// so that the serial chain carries one multiply-add per row and the
+// reciprocals 1/p_j = q_{j-1} / q_j do not wait on each other; the pair
+// (q_{j-1}, q_j) is rescaled by a power of two every 4 rows to stay in range.
+// Mathematically the same pivots as the Thomas recurrence
+// p_j = b_j - a_j c_{j-1} / p_{j-1}.
+template <typename T, int M>
+__device__ __forceinline__ void chunk_reduce_cont(T (&al)[M], const T (&be)[M], T (&ga)[M],
+                                                  T (&de)[M], Row<T> &F, Row<T> &L,
+                                                  T (&rp)[M]) {
+  static_assert(M >= 4, "chunks of at least four rows");
+  T qm2 = T(1), qm1 = be[1];
+  rp[1] = rcp(be[1]);
+#pragma unroll
+  for (int j = 2; j <= M - 2; ++j) {
+    const T q = be[j] * qm1 - (al[j] * ga[j - 1]) * qm2;
+    rp[j] = qm1 * rcp(q);
+    qm2 = qm1;
+    qm1 = q;
+    if ((j & 3) == 0) {
+      const T sc = pow2_inv_exponent(q);
+      qm1 *= sc;
+      qm2 *= sc;
+    }
+  }
+  // c' and the two right-hand-side recurrences with the pivots known
+  de[1] *= rp[1];
+  al[1] *= rp[1];
+  ga[1] *= rp[1];
+#pragma unroll
+  for (int j = 2; j <= M - 2; ++j) {
+    const T r = rp[j];
+    de[j] = (de[j] - al[j] * de[j - 1]) * r;
+    al[j] = -(al[j] * al[j - 1]) * r;
+    ga[j] = ga[j] * r;
+  }
+  T D = de[M - 2], A = al[M - 2], C = ga[M - 2];
+  L.a = -al[M - 1] * A;
+  L.b = be[M - 1] - al[M - 1] * C;
+  L.c = ga[M - 1];
+  L.d = de[M - 1] - al[M - 1] * D;
+#pragma unroll
+  for (int j = M - 3; j >= 1; --j) {
+    D = de[j] - ga[j] * D;
+    A = al[j] - ga[j] * A;
+    C = -ga[j] * C;
+  }
+  F.a = al[0];
+  F.b = be[0] - ga[0] * A;
+  F.c = -ga[0] * C;
+  F.d = de[0] - ga[0] * D;
+}
+
 // chunk_reduce with the interior's reciprocal pivots given: no divisions,
 // only multiply-add recurrences.
 template <typename T, int M>
