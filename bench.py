@@ -178,6 +178,7 @@ def run_ours(args):
     import torch
 
     import tridsolver_b200 as tb
+    from tridsolver_b200.shard import max_over_ranks
 
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
@@ -235,11 +236,8 @@ def run_ours(args):
         while time.time() < t_wall + 1.2:
             step()
             torch.cuda.synchronize()
-    ms_total = start.elapsed_time(stop)
+    ms_total = max_over_ranks(start.elapsed_time(stop))
     if dist:
-        t = torch.tensor([ms_total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
         dist.barrier()
     ms_step = ms_total / args.steps
     value = world * 3 * BYTES_PER_SOLVE / (ms_step * 1e-3) / 1e9
@@ -266,12 +264,7 @@ def run_ours(args):
         hout.copy_(td, non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_ms /= e2e_steps
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1)) / e2e_steps
     e2e_value = world * 3 * BYTES_PER_SOLVE / (e2e_ms * 1e-3) / 1e9
 
     peak, peak_kind = measured_peak()
