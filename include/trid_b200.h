@@ -230,7 +230,10 @@ TRID_EXTERN_C const char *tridGetStatusString(tridStatus_t status);
  *   method 2 = partitioned Thomas: per-thread chunks of `chunk` rows reduced to
  *              a 64-row interface system solved by warp shuffles (PCR); the
  *              rows are staged by TMA (bulk tensor copies) when the layout
- *              allows
+ *              allows.  On strided axes a tile of 128 bytes of systems (16
+ *              FP64 / 32 FP32, the default up to 256 rows) streams through
+ *              one persistent CTA per SM, the next tile's copy in flight
+ *              while the current one is solved
  *   method 3 = method 2 with plain loads only
  *   method 4 = strided axes: two-sided (twisted) Thomas, rows staged by TMA,
  *              c'/d' in shared memory (falls back to method 2 where the
@@ -246,7 +249,9 @@ TRID_EXTERN_C const char *tridGetStatusString(tridStatus_t status);
  *              513..4096 rows take method 6 with chunk 16, as do the adjoint
  *              and the forward + adjoint call from 65 rows)
  *   chunk      : rows per thread for methods 2/3 (2, 4, 8 or 16; 0 = automatic)
- *   sys_per_cta: systems per CTA for methods 2/3 on strided axes (4, 8, 16; 0 = auto)
+ *   sys_per_cta: systems per CTA for methods 2/3 on strided axes (4, 8, 16 or
+ *                32; 0 = auto; 32 applies to the FP32 streamed tiles, and
+ *                the plain-load kernels cap it at 16)
  * Applies to calls from the calling thread. */
 TRID_EXTERN_C tridStatus_t tridSetMethod(int method, int chunk, int sys_per_cta);
 

@@ -129,20 +129,18 @@ def test_method_override_and_query():
     assert (m.value, ch.value) == (2, 8)
     # long systems: blocked partition with 256-row blocks
     assert L.tridQueryMethod(8, 1, 5000, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
-    assert (m.value, ch.value) == (3, 8)
+    assert (m.value, ch.value) == (2, 8)
     assert L.tridQueryMethod(8, 0, 65536, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
     assert (m.value, ch.value) == (2, 8)
-    assert L.tridQueryMethod(8, 1, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
-    assert (m.value, ch.value, spc.value) == (3, 8, 8)
-    assert L.tridQueryMethod(8, 2, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
-    assert (m.value, ch.value, spc.value) == (2, 8, 8)
-    # strides past 1 MiB, and FP32 strided axes: plain loads, 16 systems per CTA
-    assert L.tridQueryMethod(8, 3, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
-    assert (m.value, ch.value, spc.value) == (3, 8, 16)
+    # strided axes, every stride class: streamed tiles of one 128-byte line of
+    # systems (16 FP64, 32 FP32)
     for cls in (1, 2, 3):
+        assert L.tridQueryMethod(8, cls, 256, ctypes.byref(m), ctypes.byref(ch),
+                                 ctypes.byref(spc)) == 0
+        assert (m.value, ch.value, spc.value) == (2, 8, 16)
         assert L.tridQueryMethod(4, cls, 256, ctypes.byref(m), ctypes.byref(ch),
                                  ctypes.byref(spc)) == 0
-        assert (m.value, ch.value, spc.value) == (3, 8, 16)
+        assert (m.value, ch.value, spc.value) == (2, 8, 32)
     assert L.tridQueryMethod(8, 4, 256, ctypes.byref(m), ctypes.byref(ch),
                              ctypes.byref(spc)) == INVALID
     tb.set_method(1)
@@ -156,6 +154,27 @@ def test_method_override_and_query():
         tb.set_method(2, chunk=3)
     with pytest.raises(tb.TridError):
         tb.set_method(7)
+    with pytest.raises(tb.TridError):
+        tb.set_method(2, sys_per_cta=12)
+    tb.set_method(2, sys_per_cta=32)
+    assert L.tridQueryMethod(4, 2, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+    assert (m.value, spc.value) == (2, 32)
+    tb.set_method(0)
+
+
+def test_tuning_table_rejects_bad_widths(tmp_path):
+    L = tb.lib()
+    for line in ("f64 2 256 2 8 12\n", "f64 2 256 2 3 16\n"):
+        bad = tmp_path / "bad.txt"
+        bad.write_text(line)
+        assert L.tridLoadTuningTable(str(bad).encode()) == INVALID
+    good = tmp_path / "good.txt"
+    good.write_text("f32 2 256 2 8 32\n")
+    assert L.tridLoadTuningTable(str(good).encode()) == 0
+    m, ch, spc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    assert L.tridQueryMethod(4, 2, 200, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+    assert (m.value, ch.value, spc.value) == (2, 8, 32)
+    assert L.tridLoadTuningTable(None) == 0
 
 
 def test_tuning_table_roundtrip(tmp_path):

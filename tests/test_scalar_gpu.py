@@ -147,7 +147,7 @@ def test_8d(solvedim):
 
 
 @pytest.mark.parametrize("method", [(1, 0, 0), (2, 2, 4), (2, 4, 8), (2, 8, 16), (2, 16, 4),
-                                    (2, 16, 8), (3, 8, 8), (4, 0, 0)])
+                                    (2, 16, 8), (2, 8, 32), (3, 8, 8), (3, 8, 32), (4, 0, 0)])
 @pytest.mark.parametrize("solvedim", [0, 1, 2])
 def test_forced_methods(method, solvedim):
     run_case(np.random.default_rng(3), np.float64, [30, 29, 28], solvedim, method=method)
@@ -187,16 +187,23 @@ def test_strided_tma_staged(dtype, n, solvedim):
     run_case(np.random.default_rng(n + 7 * solvedim), dtype, dims, solvedim)
 
 
-@pytest.mark.parametrize("spc", [4, 8, 16])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("spc", [4, 8, 16, 32])
 @pytest.mark.parametrize("inc", [False, True])
 @pytest.mark.parametrize("dims,solvedim,pads", [
     ([36, 70, 6], 1, [36, 72, 6]),
     ([36, 6, 70], 2, [40, 6, 70]),
     ([20, 3, 50, 4], 2, [24, 3, 50, 4]),
     ([16, 2, 3, 41, 2], 3, None),
+    ([72, 150, 33], 2, [80, 150, 33]),    # many more tiles than CTAs, partial last x tile
+    ([96, 40, 256], 2, None),             # n = 256: full 128-byte tiles, several per CTA
+    ([64, 129, 7, 3], 1, None),           # rank 4, odd n
 ])
-def test_strided_tma_spc_inc_padded(spc, inc, dims, solvedim, pads):
-    run_case(np.random.default_rng(spc + inc), np.float64, dims, solvedim, pads=pads, inc=inc,
+def test_strided_tma_spc_inc_padded(dtype, spc, inc, dims, solvedim, pads):
+    """Every systems-per-CTA width of the TMA-staged strided kernels; full-line
+    widths (16 FP64 / 32 FP32 systems) run the persistent streamed form, which
+    loops over several tiles per CTA in the larger cases."""
+    run_case(np.random.default_rng(spc + inc), dtype, dims, solvedim, pads=pads, inc=inc,
              method=(2, 0, spc))
 
 

@@ -99,7 +99,7 @@ def test_sharded_solve_matches_whole_batch(dtype, world):
     import tridsolver_b200 as tb
 
     tdt = getattr(torch, dtype)
-    fn = tb.tridDmtsvStridedBatchPadded if dtype == "float64" else tb.tridSmtsvStridedBatchPadded
+    fn = tb.tridDmtsvStridedBatch if dtype == "float64" else tb.tridSmtsvStridedBatch
     tol = 1e-12 if dtype == "float64" else 1e-5
     gen = torch.Generator().manual_seed(7)
     for dims, pads, sd in GPU_LAYOUTS:

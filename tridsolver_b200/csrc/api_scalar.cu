@@ -92,7 +92,10 @@ static tridStatus_t parse_tuning_table(const char *path, std::vector<TuneEntry> 
       return TRID_STATUS_INVALID_VALUE;
     }
     e.dtype_bytes = (strcmp(dt, "f64") == 0) ? 8 : (strcmp(dt, "f32") == 0 ? 4 : 0);
-    if (e.dtype_bytes == 0 || e.method < 1 || e.method > 6 || e.axis < 0 || e.axis > 3) {
+    const bool chunk_ok = e.chunk == 0 || e.chunk == 2 || e.chunk == 4 || e.chunk == 8 || e.chunk == 16;
+    const bool spc_ok = e.spc == 0 || e.spc == 4 || e.spc == 8 || e.spc == 16 || e.spc == 32;
+    if (e.dtype_bytes == 0 || e.method < 1 || e.method > 6 || e.axis < 0 || e.axis > 3 ||
+        !chunk_ok || !spc_ok) {
       fclose(f);
       return TRID_STATUS_INVALID_VALUE;
     }
@@ -144,19 +147,28 @@ MethodChoice choose_method(int dtype_bytes, int axis, int n, int opt_hint) {
   }
   if (m.method == 0) {
     // built-in defaults, from the B200 sweeps of tridsolver_b200.autotune:
-    // TMA staging wins on axis 0 and, in FP64, on strides of 64 KiB..1 MiB;
-    // plain coalesced loads elsewhere on strided axes, with 16 systems per
-    // CTA (64-byte row segments) in FP32 and beyond 1 MiB in FP64 (where a
-    // tile's rows fall in different 2 MiB pages and the TMA tiles slow
-    // down); long axis-0 systems take one CTA each, longer ones the blocked
-    // partition (blocks of 32*chunk rows)
+    // TMA staging on axis 0; on strided axes the streamed kernel with a full
+    // 128-byte line of systems per tile (16 FP64 / 32 FP32), fastest at every
+    // row stride measured (DRAM serves 64-byte row segments far slower once
+    // the stride reaches 64 KiB).  Where it does not apply (more than 256
+    // rows, a narrow or misaligned axis 0) the narrow-tile kernel that was
+    // best for the class takes over: plain coalesced loads with 8 systems
+    // per CTA up to 64 KiB strides, TMA tiles of 8 systems up to 1 MiB, plain
+    // loads with 16 systems beyond that and in FP32.  Long axis-0 systems
+    // take one CTA each, longer ones the blocked partition (blocks of
+    // 32*chunk rows).
     if (axis == 0) {
       m.method = 2;
-    } else if (dtype_bytes == 4 || axis == 3) {
-      m.method = 3;
-      m.spc = 16;
     } else {
-      m.method = (axis == 1) ? 3 : 2;
+      m.method = 2;
+      m.spc = 128 / dtype_bytes;
+      if (dtype_bytes == 4 || axis == 3) {
+        m.fb_method = 3;
+        m.fb_spc = 16;
+      } else {
+        m.fb_method = (axis == 1) ? 3 : 2;
+        m.fb_spc = 8;
+      }
     }
   }
   if (m.method >= 2) {
@@ -319,8 +331,9 @@ static tridStatus_t solve_level(const T *a, const T *b, const T *c, T *d, T *u, 
     A.c = c;
     A.rhs = d;
     A.out = INC ? u : d;
-    const tridStatus_t s2 = INC ? run_general<T, kGenFwdInc>(g, A, axis, m.chunk, m.spc, level, stream)
-                                : run_general<T, kGenFwd>(g, A, axis, m.chunk, m.spc, level, stream);
+    const int spc = narrow_spc(m);
+    const tridStatus_t s2 = INC ? run_general<T, kGenFwdInc>(g, A, axis, m.chunk, spc, level, stream)
+                                : run_general<T, kGenFwd>(g, A, axis, m.chunk, spc, level, stream);
     if (s2 != TRID_STATUS_SUCCESS) return s2;
     e = cudaSuccess;
   } else if (m.method >= 2) {
@@ -337,9 +350,12 @@ static tridStatus_t solve_level(const T *a, const T *b, const T *c, T *d, T *u, 
         if (!err) return TRID_STATUS_ALLOC_FAILED;
         e = launch_strided_part_tma<T, INC>(g, dims, pads, ndim, solvedim, a, b, c, d, u, m.chunk,
                                             m.spc, true, err, stream);
+        if (e == cudaErrorNotSupported && m.fb_method == 2)
+          e = launch_strided_part_tma<T, INC>(g, dims, pads, ndim, solvedim, a, b, c, d, u,
+                                              m.chunk, m.fb_spc, true, err, stream);
       }
       if (e == cudaErrorNotSupported)
-        e = launch_strided<T, INC>(g, a, b, c, d, u, m.chunk, m.spc, stream);
+        e = launch_strided<T, INC>(g, a, b, c, d, u, m.chunk, narrow_spc(m), stream);
     }
   } else {
     // Thomas with c'/d' in scratch, in batches of systems bounded to ~1 GiB
@@ -397,7 +413,7 @@ tridStatus_t solve_adjoint(const T *a, const T *b, const T *c, const T *u, const
   A.gb = gb;
   A.gc = gc;
   A.gd = gd;
-  return run_general<T, kGenAdj>(g, A, axis, m.chunk, m.spc, 0, stream);
+  return run_general<T, kGenAdj>(g, A, axis, m.chunk, narrow_spc(m), 0, stream);
 }
 // Forward solve and adjoint of the linear loss <w, x> in one pass where a
 // one-warp or one-CTA-per-system kernel applies (axis 0, n <= 4096); otherwise the
@@ -435,7 +451,7 @@ tridStatus_t solve_fwd_adj(const T *a, const T *b, const T *c, const T *d, const
   A.c = c;
   A.rhs = d;
   A.out = x;
-  const tridStatus_t s1 = run_general<T, kGenFwd>(g, A, axis, m.chunk, m.spc, 0, stream);
+  const tridStatus_t s1 = run_general<T, kGenFwd>(g, A, axis, m.chunk, narrow_spc(m), 0, stream);
   if (s1 != TRID_STATUS_SUCCESS) return s1;
   return solve_adjoint<T>(a, b, c, x, w, ga, gb, gc, gd, ndim, solvedim, dims, pads);
 }
@@ -583,7 +599,8 @@ extern "C" tridStatus_t tridSetMethod(int method, int chunk, int sys_per_cta) {
   if (method < 0 || method > 6) return TRID_STATUS_INVALID_VALUE;
   if (chunk != 0 && chunk != 2 && chunk != 4 && chunk != 8 && chunk != 16)
     return TRID_STATUS_INVALID_VALUE;
-  if (sys_per_cta != 0 && sys_per_cta != 4 && sys_per_cta != 8 && sys_per_cta != 16)
+  if (sys_per_cta != 0 && sys_per_cta != 4 && sys_per_cta != 8 && sys_per_cta != 16 &&
+      sys_per_cta != 32)
     return TRID_STATUS_INVALID_VALUE;
   tl_force = {method, chunk, sys_per_cta};
   return TRID_STATUS_SUCCESS;

@@ -16,7 +16,19 @@ struct MethodChoice {
   int method;   // 1 = Thomas (generic), 2 = partitioned
   int chunk;    // rows per thread (method 2)
   int spc;      // systems per CTA (method 2, strided axes)
+  // where the built-in default is the streamed full-line kernel (method 2
+  // with 128 bytes of systems per CTA) and that kernel does not apply: the
+  // narrow-tile method and systems per CTA to use instead (0 = none)
+  int fb_method = 0;
+  int fb_spc = 0;
 };
+
+// Systems per CTA for the narrow-tile kernels (plain strided, blocked
+// partition), which take 4, 8 or 16.
+inline int narrow_spc(const MethodChoice &m) {
+  if (m.fb_method != 0) return m.fb_spc;
+  return m.spc > 16 ? 16 : m.spc;
+}
 
 // Pick the method for (dtype bytes, axis class, n); honours the per-thread
 // override and the tuning table.

@@ -16,10 +16,35 @@
 // otherwise): solvedim >= 1, ndim <= 5, 16-byte aligned base pointers,
 // pads[0]*sizeof(T) a multiple of 16 for every array, dims[0] >= SB,
 // n <= 32*M and the tile fitting in shared memory.
+#include <algorithm>
+
 #include "partition.cuh"
 #include "tma.cuh"
 
 namespace tridb200 {
+
+// Rows [r0, r0+M) of tile system sl from the staged tile ([array][row][SB]).
+// Every shared-memory read is unconditional (row index clamped into the
+// tile), and rows past n or systems past the axis become identity rows by
+// selects afterwards, so the M*4 reads issue back to back instead of one
+// guarded read at a time.
+template <typename T, int M, int SB, int INC>
+__device__ __forceinline__ void load_rows(const T *tile, size_t tsz, int r0, int sl, int n,
+                                          int rows_cap, bool valid, T (&al)[M], T (&be)[M],
+                                          T (&ga)[M], T (&de)[M], T (&uo)[INC ? M : 1]) {
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int r = r0 + j;
+    const size_t o = (size_t)(r < rows_cap ? r : rows_cap - 1) * SB + sl;
+    const T va = tile[o], vb = tile[tsz + o], vc = tile[2 * tsz + o], vd = tile[3 * tsz + o];
+    const bool in = valid && r < n;
+    al[j] = (in && r != 0) ? va : T(0);
+    be[j] = in ? vb : T(1);
+    ga[j] = (in && r != n - 1) ? vc : T(0);
+    de[j] = in ? vd : T(0);
+    if constexpr (INC) uo[j] = in ? tile[4 * tsz + o] : T(0);
+  }
+}
 
 template <typename T, int M, int SB, int INC>
 __global__ void __launch_bounds__(SB * kWarp) strided_part_tma_kernel(
@@ -180,6 +205,183 @@ __global__ void __launch_bounds__(SB * kWarp) strided_part_tma_kernel(
   }
 }
 
+// Persistent form for wide tiles (SB * sizeof(T) >= 128: one 128-byte line
+// per row and array).  On large row strides (planes of 64 KiB and more) DRAM
+// serves 64-byte row segments at about 60% of the rate of 128-byte ones, so
+// the tile must be a full line wide; such a tile (128 KB for FP64 at n = 256)
+// leaves room for one CTA per SM, and without overlap the SM's loads would
+// stop while it computes.  So the CTA loops over tiles with one buffer: it
+// copies the tile from shared memory into registers, releases the buffer,
+// issues the next tile's bulk tensor loads, and solves and stores (plain
+// coalesced stores of full lines) while those loads are in flight.
+template <typename T, int M, int SB, int INC, bool FULL>
+__global__ void __launch_bounds__(SB * kWarp, 1) strided_stream_kernel(
+    const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mb,
+    const __grid_constant__ CUtensorMap mc, const __grid_constant__ CUtensorMap md,
+    const __grid_constant__ CUtensorMap mu, Geom g, int solvedim, int box_rows, int nbox,
+    uint32_t ntiles, uint32_t ntx_mul, uint32_t ntx_shift, T *__restrict__ d,
+    T *__restrict__ u, unsigned *err) {
+  // FULL: n == 32*M and dims[0] a multiple of SB (no row or system guards)
+  constexpr int NA = INC ? 5 : 4;
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ uint64_t bar;
+  T *tile = reinterpret_cast<T *>(smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127));
+  constexpr int kAlignElems = 128 / (int)sizeof(T);
+  const size_t tsz = FULL ? (size_t)32 * M * SB
+                          : (((size_t)box_rows * nbox * SB + kAlignElems - 1) / kAlignElems) *
+                                kAlignElems;
+  T *red = tile + NA * tsz;                                   // [8][32][SB+1]
+  T *sol = red + 8 * kWarp * (SB + 1);                        // [2][32][SB+1]
+  const int rows_cap = FULL ? 32 * M : box_rows * nbox;
+
+  const int tid = threadIdx.x;
+  const int sl = tid % SB;
+  const int t = tid / SB;
+  const int n = FULL ? 32 * M : g.n;
+  const uint32_t ntx = (uint32_t)(g.odims[0] + SB - 1) / SB;
+  // tile -> coordinates (x0 on axis 0, then the other non-solve axes) and the
+  // tile's index along the flattened outer axes; multiply-high divisions
+  auto tile_coords = [&](uint32_t blk, int (&cc)[5]) -> uint32_t {
+    const uint32_t outer = fastdiv(blk, ntx_mul, ntx_shift);
+    cc[0] = (int)(blk - outer * ntx) * SB;
+    cc[1] = cc[2] = cc[3] = cc[4] = 0;
+    uint32_t rest = outer;
+    int o = 1;
+    for (int k = 1; k < 5; ++k) {
+      if (k == solvedim || o >= g.nod) continue;
+      const uint32_t q = fastdiv(rest, g.dmul[o], g.dshift[o]);
+      cc[k] = (int)(rest - q * (uint32_t)g.odims[o]);
+      rest = q;
+      ++o;
+    }
+    return outer;
+  };
+  const CUtensorMap *maps[5] = {&ma, &mb, &mc, &md, &mu};
+  if (!tma_smem_aligned(tile) || (nbox > 1 && ((size_t)box_rows * SB * sizeof(T)) % 128 != 0)) {
+    if (tid == 0) atomicOr(err, kErrMisaligned);
+    return;
+  }
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const uint32_t tx_bytes = (uint32_t)(NA * nbox * box_rows * SB * sizeof(T));
+  auto issue = [&](const int (&cc)[5]) {
+    mbar_arrive_expect_tx(&bar, tx_bytes);
+    for (int q = 0; q < NA; ++q)
+      for (int bx = 0; bx < nbox; ++bx) {
+        int c[5] = {cc[0], cc[1], cc[2], cc[3], cc[4]};
+        c[solvedim] = bx * box_rows;
+        tma_load_5d(tile + q * tsz + (size_t)bx * box_rows * SB, maps[q], &bar, c[0], c[1], c[2],
+                    c[3], c[4]);
+      }
+  };
+  uint32_t blk = blockIdx.x;
+  if (tid == 0 && blk < ntiles) {
+    int cc[5];
+    tile_coords(blk, cc);
+    issue(cc);
+  }
+  uint32_t parity = 0;
+  const int r0 = t * M;
+  const int64_t so = INC ? g.stride[kU] : g.stride[kD];
+  T *const out = INC ? u : d;
+  auto R = [&](int comp, int chunk, int s) -> T & {
+    return red[((size_t)comp * kWarp + chunk) * (SB + 1) + s];
+  };
+  for (; blk < ntiles; blk += gridDim.x) {
+    // index work that does not need the tile, done while its copy lands: this
+    // system's output offset and, for the issuing thread, the next tile
+    int cc[5];
+    const uint32_t outer = tile_coords(blk, cc);
+    const bool valid = FULL || cc[0] + sl < g.odims[0];
+    int64_t obase = 0;
+    if (valid) {
+      int64_t off[5];
+      system_offsets(g, (int64_t)cc[0] + sl + (int64_t)g.odims[0] * outer, off);
+      obase = off[INC ? kU : kD];
+    }
+    const bool more = blk + gridDim.x < ntiles;
+    int cn[5];
+    if (tid == 0 && more) tile_coords(blk + gridDim.x, cn);
+
+    const bool got = mbar_wait(&bar, parity, err);
+    T al[M], be[M], ga[M], de[M], uo[INC ? M : 1];
+    load_rows<T, M, SB, INC>(tile, tsz, r0, sl, n, rows_cap, valid, al, be, ga, de, uo);
+    // this thread's reads of the buffer come before the next tile's copies
+    fence_proxy_async();
+    if (!__syncthreads_and(got)) {
+      // a copy that never completed: let it land (bounded) before leaving
+      if (tid == 0) mbar_wait(&bar, parity, nullptr);
+      return;
+    }
+    parity ^= 1;
+    if (tid == 0 && more) issue(cn);
+
+    Row<T> F, L;
+    chunk_reduce<T, M>(al, be, ga, de, F, L);
+    R(0, t, sl) = F.a;
+    R(1, t, sl) = F.b;
+    R(2, t, sl) = F.c;
+    R(3, t, sl) = F.d;
+    R(4, t, sl) = L.a;
+    R(5, t, sl) = L.b;
+    R(6, t, sl) = L.c;
+    R(7, t, sl) = L.d;
+    __syncthreads();
+    {
+      const int w = tid / kWarp;
+      const int lane = tid & (kWarp - 1);
+      const Row<T> F2{R(0, lane, w), R(1, lane, w), R(2, lane, w), R(3, lane, w)};
+      const Row<T> L2{R(4, lane, w), R(5, lane, w), R(6, lane, w), R(7, lane, w)};
+      T xF, xL;
+      warp_interface_solve(F2, L2, xF, xL, lane);
+      sol[(0 * kWarp + lane) * (SB + 1) + w] = xF;
+      sol[(1 * kWarp + lane) * (SB + 1) + w] = xL;
+    }
+    __syncthreads();
+    chunk_backsub<T, M>(al, ga, de, sol[(0 * kWarp + t) * (SB + 1) + sl],
+                        sol[(1 * kWarp + t) * (SB + 1) + sl]);
+    if (valid) {
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        const int r = r0 + j;
+        if (FULL || r < n) out[obase + r * so] = INC ? uo[INC ? j : 0] + de[j] : de[j];
+      }
+    }
+  }
+}
+
+template <typename T, int M, int SB, int INC>
+static cudaError_t launch_stream(const CUtensorMap *maps, const Geom &g, int solvedim,
+                                 int box_rows, int nbox, int64_t blocks, T *d, T *u,
+                                 unsigned *err, cudaStream_t st, int optin) {
+  constexpr int NA = INC ? 5 : 4;
+  constexpr int kAlignElems = 128 / (int)sizeof(T);
+  const size_t tsz = (((size_t)box_rows * nbox * SB + kAlignElems - 1) / kAlignElems) * kAlignElems;
+  const size_t smem = (size_t)NA * tsz * sizeof(T) + (size_t)10 * kWarp * (SB + 1) * sizeof(T) + 128;
+  if (smem + 64 > (size_t)optin || !g.fastdiv) return cudaErrorNotSupported;
+  const bool full = g.n == 32 * M && g.odims[0] % SB == 0;
+  auto kern = full ? strided_stream_kernel<T, M, SB, INC, true>
+                   : strided_stream_kernel<T, M, SB, INC, false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0, dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SB * kWarp, smem) != cudaSuccess ||
+      per_sm < 1)
+    return cudaErrorNotSupported;
+  const int64_t grid = std::min<int64_t>(blocks, (int64_t)per_sm * sms);
+  uint32_t ntx_mul = 0, ntx_shift = 0;
+  fastdiv_setup((uint32_t)((g.odims[0] + SB - 1) / SB), ntx_mul, ntx_shift);
+  kern<<<dim3((unsigned)grid), dim3(SB * kWarp), smem, st>>>(
+      maps[0], maps[1], maps[2], maps[3], maps[4], g, solvedim, box_rows, nbox, (uint32_t)blocks,
+      ntx_mul, ntx_shift, d, u, err);
+  return cudaGetLastError();
+}
+
 template <typename T, int M, int SB, int INC>
 static cudaError_t launch_sptma(const CUtensorMap *maps, const Geom &g, int solvedim,
                                 int box_rows, int nbox, int64_t blocks, unsigned *err,
@@ -211,10 +413,20 @@ static cudaError_t launch_sptma(const CUtensorMap *maps, const Geom &g, int solv
 
 template <typename T, int M, int INC>
 static cudaError_t launch_sptma_sb(const CUtensorMap *maps, const Geom &g, int solvedim,
-                                   int box_rows, int nbox, int spc, int64_t ntiles_rest,
-                                   unsigned *err, cudaStream_t st, int optin, bool prefetch) {
+                                   int box_rows, int nbox, int spc, int64_t ntiles_rest, T *d,
+                                   T *u, unsigned *err, cudaStream_t st, int optin, bool prefetch) {
   const int64_t blocks = ((g.odims[0] + spc - 1) / spc) * ntiles_rest;
   if (blocks > 0x7fffffff || blocks == 0) return cudaErrorNotSupported;
+  // full-line tiles (16 FP64 / 32 FP32 systems) stream through one persistent CTA per SM
+  // (at most 8 rows per thread: 16 would spill at one CTA per SM)
+  if (spc * (int)sizeof(T) >= 128) {
+    if constexpr (M <= 8 && sizeof(T) == 8) {
+      if (spc == 16) return launch_stream<T, M, 16, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
+    } else if constexpr (M <= 8) {
+      if (spc == 32) return launch_stream<T, M, 32, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
+    }
+    return cudaErrorNotSupported;
+  }
   switch (spc) {
     case 4: return launch_sptma<T, M, 4, INC>(maps, g, solvedim, box_rows, nbox, blocks, err, st, optin, prefetch);
     case 8: return launch_sptma<T, M, 8, INC>(maps, g, solvedim, box_rows, nbox, blocks, err, st, optin, prefetch);
@@ -256,10 +468,10 @@ cudaError_t launch_strided_part_tma(const Geom &g, const int *dims, const int *c
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const int64_t rest = g.nsys / dims[0];
   switch (chunk) {
-    case 2: return launch_sptma_sb<T, 2, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin, prefetch);
-    case 4: return launch_sptma_sb<T, 4, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin, prefetch);
-    case 8: return launch_sptma_sb<T, 8, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin, prefetch);
-    case 16: return launch_sptma_sb<T, 16, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, err, st, optin, prefetch);
+    case 2: return launch_sptma_sb<T, 2, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, d, u, err, st, optin, prefetch);
+    case 4: return launch_sptma_sb<T, 4, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, d, u, err, st, optin, prefetch);
+    case 8: return launch_sptma_sb<T, 8, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, d, u, err, st, optin, prefetch);
+    case 16: return launch_sptma_sb<T, 16, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, d, u, err, st, optin, prefetch);
     default: return cudaErrorNotSupported;
   }
 }
