@@ -10,10 +10,12 @@ variable ``TRID_B200_TUNING``).
 
 Candidates (see tridSetMethod in include/trid_b200.h):
     method 1            Thomas, one thread per system, c'/d' in scratch
-    method 2/3, chunk   partitioned Thomas with warp PCR (2 = TMA staging on
-                        axis 0 when possible, 3 = plain loads), with every
+    method 2/3, chunk   partitioned Thomas with warp PCR (2 = TMA staging
+                        when possible, 3 = plain loads), with every
                         rows-per-thread chunk that covers n and, on strided
-                        axes, 4/8/16 systems per CTA
+                        axes, 4/8/16 systems per CTA (and 32 for method 2;
+                        128 bytes of systems, 16 FP64 / 32 FP32, is the
+                        streamed persistent kernel)
     method 4            strided axes: two-sided Thomas with a TMA stage ring
     method 5            axis 0, longer systems: one warp per system, staged in
                         shared memory
@@ -23,8 +25,10 @@ Candidates (see tridSetMethod in include/trid_b200.h):
     block reduction, recursive block solve, block finish)
 
 --stride-sweep instead times the default algorithm on FP64 problems of
-64 M unknowns whose solve axis has plane strides from 8 KiB to 2 MiB (the
-row span of one system against 2 MiB pages), with plain and TMA-staged tiles.
+64 M unknowns whose solve axis has plane strides from 8 KiB to 2 MiB, against
+the streamed full-line tiles and the narrow (8 and 16 system) plain and
+TMA-staged tiles: 64-byte row segments lose much of DRAM's rate once the
+stride reaches 64 KiB.
 
 Axis classes: 0 = solve along axis 0 (unit stride); 1 = strided, row stride
 <= 64 KiB; 2 = <= 1 MiB; 3 = larger strides (swept with --classes 0,1,2,3).
@@ -67,6 +71,7 @@ def candidates(axis, n):
                 for spc in (4, 8, 16):
                     out.append((2, ch, spc))
                     out.append((3, ch, spc))
+                out.append((2, ch, 32))
     if axis > 0:
         out.append((4, 0, 0))
     elif n > 64:
@@ -153,7 +158,7 @@ STRIDE_SHAPES = (([256, 4, 256, 256], 2), ([256, 16, 256, 64], 2), ([256, 256, 2
                  ([256, 256, 256], 2), ([1024, 64, 256], 2), ([2048, 128, 256], 2))
 
 
-def stride_sweep(methods=((0, 0, 0), (2, 8, 8), (3, 8, 8), (3, 8, 16))):
+def stride_sweep(methods=((0, 0, 0), (2, 8, 16), (2, 8, 8), (3, 8, 8), (3, 8, 16))):
     """GB/s of FP64 solves of n=256 on strided axes whose plane stride grows
     from 8 KiB to 2 MiB (the same 40 B/unknown and about 64 M unknowns each)."""
     import torch
