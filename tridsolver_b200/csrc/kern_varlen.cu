@@ -219,11 +219,10 @@ __device__ __forceinline__ void vl_cp_async(void *dst, const void *src, bool val
 }
 
 // rows rb .. rb+32M-1 of a system (clipped to len) into the warp's four
-// regions, then this lane's rows rb+lane*M+j, transposed
+// regions (issue only; vl_read waits)
 template <typename T, int M>
-__device__ __forceinline__ void vl_load(const VLArgs<T> &A, T *reg, int64_t lo, int64_t rb,
-                                        int64_t len, int lane, T (&al)[M], T (&be)[M], T (&ga)[M],
-                                        T (&de)[M]) {
+__device__ __forceinline__ void vl_issue(const VLArgs<T> &A, T *reg, int64_t lo, int64_t rb,
+                                         int64_t len, int lane) {
   const T *src[4] = {A.a + lo, A.b + lo, A.c + lo, A.d + lo};
   __syncwarp();  // the previous item's reads of the regions are done
 #pragma unroll
@@ -236,6 +235,12 @@ __device__ __forceinline__ void vl_load(const VLArgs<T> &A, T *reg, int64_t lo, 
     for (int k = 0; k < 4; ++k)
       vl_cp_async(reg + k * kVLRegion + sq, in ? src[k] + r : src[k], in, (int)sizeof(T));
   }
+}
+
+// wait for vl_issue's copies, then this lane's rows rb+lane*M+j, transposed
+template <typename T, int M>
+__device__ __forceinline__ void vl_read(const T *reg, int64_t rb, int64_t len, int lane,
+                                        T (&al)[M], T (&be)[M], T (&ga)[M], T (&de)[M]) {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncwarp();
   const int ts = lane * (M + 1);
@@ -247,6 +252,27 @@ __device__ __forceinline__ void vl_load(const VLArgs<T> &A, T *reg, int64_t lo, 
     be[j] = in ? reg[kVLRegion + ts + j] : T(1);
     ga[j] = (r < len - 1) ? reg[2 * kVLRegion + ts + j] : T(0);
     de[j] = reg[3 * kVLRegion + ts + j];  // zero-filled past len
+  }
+}
+
+// L2 bulk prefetch of rows [first, first+count) of a, b, c, d, widened to
+// 16-byte units that stay inside the arrays (whose bases must then be 16-byte
+// aligned; otherwise nothing is prefetched: it is only a hint)
+template <typename T>
+__device__ __forceinline__ void vl_prefetch_rows(const VLArgs<T> &A, int64_t first, int64_t count) {
+  const T *base[4] = {A.a, A.b, A.c, A.d};
+  const int64_t end = (A.total * (int64_t)sizeof(T)) & ~(int64_t)15;
+  int64_t b0 = (first * (int64_t)sizeof(T)) & ~(int64_t)15;
+  int64_t b1 = ((first + count) * (int64_t)sizeof(T) + 15) & ~(int64_t)15;
+  if (b1 > end) b1 = end;
+  if (b1 <= b0) return;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (((uintptr_t)base[k] & 15) != 0) continue;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
+                     reinterpret_cast<const char *>(base[k]) + b0),
+                 "r"((uint32_t)(b1 - b0))
+                 : "memory");
   }
 }
 
@@ -267,11 +293,14 @@ __device__ __forceinline__ void vl_store(const VLArgs<T> &A, T *reg, int64_t lo,
   __syncwarp();  // the regions are reused by the warp's next item
 }
 
-template <typename T, int M>
+// `between` runs while the item's rows are in flight (it warms the next item)
+template <typename T, int M, typename Fn>
 __device__ __forceinline__ void vl_short(const VLArgs<T> &A, T *reg, int64_t lo, int64_t len,
-                                         int lane) {
+                                         int lane, Fn &&between) {
   T al[M], be[M], ga[M], de[M];
-  vl_load<T, M>(A, reg, lo, 0, len, lane, al, be, ga, de);
+  vl_issue<T, M>(A, reg, lo, 0, len, lane);
+  between();
+  vl_read<T, M>(reg, 0, len, lane, al, be, ga, de);
   Row<T> F, L;
   chunk_reduce<T, M>(al, be, ga, de, F, L);
   T xF, xL;
@@ -281,12 +310,15 @@ __device__ __forceinline__ void vl_short(const VLArgs<T> &A, T *reg, int64_t lo,
 }
 
 // one block of a long system: chunk reduction + block basis
-template <typename T>
+template <typename T, typename Fn>
 __device__ __forceinline__ void vl_block(const VLArgs<T> &A, T *reg, int64_t lo, int64_t len,
                                          int blk, int lane, T (&al)[8], T (&ga)[8], T (&de)[8],
-                                         Row<T> &F, Row<T> &L, T (&bF)[3], T (&bL)[3]) {
+                                         Row<T> &F, Row<T> &L, T (&bF)[3], T (&bL)[3],
+                                         Fn &&between) {
   T be[8];
-  vl_load<T, 8>(A, reg, lo, (int64_t)blk * kVLBlock, len, lane, al, be, ga, de);
+  vl_issue<T, 8>(A, reg, lo, (int64_t)blk * kVLBlock, len, lane);
+  between();
+  vl_read<T, 8>(reg, (int64_t)blk * kVLBlock, len, lane, al, be, ga, de);
   chunk_reduce<T, 8>(al, be, ga, de, F, L);
   warp_block_basis(F, L, lane, bF, bL);
 }
@@ -304,12 +336,30 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
   T *reg = reinterpret_cast<T *>(vl_dyn) + (size_t)(threadIdx.x / kWarp) * 4 * kVLRegion;
   const int64_t nitems = A.item_off[A.nsys];
   const int64_t nf = A.fitem_off[A.nsys];
+  // Both queues are software-pipelined: lane 0 claims the next item one
+  // iteration ahead and, while the current item's rows are in flight, looks
+  // up the next item's rows and warms L2 with them.
+  auto warm = [&](unsigned long long nx, int64_t nlimit, const int *tsys,
+                  const int64_t *toff, bool long_only) {
+    if (lane != 0 || (int64_t)nx >= nlimit) return;
+    const int64_t s2 = tsys[nx];
+    const int64_t lo2 = A.offsets[s2], hi2 = A.offsets[s2 + 1];
+    if (vl_bad(lo2, hi2, A.total) || hi2 == lo2) return;
+    int64_t first = lo2, cnt = hi2 - lo2;
+    if (long_only || cnt > kVLShort) {
+      first = lo2 + ((int64_t)nx - toff[s2]) * kVLBlock;
+      cnt = hi2 - first < kVLBlock ? hi2 - first : kVLBlock;
+    }
+    if (cnt > 0) vl_prefetch_rows(A, first, cnt);
+  };
   // ---- reduce queue ----
+  unsigned long long nit = 0;  // lane 0: the next claimed reduce item
+  if (lane == 0) nit = atomicAdd(&A.queue[0], 1ull);
   for (;;) {
-    unsigned long long it = 0;
-    if (lane == 0) it = atomicAdd(&A.queue[0], 1ull);
-    it = __shfl_sync(0xffffffffu, it, 0);
+    const unsigned long long it = __shfl_sync(0xffffffffu, nit, 0);
     if ((int64_t)it >= nitems) break;
+    if (lane == 0) nit = atomicAdd(&A.queue[0], 1ull);
+    auto between = [&]() { warm(nit, nitems, A.item_sys, A.item_off, false); };
     const int64_t s = A.item_sys[it];
     const int64_t lo = A.offsets[s], hi = A.offsets[s + 1];
     const int64_t len = hi - lo;
@@ -320,11 +370,11 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
     if (len == 0) continue;
     if (len <= kVLShort) {
       if (len <= 64)
-        vl_short<T, 2>(A, reg, lo, len, lane);
+        vl_short<T, 2>(A, reg, lo, len, lane, between);
       else if (len <= 128)
-        vl_short<T, 4>(A, reg, lo, len, lane);
+        vl_short<T, 4>(A, reg, lo, len, lane, between);
       else
-        vl_short<T, 8>(A, reg, lo, len, lane);
+        vl_short<T, 8>(A, reg, lo, len, lane, between);
       continue;
     }
     const int nblk = (int)((len + kVLBlock - 1) / kVLBlock);
@@ -335,7 +385,7 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
     const int blk = (int)((int64_t)it - A.item_off[s]);
     T al[8], ga[8], de[8], bF[3], bL[3];
     Row<T> F, L, FB, LB;
-    vl_block<T>(A, reg, lo, len, blk, lane, al, ga, de, F, L, bF, bL);
+    vl_block<T>(A, reg, lo, len, blk, lane, al, ga, de, F, L, bF, bL, between);
     block_rows(F, L, bF, bL, lane, FB, LB);
     T *rw = A.rows + ((int64_t)A.item_off[s] + blk) * 8;
     if (lane == 0) {
@@ -370,11 +420,12 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
     if (lane == 0) atomicOr(&A.sys_count[s], kVLSolved);
   }
   // ---- finish queue ----
+  unsigned long long nfi = 0;  // lane 0: the next claimed finish item
+  if (lane == 0) nfi = atomicAdd(&A.queue[1], 1ull);
   for (;;) {
-    unsigned long long fi = 0;
-    if (lane == 0) fi = atomicAdd(&A.queue[1], 1ull);
-    fi = __shfl_sync(0xffffffffu, fi, 0);
+    const unsigned long long fi = __shfl_sync(0xffffffffu, nfi, 0);
     if ((int64_t)fi >= nf) break;
+    if (lane == 0) nfi = atomicAdd(&A.queue[1], 1ull);
     const int64_t s = A.fitem_sys[fi];
     // the system's reduce items were all taken by running warps: its mark
     // comes; poll a bounded number of times
@@ -395,7 +446,8 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
     const int64_t lo = A.offsets[s], len = A.offsets[s + 1] - lo;
     T al[8], ga[8], de[8], bF[3], bL[3];
     Row<T> F, L;
-    vl_block<T>(A, reg, lo, len, blk, lane, al, ga, de, F, L, bF, bL);
+    vl_block<T>(A, reg, lo, len, blk, lane, al, ga, de, F, L, bF, bL,
+                [&]() { warm(nfi, nf, A.fitem_sys, A.fitem_off, true); });
     const T *bs = A.rows + ((int64_t)A.item_off[s] + blk) * 8;
     const T f = __ldcg(bs), l = __ldcg(bs + 1);
     const T xF = bF[0] + f * bF[1] + l * bF[2];
