@@ -126,7 +126,8 @@ struct Stage {
   }
 };
 
-template <typename T, int M>
+// FULL: n is a whole number of warp blocks (no row past n anywhere)
+template <typename T, int M, bool FULL = false>
 __device__ __forceinline__ void stage_in(const Stage<T, M> &S, int k, int w, int lane, const T *p,
                                          int n) {
   T *reg = S.region(k, w);
@@ -134,13 +135,13 @@ __device__ __forceinline__ void stage_in(const Stage<T, M> &S, int k, int w, int
 #pragma unroll
   for (int j = 0; j < M; ++j) {
     const int q = j * kWarp + lane;
-    const bool in = wb + q < n;
+    const bool in = FULL || wb + q < n;
     cp_async_elem(reg + pidx<M>(q), in ? p + wb + q : p, in);
   }
 }
 
 // v (rows lane*M + j of warp w) -> region k -> coalesced store to p (ADD: +=)
-template <typename T, int M, bool ADD>
+template <typename T, int M, bool ADD, bool FULL = false>
 __device__ __forceinline__ void stage_out(const Stage<T, M> &S, int k, int w, int lane,
                                           const T (&v)[M], T *p, int n) {
   T *reg = S.region(k, w);
@@ -151,7 +152,7 @@ __device__ __forceinline__ void stage_out(const Stage<T, M> &S, int k, int w, in
 #pragma unroll
   for (int j = 0; j < M; ++j) {
     const int q = j * kWarp + lane;
-    if (wb + q < n) {
+    if (FULL || wb + q < n) {
       if (ADD)
         p[wb + q] += reg[pidx<M>(q)];
       else
@@ -160,9 +161,10 @@ __device__ __forceinline__ void stage_out(const Stage<T, M> &S, int k, int w, in
   }
 }
 
-// Warm L2 with the system `dist` CTAs ahead (the CTA that will take this
-// one's place on the GPU): one bulk prefetch per array, so that DRAM keeps
-// streaming while the resident CTAs compute.  Needs 16-byte aligned rows of a
+// Warm L2 with the system `dist` CTAs ahead (half a resident set ahead: its
+// rows arrive well before their CTA starts, without crowding L2): one bulk
+// prefetch per array, so that DRAM keeps streaming while the resident CTAs
+// compute.  Needs 16-byte aligned rows of a
 // whole number of 16-byte units.
 template <typename T>
 __device__ __forceinline__ void prefetch_system_l2(const T *p, int n) {
@@ -171,7 +173,7 @@ __device__ __forceinline__ void prefetch_system_l2(const T *p, int n) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-template <typename T, int M, int MODE>
+template <typename T, int M, int MODE, bool FULL>
 __device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int dist) {
   extern __shared__ __align__(16) unsigned char xcta_dyn[];
   __shared__ T sm[128 + 32 + 2 * 16];
@@ -187,14 +189,14 @@ __device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int 
   // staged arrays: 0 a, 1 b, 2 c, 3 d (forward modes) or the solution
   // (kXAdj), 4 w (kXAdj, kXFused)
   constexpr bool kHasW = (MODE == kXAdj || MODE == kXFused);
-  stage_in<T, M>(S, 0, w, lane, A.a + off[kA], n);
-  stage_in<T, M>(S, 1, w, lane, A.b + off[kB], n);
-  stage_in<T, M>(S, 2, w, lane, A.c + off[kC], n);
+  stage_in<T, M, FULL>(S, 0, w, lane, A.a + off[kA], n);
+  stage_in<T, M, FULL>(S, 1, w, lane, A.b + off[kB], n);
+  stage_in<T, M, FULL>(S, 2, w, lane, A.c + off[kC], n);
   if (MODE == kXAdj)
-    stage_in<T, M>(S, 3, w, lane, A.usol + off[kU], n);
+    stage_in<T, M, FULL>(S, 3, w, lane, A.usol + off[kU], n);
   else
-    stage_in<T, M>(S, 3, w, lane, A.d + off[kD], n);
-  if (kHasW) stage_in<T, M>(S, 4, w, lane, A.w + off[kD], n);
+    stage_in<T, M, FULL>(S, 3, w, lane, A.d + off[kD], n);
+  if (kHasW) stage_in<T, M, FULL>(S, 4, w, lane, A.w + off[kD], n);
   if (dist > 0 && threadIdx.x == 0 && blockIdx.x + (int64_t)dist < g.nsys) {
     int64_t po[5];
     system_offsets(g, blockIdx.x + (int64_t)dist, po);
@@ -221,7 +223,7 @@ __device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int 
 #pragma unroll
     for (int j = 0; j < M; ++j) {
       const int r = r0 + j;
-      const bool in = r < n;
+      const bool in = FULL || r < n;
       ta[j] = (in && r > 0) ? (j > 0 ? rc[j - 1] : S.row(2, r - 1)) : T(0);
       tg[j] = (r + 1 < n) ? (j < M - 1 ? ra[j + 1] : S.row(0, r + 1)) : T(0);
       be[j] = in ? rb[j] : T(1);
@@ -236,7 +238,7 @@ __device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int 
 #pragma unroll
     for (int j = 0; j < M; ++j) {
       const int r = r0 + j;
-      const bool in = r < n;
+      const bool in = FULL || r < n;
       al[j] = (in && r > 0) ? ra[j] : T(0);
       be[j] = in ? rb[j] : T(1);
       ga[j] = (r < n - 1) ? rc[j] : T(0);
@@ -246,9 +248,9 @@ __device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int 
       Row<T> F, L;
       chunk_reduce_cont<T, M>(al, be, ga, xs, F, L, rp);
       // the transposed reduction needs b only at the chunk's first and last
-      // rows; the interior pivots wait in this thread's own b slots (read by
-      // this thread alone), so that neither occupies registers meanwhile
-      const T b0 = be[0], bl = be[M - 1];
+      // rows, where it stays in this thread's own b slots (read by this
+      // thread alone); the interior pivots wait in the other slots, so that
+      // neither occupies registers meanwhile
       T *rbw = S.region(1, w) + lane * (M + 1);
 #pragma unroll
       for (int j = 1; j <= M - 2; ++j) rbw[j] = rp[j];
@@ -258,6 +260,18 @@ __device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int 
       T *rx = S.region(3, w) + lane * (M + 1);
 #pragma unroll
       for (int j = 0; j < M; ++j) rx[j] = xs[j];
+      // x leaves now (coalesced from the warp's own region), its stores
+      // overlapping the transposed solve
+      __syncwarp();
+      {
+        const T *reg = S.region(3, w);
+        const int wb = w * 32 * M;
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+          const int q = j * kWarp + lane;
+          if (FULL || wb + q < n) A.x[off[kD] + wb + q] = reg[pidx<M>(q)];
+        }
+      }
       // the transposed system: rows (c_{r-1}, b_r, a_{r+1}); its chunk
       // interiors have the forward pivots
       const T *rw = S.region(4, w) + lane * (M + 1);
@@ -265,11 +279,12 @@ __device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int 
 #pragma unroll
       for (int j = 0; j < M; ++j) {
         const int r = r0 + j;
-        const bool in = r < n;
+        const bool in = FULL || r < n;
         ta[j] = (in && r > 0) ? (j > 0 ? rc[j - 1] : S.row(2, r - 1)) : T(0);
         tg[j] = (r + 1 < n) ? (j < M - 1 ? ra[j + 1] : S.row(0, r + 1)) : T(0);
         gsol[j] = rw[j];  // zero-filled past n
-        tb[j] = (j == 0) ? b0 : (j == M - 1 ? bl : T(1));  // interior b unused
+        // interior b unused; rows past n are identity rows (staged b is 0 there)
+        tb[j] = ((j == 0 || j == M - 1) && in) ? rbw[j] : T(1);
         tp[j] = (j >= 1 && j <= M - 2) ? rbw[j] : T(0);
       }
       chunk_reduce_given<T, M>(ta, tb, tg, gsol, F, L, tp);
@@ -280,11 +295,11 @@ __device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int 
   }
 
   if (MODE == kXFwd) {
-    stage_out<T, M, false>(S, 3, w, lane, xs, A.x + off[kD], n);
+    stage_out<T, M, false, FULL>(S, 3, w, lane, xs, A.x + off[kD], n);
     return;
   }
   if (MODE == kXFwdInc) {
-    stage_out<T, M, true>(S, 3, w, lane, xs, A.x + off[kU], n);
+    stage_out<T, M, true, FULL>(S, 3, w, lane, xs, A.x + off[kU], n);
     return;
   }
   // gradients: x_{r-1} and x_{r+1} from the staged solution (region 3)
@@ -303,12 +318,12 @@ __device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int 
       const T xm = (j > 0) ? xs[j - 1] : xprev;
       v[j] = (r0 + j > 0) ? -gsol[j] * xm : T(0);
     }
-    stage_out<T, M, false>(S, 0, w, lane, v, A.ga + off[kA], n);
+    stage_out<T, M, false, FULL>(S, 0, w, lane, v, A.ga + off[kA], n);
   }
   if (A.gb) {
 #pragma unroll
     for (int j = 0; j < M; ++j) v[j] = -gsol[j] * xs[j];
-    stage_out<T, M, false>(S, 1, w, lane, v, A.gb + off[kB], n);
+    stage_out<T, M, false, FULL>(S, 1, w, lane, v, A.gb + off[kB], n);
   }
   if (A.gc) {
 #pragma unroll
@@ -316,27 +331,16 @@ __device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int 
       const T xp = (j < M - 1) ? xs[j + 1] : xnext;
       v[j] = (r0 + j + 1 < n) ? -gsol[j] * xp : T(0);
     }
-    stage_out<T, M, false>(S, 2, w, lane, v, A.gc + off[kC], n);
+    stage_out<T, M, false, FULL>(S, 2, w, lane, v, A.gc + off[kC], n);
   }
-  if (A.gd) stage_out<T, M, false>(S, 4, w, lane, gsol, A.gd + off[kD], n);
-  if (MODE == kXFused) {
-    // x is already in region 3 in the transposed order
-    __syncwarp();
-    const T *reg = S.region(3, w);
-    const int wb = w * 32 * M;
-#pragma unroll
-    for (int j = 0; j < M; ++j) {
-      const int q = j * kWarp + lane;
-      if (wb + q < n) A.x[off[kD] + wb + q] = reg[pidx<M>(q)];
-    }
-  }
+  if (A.gd) stage_out<T, M, false, FULL>(S, 4, w, lane, gsol, A.gd + off[kD], n);
 }
 
 // The kernel: register use bounded by its launch bounds (MAXW warps, MINB
 // CTAs per SM).
-template <typename T, int M, int MODE, int MAXW, int MINB>
+template <typename T, int M, int MODE, int MAXW, int MINB, bool FULL>
 __global__ void __launch_bounds__(MAXW * 32, MINB) xcta_kernel(Geom g, XArgs<T> A, int dist) {
-  xcta_body<T, M, MODE>(g, A, dist);
+  xcta_body<T, M, MODE, FULL>(g, A, dist);
 }
 
 template <typename T, int M, int MODE, auto kern>
@@ -355,7 +359,10 @@ static cudaError_t launch_xcta_k(int max_warps, const Geom &g, const XArgs<T> &A
     if (e != cudaSuccess) return e;
     attr_set[dev] = true;
   }
-  // prefetch distance: the CTAs resident on the whole GPU at once
+  // prefetch distance: half the CTAs resident on the whole GPU at once (16,384
+  // systems of 1024 rows: the forward and forward+adjoint passes both run
+  // fastest there; the full resident count is 2-6% slower, twice it 26-47%,
+  // a quarter 2-14%, none 11-34%)
   int per_sm = 0, sms = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * kWarp, smem) !=
           cudaSuccess ||
@@ -363,13 +370,14 @@ static cudaError_t launch_xcta_k(int max_warps, const Geom &g, const XArgs<T> &A
     per_sm = 0;
     cudaGetLastError();
   }
-  kern<<<(unsigned)g.nsys, warps * kWarp, smem, st>>>(g, A, per_sm * sms);
+  kern<<<(unsigned)g.nsys, warps * kWarp, smem, st>>>(g, A, per_sm * sms / 2);
   return cudaGetLastError();
 }
 
-template <typename T, int M, int MODE, int MAXW, int MINB = 1>
+template <typename T, int M, int MODE, int MAXW, int MINB = 1, bool FULL = false>
 static cudaError_t launch_xcta_m(const Geom &g, const XArgs<T> &A, int warps, cudaStream_t st) {
-  return launch_xcta_k<T, M, MODE, xcta_kernel<T, M, MODE, MAXW, MINB>>(MAXW, g, A, warps, st);
+  return launch_xcta_k<T, M, MODE, xcta_kernel<T, M, MODE, MAXW, MINB, FULL>>(MAXW, g, A, warps,
+                                                                            st);
 }
 
 template <typename T, int MODE>
@@ -388,9 +396,16 @@ cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, int chunk, cudaStream_
     return warps <= 8 ? launch_xcta_m<T, 8, MODE, 8>(g, A, warps, st)
                       : launch_xcta_m<T, 8, MODE, 16>(g, A, warps, st);
   // forward modes up to 1024 rows (two warps): registers capped for 6 CTAs
-  // per SM (the adjoint modes spill under such caps, and measured slower)
+  // per SM (the adjoint modes spill under such caps, and measured slower);
+  // systems of whole warp blocks (n = 512 * warps) drop every row guard
+  const bool full = n == warps * 32 * 16;
   if constexpr (MODE == kXFwd || MODE == kXFwdInc) {
-    if (warps <= 2) return launch_xcta_m<T, 16, MODE, 2, 6>(g, A, warps, st);
+    if (warps <= 2)
+      return full ? launch_xcta_m<T, 16, MODE, 2, 6, true>(g, A, warps, st)
+                  : launch_xcta_m<T, 16, MODE, 2, 6>(g, A, warps, st);
+  }
+  if constexpr (MODE == kXFused) {  // (the adjoint measured slower without guards)
+    if (full) return launch_xcta_m<T, 16, MODE, 8, 1, true>(g, A, warps, st);
   }
   return launch_xcta_m<T, 16, MODE, 8>(g, A, warps, st);
 }
