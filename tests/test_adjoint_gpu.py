@@ -72,7 +72,7 @@ def run_adjoint(dtype, dims, solvedim, seed=0, method=None):
         assert rel_err(host(got), want) <= tol
 
 
-@pytest.mark.parametrize("n", [1, 2, 7, 64, 256, 300, 512, 1024, 5000])
+@pytest.mark.parametrize("n", [1, 2, 7, 64, 256, 300, 512, 1024, 5000, 8192])
 def test_adjoint_axis0(n):
     run_adjoint(np.float64, [n, 23], 0, seed=n)
 
@@ -172,9 +172,10 @@ def test_autograd_finite_differences():
 
 # --------------------------------------------------------- long systems --
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
-@pytest.mark.parametrize("n", [513, 1000, 1024, 4097, 20000])
+@pytest.mark.parametrize("n", [513, 1000, 1024, 4097, 8192, 20000])
 @pytest.mark.parametrize("inc", [False, True])
 def test_long_axis0(dtype, n, inc):
+    """8192 rows: whole 256-row blocks (the guard-free block kernels)."""
     from test_scalar_gpu import run_case
     run_case(np.random.default_rng(n), dtype, [n, 9], 0, inc=inc)
 
