@@ -136,6 +136,46 @@ TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchFwdAdj(const float *a, const flo
                                                        float *db, float *dc, float *dd, int ndim,
                                                        int solvedim, int *dims, int *pads);
 
+/* Systems split along the solve dimension across ranks (one slab of rows
+ * per rank, in rank order): the two device-side phases of the reference's
+ * tridDmtsvStridedBatchMPI / tridDmtsvStridedBatchIncMPI
+ * (scalar/include/trid_mpi_cuda.hpp:51-80, implementation
+ * scalar/src/cuda/trid_cuda_mpi.cu:473-583).  The exchange between them is
+ * the caller's -- an all-gather of `bnd` over the ranks of the solve
+ * dimension (tridsolver_b200/mpi.py does it over torch.distributed):
+ *   SplitReduce : this rank's slab (dims/pads are the local extents; at least
+ *                 2 rows along solvedim) reduced to six FP64 numbers per
+ *                 system, bnd laid out [6][nsys] (nsys = product of the other
+ *                 dims, systems in the order of the strided-batch solve);
+ *   SplitFinish : bnd_all = every rank's bnd, [nranks][6][nsys] in rank
+ *                 order; solves this rank's slab (into d, or added into u
+ *                 when inc != 0, d then left as it was).  a of the first
+ *                 rank's first row and c of the last rank's last row are
+ *                 ignored, as in the single-GPU solve.
+ * Errors as the strided-batch solve; both are stream-ordered. */
+TRID_EXTERN_C tridStatus_t tridDmtsvStridedBatchSplitReduce(const double *a, const double *b,
+                                                            const double *c, const double *d,
+                                                            int ndim, int solvedim,
+                                                            const int *dims, const int *pads,
+                                                            double *bnd);
+TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchSplitReduce(const float *a, const float *b,
+                                                            const float *c, const float *d,
+                                                            int ndim, int solvedim,
+                                                            const int *dims, const int *pads,
+                                                            double *bnd);
+TRID_EXTERN_C tridStatus_t tridDmtsvStridedBatchSplitFinish(const double *a, const double *b,
+                                                            const double *c, double *d, double *u,
+                                                            int ndim, int solvedim,
+                                                            const int *dims, const int *pads,
+                                                            const double *bnd_all, int nranks,
+                                                            int rank, int inc);
+TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchSplitFinish(const float *a, const float *b,
+                                                            const float *c, float *d, float *u,
+                                                            int ndim, int solvedim,
+                                                            const int *dims, const int *pads,
+                                                            const double *bnd_all, int nranks,
+                                                            int rank, int inc);
+
 /* ---- variable-length packed batch (no reference counterpart) --------------
  * nsys independent systems packed back to back: system s occupies rows
  * [offsets[s], offsets[s+1]) of a, b, c, d (unit stride); offsets is a DEVICE

@@ -39,12 +39,18 @@ _PADDED = [vp, ip, vp, ip, vp, ip, vp, ip, vp, ip, c_int, c_int, ip, ip, c_int]
 # name -> (restype, argtypes) for the symbols every library exports
 _ADJ = [vp, vp, vp, vp, vp, vp, vp, vp, vp, c_int, c_int, ip, ip]
 _FWDADJ = [vp] * 10 + [c_int, c_int, ip, ip]
+_SPLIT_REDUCE = [vp, vp, vp, vp, c_int, c_int, ip, ip, vp]
+_SPLIT_FINISH = [vp, vp, vp, vp, vp, c_int, c_int, ip, ip, vp, c_int, c_int, c_int]
 
 _COMMON = {
     "tridDmtsvStridedBatchAdjoint": (c_int, _ADJ),
     "tridSmtsvStridedBatchAdjoint": (c_int, _ADJ),
     "tridDmtsvStridedBatchFwdAdj": (c_int, _FWDADJ),
     "tridSmtsvStridedBatchFwdAdj": (c_int, _FWDADJ),
+    "tridDmtsvStridedBatchSplitReduce": (c_int, _SPLIT_REDUCE),
+    "tridSmtsvStridedBatchSplitReduce": (c_int, _SPLIT_REDUCE),
+    "tridDmtsvStridedBatchSplitFinish": (c_int, _SPLIT_FINISH),
+    "tridSmtsvStridedBatchSplitFinish": (c_int, _SPLIT_FINISH),
     "tridDmtsvStridedBatchPadded": (c_int, _PADDED),
     "tridDmtsvStridedBatchPaddedInc": (c_int, _PADDED),
     "tridSmtsvStridedBatchPadded": (c_int, _PADDED),

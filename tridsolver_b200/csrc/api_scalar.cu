@@ -23,7 +23,8 @@ struct ScratchBuf {
   void *ptr = nullptr;
   size_t bytes = 0;
 };
-constexpr int kScratchLevels = 4;
+constexpr int kScratchLevels = 5;
+constexpr int kSplitScratch = kScratchLevels - 1;  // split finish (the solves recurse below it)
 static std::mutex g_scratch_mu;
 static std::vector<ScratchBuf> g_scratch;  // [device * kScratchLevels + level]
 
@@ -463,6 +464,57 @@ template tridStatus_t solve_fwd_adj<double>(const double *, const double *, cons
                                             double *, double *, double *, int, int, const int *,
                                             const int *);
 
+// Systems split along the solve axis across ranks (reference:
+// scalar/src/cuda/trid_cuda_mpi.cu:473-583 and include/trid_mpi_cuda.hpp):
+// this rank's slab reduced to six boundary numbers per system, and the finish
+// from the slabs of every rank gathered in rank order.  The exchange between
+// the two is the caller's (tridsolver_b200/mpi.py: an all-gather over the
+// ranks of the solve dimension).
+template <typename T>
+static tridStatus_t split_reduce(const T *a, const T *b, const T *c, const T *d, int ndim,
+                                 int solvedim, const int *dims, const int *pads, double *bnd) {
+  const int *p[5] = {pads, pads, pads, pads, pads};
+  Geom g;
+  const tridStatus_t st = make_geom(ndim, solvedim, dims, p, false, g);
+  if (st != TRID_STATUS_SUCCESS) return st;
+  if (!aligned_ptr(a) || !aligned_ptr(b) || !aligned_ptr(c) || !aligned_ptr(d) || !bnd ||
+      ((uintptr_t)bnd % sizeof(double)) != 0)
+    return TRID_STATUS_INVALID_VALUE;
+  if (g.nsys == 0) return TRID_STATUS_SUCCESS;
+  if (g.n < 2) return TRID_STATUS_INVALID_VALUE;  // one row: both ends are the same unknown
+  return launch_split_reduce<T>(g, a, b, c, d, bnd, current_stream()) == cudaSuccess
+             ? TRID_STATUS_SUCCESS
+             : TRID_STATUS_EXECUTION_FAILED;
+}
+
+template <typename T, int INC>
+static tridStatus_t split_finish(const T *a, const T *b, const T *c, T *d, T *u, int ndim,
+                                 int solvedim, const int *dims, const int *pads,
+                                 const double *bnd_all, int nranks, int rank) {
+  const int *p[5] = {pads, pads, pads, pads, pads};
+  Geom g;
+  tridStatus_t st = make_geom(ndim, solvedim, dims, p, INC != 0, g);
+  if (st != TRID_STATUS_SUCCESS) return st;
+  if (!aligned_ptr(a) || !aligned_ptr(b) || !aligned_ptr(c) || !aligned_ptr(d) ||
+      (INC && !aligned_ptr(u)) || !bnd_all || ((uintptr_t)bnd_all % sizeof(double)) != 0 ||
+      nranks < 1 || rank < 0 || rank >= nranks)
+    return TRID_STATUS_INVALID_VALUE;
+  if (g.nsys == 0) return TRID_STATUS_SUCCESS;
+  if (g.n < 2) return TRID_STATUS_INVALID_VALUE;
+  const cudaStream_t stream = current_stream();
+  T *saved = nullptr;  // Inc leaves d as it was: the patched entries come back
+  if (INC) {
+    saved = (T *)scratch((size_t)2 * g.nsys * sizeof(T), kSplitScratch);
+    if (!saved) return TRID_STATUS_ALLOC_FAILED;
+  }
+  if (launch_split_patch<T>(g, a, c, d, bnd_all, nranks, rank, saved, stream) != cudaSuccess)
+    return TRID_STATUS_EXECUTION_FAILED;
+  st = solve_level<T, INC>(a, b, c, d, u, ndim, solvedim, dims, p, nullptr, 0, 0);
+  if (INC && launch_split_restore<T>(g, d, saved, stream) != cudaSuccess)
+    return TRID_STATUS_EXECUTION_FAILED;
+  return st;
+}
+
 template tridStatus_t solve_adjoint<float>(const float *, const float *, const float *,
                                            const float *, const float *, float *, float *,
                                            float *, float *, int, int, const int *, const int *);
@@ -565,6 +617,23 @@ extern "C" tridStatus_t tridSmtsvStridedBatchFwdAdj(const float *a, const float 
                                                     int solvedim, int *dims, int *pads) {
   return solve_fwd_adj<float>(a, b, c, d, w, x, da, db, dc, dd, ndim, solvedim, dims, pads);
 }
+
+#define TRID_SPLIT(TAG, T)                                                                     \
+  extern "C" tridStatus_t trid##TAG##mtsvStridedBatchSplitReduce(                              \
+      const T *a, const T *b, const T *c, const T *d, int ndim, int solvedim, const int *dims,  \
+      const int *pads, double *bnd) {                                                          \
+    return split_reduce<T>(a, b, c, d, ndim, solvedim, dims, pads, bnd);                       \
+  }                                                                                            \
+  extern "C" tridStatus_t trid##TAG##mtsvStridedBatchSplitFinish(                              \
+      const T *a, const T *b, const T *c, T *d, T *u, int ndim, int solvedim, const int *dims, \
+      const int *pads, const double *bnd_all, int nranks, int rank, int inc) {                 \
+    return inc ? split_finish<T, 1>(a, b, c, d, u, ndim, solvedim, dims, pads, bnd_all, nranks, \
+                                    rank)                                                      \
+               : split_finish<T, 0>(a, b, c, d, nullptr, ndim, solvedim, dims, pads, bnd_all,  \
+                                    nranks, rank);                                             \
+  }
+TRID_SPLIT(D, double)
+TRID_SPLIT(S, float)
 
 extern "C" void initTridMultiDimBatchSolve(int ndim, int *dims, int *pads) {
   (void)ndim;

@@ -180,4 +180,17 @@ template <typename T, int INC>
 cudaError_t launch_generic(const Geom &g, const T *a, const T *b, const T *c, T *d, T *u,
                            T *work, int64_t work_systems, cudaStream_t st);
 
+// systems split along the solve axis across ranks (kern_split.cu): a slab's
+// six boundary numbers [6][nsys] in FP64; the gathered slabs [nranks][6][nsys]
+// turned into the slab's patched first and last d (old values to `saved`,
+// [2][nsys], when not null); their restore
+template <typename T>
+cudaError_t launch_split_reduce(const Geom &g, const T *a, const T *b, const T *c, const T *d,
+                                double *bnd, cudaStream_t st);
+template <typename T>
+cudaError_t launch_split_patch(const Geom &g, const T *a, const T *c, T *d, const double *bnd_all,
+                               int nranks, int rank, T *saved, cudaStream_t st);
+template <typename T>
+cudaError_t launch_split_restore(const Geom &g, T *d, const T *saved, cudaStream_t st);
+
 }  // namespace tridb200
