@@ -539,6 +539,47 @@ def run_suite(args):
           "gbs": round((40 * total + 8 * (len(lens) + 1)) / (ms * 1e-3) / 1e9, 1)})
     del a, b, c, d, off
 
+    # systems split along the solve dimension: 256^3 FP64 along z cut into P
+    # slabs, every "rank" run in turn on this one GPU (reduce of every slab,
+    # the stacked numbers standing in for the all-gather, finish of every
+    # slab); per-rank time on P GPUs ~ total / P plus the exchange
+    import ctypes as _ct
+
+    from tridsolver_b200 import _lib as _tl
+
+    a, b, c, d = coeffs((UNKNOWNS,), torch.float64)
+    Ls = tb.lib()
+    plane = DIMS[0] * DIMS[1]
+    nsys_z = plane
+
+    def split_step(P):
+        m = DIMS[2] // P
+        loc, pads = _tl.int_array([DIMS[0], DIMS[1], m]), _tl.int_array(DIMS)
+        bn = torch.empty((P, 6, nsys_z), dtype=torch.float64, device=dev)
+        v = lambda t: _ct.c_void_p(t.data_ptr())
+        for r in range(P):
+            o = r * m * plane
+            st = Ls.tridDmtsvStridedBatchSplitReduce(v(a[o:]), v(b[o:]), v(c[o:]), v(d[o:]), 3, 2,
+                                                     loc, pads, v(bn[r]))
+            assert st == 0
+        for r in range(P):
+            o = r * m * plane
+            st = Ls.tridDmtsvStridedBatchSplitFinish(v(a[o:]), v(b[o:]), v(c[o:]), v(d[o:]), None,
+                                                     3, 2, loc, pads, v(bn), P, r, 0)
+            assert st == 0
+
+    tb.scalar._bind_stream(Ls)
+    ms1 = timed(lambda: tb.tridDmtsvStridedBatch(a, b, c, d, None, 3, 2, DIMS, DIMS))
+    for P in (2, 4):
+        ms = timed(lambda: split_step(P))
+        emit({"workload": f"FP64 256^3 along z split into {P} slabs (ranks emulated on one GPU)",
+              "ms_all_slabs": round(ms, 4), "ms_unsplit": round(ms1, 4),
+              "ms_per_rank_estimate": round(ms / P, 4),
+              "gbs_all_slabs": round(40 * UNKNOWNS / (ms * 1e-3) / 1e9, 1),
+              "bytes_per_unknown": "72 (slab reduce 32 + patched local solve 40), plus 48 B per "
+                                   "system and rank exchanged"})
+    del a, b, c, d
+
     # block tridiagonal: M in {2, 4, 8}, N=256, P=32,768 (interleaved layout)
     for M in (2, 4, 8):
         N, P = 256, max(1, int(32768 * sc))
