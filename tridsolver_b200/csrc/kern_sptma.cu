@@ -214,30 +214,33 @@ __global__ void __launch_bounds__(SB * kWarp) strided_part_tma_kernel(
 // copies the tile from shared memory into registers, releases the buffer,
 // issues the next tile's bulk tensor loads, and solves and stores (plain
 // coalesced stores of full lines) while those loads are in flight.
-template <typename T, int M, int SB, int INC, bool FULL>
-__global__ void __launch_bounds__(SB * kWarp, 1) strided_stream_kernel(
+template <typename T, int M, int SB, int NCH, int INC, bool FULL>
+__global__ void __launch_bounds__(SB * NCH, 1) strided_stream_kernel(
     const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mb,
     const __grid_constant__ CUtensorMap mc, const __grid_constant__ CUtensorMap md,
     const __grid_constant__ CUtensorMap mu, Geom g, int solvedim, int box_rows, int nbox,
     uint32_t ntiles, uint32_t ntx_mul, uint32_t ntx_shift, T *__restrict__ d,
     T *__restrict__ u, unsigned *err) {
-  // FULL: n == 32*M and dims[0] a multiple of SB (no row or system guards)
+  // NCH chunks of M rows per system (32, or 16 for short systems: a warp
+  // then solves the interface systems of two tile systems side by side);
+  // FULL: n == NCH*M and dims[0] a multiple of SB (no row or system guards)
   constexpr int NA = INC ? 5 : 4;
+  constexpr int kSysPerWarp = kWarp / NCH;
   extern __shared__ unsigned char smem_raw[];
   __shared__ uint64_t bar;
   T *tile = reinterpret_cast<T *>(smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127));
   constexpr int kAlignElems = 128 / (int)sizeof(T);
-  const size_t tsz = FULL ? (size_t)32 * M * SB
+  const size_t tsz = FULL ? (size_t)NCH * M * SB
                           : (((size_t)box_rows * nbox * SB + kAlignElems - 1) / kAlignElems) *
                                 kAlignElems;
-  T *red = tile + NA * tsz;                                   // [8][32][SB+1]
-  T *sol = red + 8 * kWarp * (SB + 1);                        // [2][32][SB+1]
-  const int rows_cap = FULL ? 32 * M : box_rows * nbox;
+  T *red = tile + NA * tsz;                                   // [8][NCH][SB+1]
+  T *sol = red + 8 * NCH * (SB + 1);                          // [2][NCH][SB+1]
+  const int rows_cap = FULL ? NCH * M : box_rows * nbox;
 
   const int tid = threadIdx.x;
   const int sl = tid % SB;
   const int t = tid / SB;
-  const int n = FULL ? 32 * M : g.n;
+  const int n = FULL ? NCH * M : g.n;
   const uint32_t ntx = (uint32_t)(g.odims[0] + SB - 1) / SB;
   // tile -> coordinates (x0 on axis 0, then the other non-solve axes) and the
   // tile's index along the flattened outer axes; multiply-high divisions
@@ -288,7 +291,7 @@ __global__ void __launch_bounds__(SB * kWarp, 1) strided_stream_kernel(
   const int64_t so = INC ? g.stride[kU] : g.stride[kD];
   T *const out = INC ? u : d;
   auto R = [&](int comp, int chunk, int s) -> T & {
-    return red[((size_t)comp * kWarp + chunk) * (SB + 1) + s];
+    return red[((size_t)comp * NCH + chunk) * (SB + 1) + s];
   };
   for (; blk < ntiles; blk += gridDim.x) {
     // index work that does not need the tile, done while its copy lands: this
@@ -331,18 +334,20 @@ __global__ void __launch_bounds__(SB * kWarp, 1) strided_stream_kernel(
     R(7, t, sl) = L.d;
     __syncthreads();
     {
-      const int w = tid / kWarp;
       const int lane = tid & (kWarp - 1);
-      const Row<T> F2{R(0, lane, w), R(1, lane, w), R(2, lane, w), R(3, lane, w)};
-      const Row<T> L2{R(4, lane, w), R(5, lane, w), R(6, lane, w), R(7, lane, w)};
+      // this lane's system and chunk
+      const int sw = (NCH == kWarp) ? tid / kWarp : (tid / kWarp) * kSysPerWarp + lane / NCH;
+      const int ch = (NCH == kWarp) ? lane : lane & (NCH - 1);
+      const Row<T> F2{R(0, ch, sw), R(1, ch, sw), R(2, ch, sw), R(3, ch, sw)};
+      const Row<T> L2{R(4, ch, sw), R(5, ch, sw), R(6, ch, sw), R(7, ch, sw)};
       T xF, xL;
-      warp_interface_solve(F2, L2, xF, xL, lane);
-      sol[(0 * kWarp + lane) * (SB + 1) + w] = xF;
-      sol[(1 * kWarp + lane) * (SB + 1) + w] = xL;
+      warp_interface_solve<T, NCH>(F2, L2, xF, xL, lane);
+      sol[(0 * NCH + ch) * (SB + 1) + sw] = xF;
+      sol[(1 * NCH + ch) * (SB + 1) + sw] = xL;
     }
     __syncthreads();
-    chunk_backsub<T, M>(al, ga, de, sol[(0 * kWarp + t) * (SB + 1) + sl],
-                        sol[(1 * kWarp + t) * (SB + 1) + sl]);
+    chunk_backsub<T, M>(al, ga, de, sol[(0 * NCH + t) * (SB + 1) + sl],
+                        sol[(1 * NCH + t) * (SB + 1) + sl]);
     if (valid) {
 #pragma unroll
       for (int j = 0; j < M; ++j) {
@@ -353,30 +358,30 @@ __global__ void __launch_bounds__(SB * kWarp, 1) strided_stream_kernel(
   }
 }
 
-template <typename T, int M, int SB, int INC>
+template <typename T, int M, int SB, int NCH, int INC>
 static cudaError_t launch_stream(const CUtensorMap *maps, const Geom &g, int solvedim,
                                  int box_rows, int nbox, int64_t blocks, T *d, T *u,
                                  unsigned *err, cudaStream_t st, int optin) {
   constexpr int NA = INC ? 5 : 4;
   constexpr int kAlignElems = 128 / (int)sizeof(T);
   const size_t tsz = (((size_t)box_rows * nbox * SB + kAlignElems - 1) / kAlignElems) * kAlignElems;
-  const size_t smem = (size_t)NA * tsz * sizeof(T) + (size_t)10 * kWarp * (SB + 1) * sizeof(T) + 128;
-  if (smem + 64 > (size_t)optin || !g.fastdiv) return cudaErrorNotSupported;
-  const bool full = g.n == 32 * M && g.odims[0] % SB == 0;
-  auto kern = full ? strided_stream_kernel<T, M, SB, INC, true>
-                   : strided_stream_kernel<T, M, SB, INC, false>;
+  const size_t smem = (size_t)NA * tsz * sizeof(T) + (size_t)10 * NCH * (SB + 1) * sizeof(T) + 128;
+  if (smem + 64 > (size_t)optin || !g.fastdiv || g.n > NCH * M) return cudaErrorNotSupported;
+  const bool full = g.n == NCH * M && g.odims[0] % SB == 0;
+  auto kern = full ? strided_stream_kernel<T, M, SB, NCH, INC, true>
+                   : strided_stream_kernel<T, M, SB, NCH, INC, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0, dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SB * kWarp, smem) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SB * NCH, smem) != cudaSuccess ||
       per_sm < 1)
     return cudaErrorNotSupported;
   const int64_t grid = std::min<int64_t>(blocks, (int64_t)per_sm * sms);
   uint32_t ntx_mul = 0, ntx_shift = 0;
   fastdiv_setup((uint32_t)((g.odims[0] + SB - 1) / SB), ntx_mul, ntx_shift);
-  kern<<<dim3((unsigned)grid), dim3(SB * kWarp), smem, st>>>(
+  kern<<<dim3((unsigned)grid), dim3(SB * NCH), smem, st>>>(
       maps[0], maps[1], maps[2], maps[3], maps[4], g, solvedim, box_rows, nbox, (uint32_t)blocks,
       ntx_mul, ntx_shift, d, u, err);
   return cudaGetLastError();
@@ -421,9 +426,11 @@ static cudaError_t launch_sptma_sb(const CUtensorMap *maps, const Geom &g, int s
   // (at most 8 rows per thread: 16 would spill at one CTA per SM)
   if (spc * (int)sizeof(T) >= 128) {
     if constexpr (M <= 8 && sizeof(T) == 8) {
-      if (spc == 16) return launch_stream<T, M, 16, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
+      if (spc == 16) return launch_stream<T, M, 16, 32, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
+      // short FP64 systems (16 chunks of M rows): 32 systems, 256-byte rows
+      if (spc == 32) return launch_stream<T, M, 32, 16, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
     } else if constexpr (M <= 8) {
-      if (spc == 32) return launch_stream<T, M, 32, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
+      if (spc == 32) return launch_stream<T, M, 32, 32, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
     }
     return cudaErrorNotSupported;
   }
@@ -440,6 +447,12 @@ cudaError_t launch_strided_part_tma(const Geom &g, const int *dims, const int *c
                                     int ndim, int solvedim, const T *a, const T *b, const T *c,
                                     T *d, T *u, int chunk, int spc, bool prefetch,
                                     unsigned *err, cudaStream_t st) {
+  // FP64 full-line tiles of systems of at most 128 rows: 32 systems x 16
+  // chunks of chunk rows (as many bytes in flight per SM as 256-row tiles)
+  if (sizeof(T) == 8 && spc == 16 && g.n <= 128 && dims[0] >= 32) {
+    spc = 32;
+    chunk = g.n <= 32 ? 2 : (g.n <= 64 ? 4 : 8);
+  }
   if (solvedim < 1 || ndim > 5 || g.n > 32 * chunk || dims[0] < spc) return cudaErrorNotSupported;
   const int box_rows = g.n < 256 ? g.n : 256;
   const int nbox = (g.n + box_rows - 1) / box_rows;

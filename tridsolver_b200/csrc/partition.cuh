@@ -239,17 +239,62 @@ __device__ __forceinline__ void chunk_backsub(const T (&al)[M], const T (&ga)[M]
 // span: a power of two >= the number of lanes holding non-identity rows
 // (lanes at or past it hold identity rows); PCR stops after log2(span)
 // steps, when every such row is decoupled.
-template <typename T>
+template <typename T, int W = kWarp>
 __device__ __forceinline__ void warp_interface_solve(const Row<T> &F, const Row<T> &L, T &xF,
-                                                     T &xL, int lane, int span = kWarp) {
+                                                     T &xL, int lane, int span = W) {
+  // W < 32: the warp holds 32/W independent systems of W lanes each (lane
+  // groups of W; shuffles stay inside a group)
+  static_assert(W == 8 || W == 16 || W == 32, "lane groups of 8, 16 or 32");
   constexpr unsigned kFull = 0xffffffffu;
+  if constexpr (W == kWarp) {  // the whole warp: the plain shuffles
+    const T ifb = rcp(F.b);
+    T nfa = __shfl_down_sync(kFull, F.a, 1);
+    T nfi = __shfl_down_sync(kFull, ifb, 1);
+    T nfc = __shfl_down_sync(kFull, F.c, 1);
+    T nfd = __shfl_down_sync(kFull, F.d, 1);
+    if (lane == kWarp - 1) {
+      nfa = T(0);
+      nfi = T(1);
+      nfc = T(0);
+      nfd = T(0);
+    }
+    const T p = L.a * ifb;
+    const T q = L.c * nfi;
+    T ra = -p * F.a;
+    T rb = L.b - p * F.c - q * nfa;
+    T rc = -q * nfc;
+    T rd = L.d - p * F.d - q * nfd;
+#pragma unroll
+    for (int s = 1; s < kWarp; s <<= 1) {
+      if (s >= span) break;
+      const T ib = rcp(rb);
+      const T sa = ra * ib, sc = rc * ib, sd = rd * ib;
+      const T ua = __shfl_up_sync(kFull, sa, s);
+      const T uc = __shfl_up_sync(kFull, sc, s);
+      const T ud = __shfl_up_sync(kFull, sd, s);
+      const T da = __shfl_down_sync(kFull, sa, s);
+      const T dc = __shfl_down_sync(kFull, sc, s);
+      const T dd = __shfl_down_sync(kFull, sd, s);
+      const T k1 = (lane >= s) ? ra : T(0);
+      const T k2 = (lane + s < kWarp) ? rc : T(0);
+      ra = -k1 * ua;
+      rc = -k2 * dc;
+      rb = rb - k1 * uc - k2 * da;
+      rd = rd - k1 * ud - k2 * dd;
+    }
+    xL = rd * rcp(rb);
+    const T lprev = __shfl_up_sync(kFull, xL, 1);
+    xF = (F.d - (lane > 0 ? F.a * lprev : T(0)) - F.c * xL) * ifb;
+    return;
+  }
+  const int ll = lane & (W - 1);  // lane within its group
   const T ifb = rcp(F.b);
   // F row of the next chunk (its pivot as a reciprocal)
-  T nfa = __shfl_down_sync(kFull, F.a, 1);
-  T nfi = __shfl_down_sync(kFull, ifb, 1);
-  T nfc = __shfl_down_sync(kFull, F.c, 1);
-  T nfd = __shfl_down_sync(kFull, F.d, 1);
-  if (lane == kWarp - 1) {
+  T nfa = __shfl_down_sync(kFull, F.a, 1, W);
+  T nfi = __shfl_down_sync(kFull, ifb, 1, W);
+  T nfc = __shfl_down_sync(kFull, F.c, 1, W);
+  T nfd = __shfl_down_sync(kFull, F.d, 1, W);
+  if (ll == W - 1) {
     nfa = T(0);
     nfi = T(1);
     nfc = T(0);
@@ -262,29 +307,29 @@ __device__ __forceinline__ void warp_interface_solve(const Row<T> &F, const Row<
   T rb = L.b - p * F.c - q * nfa;
   T rc = -q * nfc;
   T rd = L.d - p * F.d - q * nfd;
-  // parallel cyclic reduction over the 32 lanes; each row sends its
+  // parallel cyclic reduction over the W lanes; each row sends its
   // coefficients pre-divided by its pivot, so a neighbour needs 3 values
 #pragma unroll
-  for (int s = 1; s < kWarp; s <<= 1) {
+  for (int s = 1; s < W; s <<= 1) {
     if (s >= span) break;
     const T ib = rcp(rb);
     const T sa = ra * ib, sc = rc * ib, sd = rd * ib;
-    const T ua = __shfl_up_sync(kFull, sa, s);
-    const T uc = __shfl_up_sync(kFull, sc, s);
-    const T ud = __shfl_up_sync(kFull, sd, s);
-    const T da = __shfl_down_sync(kFull, sa, s);
-    const T dc = __shfl_down_sync(kFull, sc, s);
-    const T dd = __shfl_down_sync(kFull, sd, s);
-    const T k1 = (lane >= s) ? ra : T(0);
-    const T k2 = (lane + s < kWarp) ? rc : T(0);
+    const T ua = __shfl_up_sync(kFull, sa, s, W);
+    const T uc = __shfl_up_sync(kFull, sc, s, W);
+    const T ud = __shfl_up_sync(kFull, sd, s, W);
+    const T da = __shfl_down_sync(kFull, sa, s, W);
+    const T dc = __shfl_down_sync(kFull, sc, s, W);
+    const T dd = __shfl_down_sync(kFull, sd, s, W);
+    const T k1 = (ll >= s) ? ra : T(0);
+    const T k2 = (ll + s < W) ? rc : T(0);
     ra = -k1 * ua;
     rc = -k2 * dc;
     rb = rb - k1 * uc - k2 * da;
     rd = rd - k1 * ud - k2 * dd;
   }
   xL = rd * rcp(rb);
-  const T lprev = __shfl_up_sync(kFull, xL, 1);
-  xF = (F.d - (lane > 0 ? F.a * lprev : T(0)) - F.c * xL) * ifb;
+  const T lprev = __shfl_up_sync(kFull, xL, 1, W);
+  xF = (F.d - (ll > 0 ? F.a * lprev : T(0)) - F.c * xL) * ifb;
 }
 
 // The interface system of one warp with several right-hand sides: NR
