@@ -418,19 +418,25 @@ static cudaError_t launch_sptma(const CUtensorMap *maps, const Geom &g, int solv
 
 template <typename T, int M, int INC>
 static cudaError_t launch_sptma_sb(const CUtensorMap *maps, const Geom &g, int solvedim,
-                                   int box_rows, int nbox, int spc, int64_t ntiles_rest, T *d,
-                                   T *u, unsigned *err, cudaStream_t st, int optin, bool prefetch) {
+                                   int box_rows, int nbox, int spc, int nch, int64_t ntiles_rest,
+                                   T *d, T *u, unsigned *err, cudaStream_t st, int optin,
+                                   bool prefetch) {
   const int64_t blocks = ((g.odims[0] + spc - 1) / spc) * ntiles_rest;
   if (blocks > 0x7fffffff || blocks == 0) return cudaErrorNotSupported;
   // full-line tiles (16 FP64 / 32 FP32 systems) stream through one persistent CTA per SM
   // (at most 8 rows per thread: 16 would spill at one CTA per SM)
   if (spc * (int)sizeof(T) >= 128) {
-    if constexpr (M <= 8 && sizeof(T) == 8) {
-      if (spc == 16) return launch_stream<T, M, 16, 32, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
-      // short FP64 systems (16 chunks of M rows): 32 systems, 256-byte rows
-      if (spc == 32) return launch_stream<T, M, 32, 16, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
-    } else if constexpr (M <= 8) {
-      if (spc == 32) return launch_stream<T, M, 32, 32, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
+    if constexpr (sizeof(T) == 8) {
+      if constexpr (M <= 8) {
+        if (spc == 16) return launch_stream<T, M, 16, 32, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
+        // short FP64 systems (16 chunks of M rows): 32 systems, 256-byte rows
+        if (spc == 32 && nch == 16) return launch_stream<T, M, 32, 16, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
+      }
+    } else {
+      if (spc == 32 && nch == 16) return launch_stream<T, M, 32, 16, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
+      if constexpr (M <= 8) {
+        if (spc == 32) return launch_stream<T, M, 32, 32, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
+      }
     }
     return cudaErrorNotSupported;
   }
@@ -447,11 +453,16 @@ cudaError_t launch_strided_part_tma(const Geom &g, const int *dims, const int *c
                                     int ndim, int solvedim, const T *a, const T *b, const T *c,
                                     T *d, T *u, int chunk, int spc, bool prefetch,
                                     unsigned *err, cudaStream_t st) {
-  // FP64 full-line tiles of systems of at most 128 rows: 32 systems x 16
-  // chunks of chunk rows (as many bytes in flight per SM as 256-row tiles)
-  if (sizeof(T) == 8 && spc == 16 && g.n <= 128 && dims[0] >= 32) {
+  // Full-line tiles with 16 chunks per system (a warp solves two interface
+  // systems): FP64 systems of at most 128 rows as 32 systems x 16 chunks (as
+  // many bytes in flight per SM as 256-row tiles), FP32 systems of at most
+  // 256 rows as 32 systems x 16 chunks (512 threads instead of 1024)
+  int nch = 32;
+  if (dims[0] >= 32 && ((sizeof(T) == 8 && spc == 16 && g.n <= 128) ||
+                        (sizeof(T) == 4 && spc == 32 && g.n <= 256))) {
     spc = 32;
-    chunk = g.n <= 32 ? 2 : (g.n <= 64 ? 4 : 8);
+    nch = 16;
+    chunk = g.n <= 32 ? 2 : (g.n <= 64 ? 4 : (g.n <= 128 ? 8 : 16));
   }
   if (solvedim < 1 || ndim > 5 || g.n > 32 * chunk || dims[0] < spc) return cudaErrorNotSupported;
   const int box_rows = g.n < 256 ? g.n : 256;
@@ -481,10 +492,10 @@ cudaError_t launch_strided_part_tma(const Geom &g, const int *dims, const int *c
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const int64_t rest = g.nsys / dims[0];
   switch (chunk) {
-    case 2: return launch_sptma_sb<T, 2, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, d, u, err, st, optin, prefetch);
-    case 4: return launch_sptma_sb<T, 4, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, d, u, err, st, optin, prefetch);
-    case 8: return launch_sptma_sb<T, 8, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, d, u, err, st, optin, prefetch);
-    case 16: return launch_sptma_sb<T, 16, INC>(maps, g, solvedim, box_rows, nbox, spc, rest, d, u, err, st, optin, prefetch);
+    case 2: return launch_sptma_sb<T, 2, INC>(maps, g, solvedim, box_rows, nbox, spc, nch, rest, d, u, err, st, optin, prefetch);
+    case 4: return launch_sptma_sb<T, 4, INC>(maps, g, solvedim, box_rows, nbox, spc, nch, rest, d, u, err, st, optin, prefetch);
+    case 8: return launch_sptma_sb<T, 8, INC>(maps, g, solvedim, box_rows, nbox, spc, nch, rest, d, u, err, st, optin, prefetch);
+    case 16: return launch_sptma_sb<T, 16, INC>(maps, g, solvedim, box_rows, nbox, spc, nch, rest, d, u, err, st, optin, prefetch);
     default: return cudaErrorNotSupported;
   }
 }
