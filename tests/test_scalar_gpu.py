@@ -188,6 +188,17 @@ def test_strided_tma_staged(dtype, n, solvedim):
 
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("n", [2, 5, 16, 17, 32, 33, 64, 65, 100, 128])
+@pytest.mark.parametrize("solvedim,inc", [(1, False), (2, False), (2, True)])
+def test_strided_short_wide_tiles(dtype, n, solvedim, inc):
+    """Short strided systems with an axis 0 of at least 64: tiles of 64
+    systems x 8 chunks (FP64 up to 64 rows, FP32 up to 128) or 32 x 16; axis 0
+    of 70 leaves a partial last tile."""
+    dims = [70, n, 3] if solvedim == 1 else [70, 3, n]
+    run_case(np.random.default_rng(n + 3 * solvedim + inc), dtype, dims, solvedim, inc=inc)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
 @pytest.mark.parametrize("spc", [4, 8, 16, 32])
 @pytest.mark.parametrize("inc", [False, True])
 @pytest.mark.parametrize("dims,solvedim,pads", [

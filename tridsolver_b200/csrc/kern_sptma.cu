@@ -431,9 +431,11 @@ static cudaError_t launch_sptma_sb(const CUtensorMap *maps, const Geom &g, int s
         if (spc == 16) return launch_stream<T, M, 16, 32, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
         // short FP64 systems (16 chunks of M rows): 32 systems, 256-byte rows
         if (spc == 32 && nch == 16) return launch_stream<T, M, 32, 16, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
+        if (spc == 64 && nch == 8) return launch_stream<T, M, 64, 8, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
       }
     } else {
       if (spc == 32 && nch == 16) return launch_stream<T, M, 32, 16, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
+      if (spc == 64 && nch == 8) return launch_stream<T, M, 64, 8, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
       if constexpr (M <= 8) {
         if (spc == 32) return launch_stream<T, M, 32, 32, INC>(maps, g, solvedim, box_rows, nbox, blocks, d, u, err, st, optin);
       }
@@ -458,8 +460,15 @@ cudaError_t launch_strided_part_tma(const Geom &g, const int *dims, const int *c
   // many bytes in flight per SM as 256-row tiles), FP32 systems of at most
   // 256 rows as 32 systems x 16 chunks (512 threads instead of 1024)
   int nch = 32;
-  if (dims[0] >= 32 && ((sizeof(T) == 8 && spc == 16 && g.n <= 128) ||
-                        (sizeof(T) == 4 && spc == 32 && g.n <= 256))) {
+  const bool wide = (sizeof(T) == 8 && spc == 16) || (sizeof(T) == 4 && spc == 32);
+  if (wide && dims[0] >= 64 && g.n <= (sizeof(T) == 8 ? 64 : 128)) {
+    // shorter still (FP64 up to 64 rows, FP32 up to 128): 64 systems x 8
+    // chunks, four interface systems per warp -- 128 KB tiles again
+    spc = 64;
+    nch = 8;
+    chunk = g.n <= 16 ? 2 : (g.n <= 32 ? 4 : (g.n <= 64 ? 8 : 16));
+  } else if (dims[0] >= 32 && ((sizeof(T) == 8 && spc == 16 && g.n <= 128) ||
+                               (sizeof(T) == 4 && spc == 32 && g.n <= 256))) {
     spc = 32;
     nch = 16;
     chunk = g.n <= 32 ? 2 : (g.n <= 64 ? 4 : (g.n <= 128 ? 8 : 16));
