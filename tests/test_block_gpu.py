@@ -71,6 +71,29 @@ def test_block_caller_scratch_and_unused_blocks():
     assert rel_err(x.cpu().numpy(), expect) <= 1e-12
 
 
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-12), (np.float32, 1e-5)])
+def test_block_m2_unused_blocks_and_misaligned(dtype, tol):
+    """M = 2 (one thread per system when every array is 16-byte aligned):
+    A_0 and C_{N-1} are never read; arrays one element off a 16-byte boundary
+    take the M-lanes kernel and give the same answer."""
+    rng = np.random.default_rng(22)
+    N, P, M = 37, 300, 2
+    A, B, C, d = block_system(rng, N, P, M)
+    expect = oracle.btsv(A, B, C, d, N, P, M, layout=0).reshape(N, P, M)
+    A2, C2 = A.copy(), C.copy()
+    A2[0] = np.nan
+    C2[N - 1] = np.inf
+    x = block.btsv(*(cuda(v, dtype) for v in (A2, B, C2, d)))
+    assert rel_err(x.cpu().numpy(), expect) <= tol
+
+    def off(v):  # the same values one element past a 16-byte boundary
+        flat = np.concatenate([[0.0], v.ravel()]).astype(dtype)
+        return torch.from_numpy(flat).cuda()[1:].view(v.shape)
+
+    x2 = block.btsv(off(A2), off(B), off(C2), off(d), x=off(np.zeros_like(d)))
+    assert rel_err(x2.cpu().numpy(), expect) <= tol
+
+
 def test_reference_cxx_entry_point():
     """dbtsv_gpu(A, B, C, d, Cstar, dstar, u, N, P, blkdim) with C++ linkage."""
     rng = np.random.default_rng(4)

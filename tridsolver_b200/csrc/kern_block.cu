@@ -352,6 +352,260 @@ __global__ void __launch_bounds__(128) block_thomas_kernel(BlkArgs<T> a) {
   }
 }
 
+// M = 2 forward: one thread per system with the 2 x 2 algebra in registers
+// (the M-lanes kernel above spends each step on shared-memory row
+// broadcasts, and gives only 2 lanes per system: 14 warps per SM at P =
+// 32,768).  Consecutive threads take consecutive systems, whose blocks are
+// adjacent in the interleaved layout, so every 16-byte load and store of a
+// warp is one contiguous 1 KB stretch.  Loads run D block rows ahead in a
+// register ring.  X_n^{-1} by the adjugate (no pivoting, as the M-lanes
+// kernel and the reference GPU kernel: block diagonal dominance).
+template <typename T>
+struct Blk2Row {
+  T A[4], B[4], C[4], d[2];
+};
+
+template <typename T>
+__device__ __forceinline__ void blk2_ld4(const T *p, T (&r)[4]) {
+  if constexpr (sizeof(T) == 8) {
+    const double2 u = *reinterpret_cast<const double2 *>(p);
+    const double2 v = *reinterpret_cast<const double2 *>(p + 2);
+    r[0] = u.x; r[1] = u.y; r[2] = v.x; r[3] = v.y;
+  } else {
+    const float4 u = *reinterpret_cast<const float4 *>(p);
+    r[0] = u.x; r[1] = u.y; r[2] = u.z; r[3] = u.w;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void blk2_ld2(const T *p, T (&r)[2]) {
+  if constexpr (sizeof(T) == 8) {
+    const double2 u = *reinterpret_cast<const double2 *>(p);
+    r[0] = u.x; r[1] = u.y;
+  } else {
+    const float2 u = *reinterpret_cast<const float2 *>(p);
+    r[0] = u.x; r[1] = u.y;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void blk2_st2(T *p, T x, T y) {
+  if constexpr (sizeof(T) == 8)
+    *reinterpret_cast<double2 *>(p) = make_double2(x, y);
+  else
+    *reinterpret_cast<float2 *>(p) = make_float2(x, y);
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(128) block2_kernel(BlkArgs<T> a) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.P) return;
+  const int64_t P = a.P;
+  const int N = a.N;
+  auto bx = [&](int n) { return ((int64_t)n * P + p) * 4; };
+  auto vx = [&](int n) { return ((int64_t)n * P + p) * 2; };
+  auto fetch = [&](int n, Blk2Row<T> &s) {
+    if (n >= N) return;
+    blk2_ld4(a.B + bx(n), s.B);
+    if (n > 0) {
+      blk2_ld4(a.A + bx(n), s.A);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) s.A[j] = T(0);
+    }
+    if (n < N - 1) {
+      blk2_ld4(a.C + bx(n), s.C);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) s.C[j] = T(0);
+    }
+    blk2_ld2(a.d + vx(n), s.d);
+  };
+  Blk2Row<T> ring[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) fetch(k, ring[k]);
+  // C'_{n-1} (row major) and d'_{n-1}
+  T c0 = T(0), c1 = T(0), c2 = T(0), c3 = T(0), e0 = T(0), e1 = T(0);
+  for (int n0 = 0; n0 < N; n0 += D) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      const int n = n0 + k;
+      if (n >= N) break;
+      const Blk2Row<T> r = ring[k];
+      fetch(n + D, ring[k]);
+      // X = B - A C', rhs = d - A d'
+      const T x0 = r.B[0] - (r.A[0] * c0 + r.A[1] * c2);
+      const T x1 = r.B[1] - (r.A[0] * c1 + r.A[1] * c3);
+      const T x2 = r.B[2] - (r.A[2] * c0 + r.A[3] * c2);
+      const T x3 = r.B[3] - (r.A[2] * c1 + r.A[3] * c3);
+      const T h0 = r.d[0] - (r.A[0] * e0 + r.A[1] * e1);
+      const T h1 = r.d[1] - (r.A[2] * e0 + r.A[3] * e1);
+      const T inv = rcp(x0 * x3 - x1 * x2);
+      const T i0 = x3 * inv, i1 = -x1 * inv, i2 = -x2 * inv, i3 = x0 * inv;
+      c0 = i0 * r.C[0] + i1 * r.C[2];
+      c1 = i0 * r.C[1] + i1 * r.C[3];
+      c2 = i2 * r.C[0] + i3 * r.C[2];
+      c3 = i2 * r.C[1] + i3 * r.C[3];
+      e0 = i0 * h0 + i1 * h1;
+      e1 = i2 * h0 + i3 * h1;
+      blk2_st2(a.Cs + bx(n), c0, c1);
+      blk2_st2(a.Cs + bx(n) + 2, c2, c3);
+      blk2_st2(a.ds + vx(n), e0, e1);
+    }
+  }
+  // backward: x_{N-1} = d'_{N-1}; x_n = d'_n - C'_n x_{n+1}
+  T u0 = e0, u1 = e1;
+  blk2_st2(a.x + vx(N - 1), u0, u1);
+  struct Back {
+    T c[4], d[2];
+  };
+  auto fetch_back = [&](int n, Back &s) {
+    if (n < 0) return;
+    blk2_ld4(a.Cs + bx(n), s.c);
+    blk2_ld2(a.ds + vx(n), s.d);
+  };
+  Back bring[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) fetch_back(N - 2 - k, bring[k]);
+  for (int n0 = N - 2; n0 >= 0; n0 -= D) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      const int n = n0 - k;
+      if (n < 0) break;
+      const Back b = bring[k];
+      fetch_back(n - D, bring[k]);
+      const T v0 = b.d[0] - (b.c[0] * u0 + b.c[1] * u1);
+      const T v1 = b.d[1] - (b.c[2] * u0 + b.c[3] * u1);
+      u0 = v0;
+      u1 = v1;
+      blk2_st2(a.x + vx(n), u0, u1);
+    }
+  }
+}
+
+// M = 2 adjoint, one thread per system: the transposed block system
+// (sub-diagonal C_{n-1}^T, diagonal B_n^T, super-diagonal A_{n+1}^T) with
+// right-hand side w, then the gradients from g (its solution) and u in the
+// backward sweep: dA_n = -g_n u_{n-1}^T, dB_n = -g_n u_n^T,
+// dC_n = -g_n u_{n+1}^T, dd_n = g_n.
+template <typename T, int D>
+__global__ void __launch_bounds__(128) block2_adj_kernel(BlkArgs<T> a) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.P) return;
+  const int64_t P = a.P;
+  const int N = a.N;
+  auto bx = [&](int n) { return ((int64_t)n * P + p) * 4; };
+  auto vx = [&](int n) { return ((int64_t)n * P + p) * 2; };
+  // the forward sweep's blocks, as read (transposed in the arithmetic)
+  auto fetch = [&](int n, Blk2Row<T> &s) {
+    if (n >= N) return;
+    blk2_ld4(a.B + bx(n), s.B);
+    if (n > 0) {
+      blk2_ld4(a.C + bx(n - 1), s.A);  // C_{n-1}: the sub-diagonal, transposed
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) s.A[j] = T(0);
+    }
+    if (n < N - 1) {
+      blk2_ld4(a.A + bx(n + 1), s.C);  // A_{n+1}: the super-diagonal, transposed
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) s.C[j] = T(0);
+    }
+    blk2_ld2(a.d + vx(n), s.d);  // w
+  };
+  Blk2Row<T> ring[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) fetch(k, ring[k]);
+  T c0 = T(0), c1 = T(0), c2 = T(0), c3 = T(0), e0 = T(0), e1 = T(0);
+  for (int n0 = 0; n0 < N; n0 += D) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      const int n = n0 + k;
+      if (n >= N) break;
+      const Blk2Row<T> r = ring[k];
+      fetch(n + D, ring[k]);
+      // L = C_{n-1}^T = [A0 A2; A1 A3] of the stage; X = B^T - L C'
+      const T l0 = r.A[0], l1 = r.A[2], l2 = r.A[1], l3 = r.A[3];
+      const T x0 = r.B[0] - (l0 * c0 + l1 * c2);
+      const T x1 = r.B[2] - (l0 * c1 + l1 * c3);
+      const T x2 = r.B[1] - (l2 * c0 + l3 * c2);
+      const T x3 = r.B[3] - (l2 * c1 + l3 * c3);
+      const T h0 = r.d[0] - (l0 * e0 + l1 * e1);
+      const T h1 = r.d[1] - (l2 * e0 + l3 * e1);
+      const T inv = rcp(x0 * x3 - x1 * x2);
+      const T i0 = x3 * inv, i1 = -x1 * inv, i2 = -x2 * inv, i3 = x0 * inv;
+      // R = A_{n+1}^T = [C0 C2; C1 C3] of the stage
+      const T r0 = r.C[0], r1 = r.C[2], r2 = r.C[1], r3 = r.C[3];
+      c0 = i0 * r0 + i1 * r2;
+      c1 = i0 * r1 + i1 * r3;
+      c2 = i2 * r0 + i3 * r2;
+      c3 = i2 * r1 + i3 * r3;
+      e0 = i0 * h0 + i1 * h1;
+      e1 = i2 * h0 + i3 * h1;
+      blk2_st2(a.Cs + bx(n), c0, c1);
+      blk2_st2(a.Cs + bx(n) + 2, c2, c3);
+      blk2_st2(a.ds + vx(n), e0, e1);
+    }
+  }
+  // backward: g_{N-1} = d'_{N-1}; g_n = d'_n - C'_n g_{n+1}; gradients of row n
+  struct Back {
+    T c[4], d[2], up[2];
+  };
+  auto fetch_back = [&](int n, Back &s) {
+    if (n < 0) return;
+    if (n < N - 1) {
+      blk2_ld4(a.Cs + bx(n), s.c);
+      blk2_ld2(a.ds + vx(n), s.d);
+    }
+    if (n > 0) {
+      blk2_ld2(a.u + vx(n - 1), s.up);
+    } else {
+      s.up[0] = T(0);
+      s.up[1] = T(0);
+    }
+  };
+  T g0 = e0, g1 = e1;
+  T un0 = T(0), un1 = T(0);  // u_{n+1}
+  T uc[2];
+  blk2_ld2(a.u + vx(N - 1), uc);
+  Back bring[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) fetch_back(N - 1 - k, bring[k]);
+  for (int n0 = N - 1; n0 >= 0; n0 -= D) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      const int n = n0 - k;
+      if (n < 0) break;
+      const Back b = bring[k];
+      fetch_back(n - D, bring[k]);
+      if (n < N - 1) {
+        const T v0 = b.d[0] - (b.c[0] * g0 + b.c[1] * g1);
+        const T v1 = b.d[1] - (b.c[2] * g0 + b.c[3] * g1);
+        g0 = v0;
+        g1 = v1;
+      }
+      if (a.dd) blk2_st2(a.dd + vx(n), g0, g1);
+      if (a.dA) {
+        blk2_st2(a.dA + bx(n), -g0 * b.up[0], -g0 * b.up[1]);
+        blk2_st2(a.dA + bx(n) + 2, -g1 * b.up[0], -g1 * b.up[1]);
+      }
+      if (a.dB) {
+        blk2_st2(a.dB + bx(n), -g0 * uc[0], -g0 * uc[1]);
+        blk2_st2(a.dB + bx(n) + 2, -g1 * uc[0], -g1 * uc[1]);
+      }
+      if (a.dC) {
+        blk2_st2(a.dC + bx(n), -g0 * un0, -g0 * un1);
+        blk2_st2(a.dC + bx(n) + 2, -g1 * un0, -g1 * un1);
+      }
+      un0 = uc[0];
+      un1 = uc[1];
+      uc[0] = b.up[0];
+      uc[1] = b.up[1];
+    }
+  }
+}
+
 template <typename T, bool ADJ>
 cudaError_t launch_block(const BlkArgs<T> &a, int M, cudaStream_t st) {
   auto go = [&](auto kern, int m) {
@@ -362,6 +616,22 @@ cudaError_t launch_block(const BlkArgs<T> &a, int M, cudaStream_t st) {
     kern<<<dim3((unsigned)blocks), dim3(128), 0, st>>>(a);
     return cudaGetLastError();
   };
+  {
+    // M = 2, one thread per system: every array 16-byte aligned (a null
+    // gradient output counts as aligned)
+    const uintptr_t bits = (uintptr_t)a.A | (uintptr_t)a.B | (uintptr_t)a.C | (uintptr_t)a.d |
+                           (uintptr_t)a.u | (uintptr_t)a.x | (uintptr_t)a.dA | (uintptr_t)a.dB |
+                           (uintptr_t)a.dC | (uintptr_t)a.dd | (uintptr_t)a.Cs | (uintptr_t)a.ds;
+    if (M == 2 && (bits & 15) == 0) {
+      const int64_t blocks = (a.P + 127) / 128;
+      if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
+      if constexpr (ADJ)
+        block2_adj_kernel<T, 4><<<dim3((unsigned)blocks), dim3(128), 0, st>>>(a);
+      else
+        block2_kernel<T, 4><<<dim3((unsigned)blocks), dim3(128), 0, st>>>(a);
+      return cudaGetLastError();
+    }
+  }
   switch (M) {
     case 1: return go(block_thomas_kernel<T, 1, ADJ>, 1);
     case 2: return go(block_thomas_kernel<T, 2, ADJ>, 2);
