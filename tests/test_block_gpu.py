@@ -71,13 +71,15 @@ def test_block_caller_scratch_and_unused_blocks():
     assert rel_err(x.cpu().numpy(), expect) <= 1e-12
 
 
+@pytest.mark.parametrize("M", [2, 3, 4])
 @pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-12), (np.float32, 1e-5)])
-def test_block_m2_unused_blocks_and_misaligned(dtype, tol):
-    """M = 2 (one thread per system when every array is 16-byte aligned):
-    A_0 and C_{N-1} are never read; arrays one element off a 16-byte boundary
-    take the M-lanes kernel and give the same answer."""
-    rng = np.random.default_rng(22)
-    N, P, M = 37, 300, 2
+def test_block_register_unused_blocks_and_misaligned(dtype, tol, M):
+    """M = 2..4 (one thread per system; for M = 2, 4 only when every array is
+    16-byte aligned): A_0 and C_{N-1} are never read; arrays one element off
+    a 16-byte boundary take the M-lanes kernel (M = 2, 4) and give the same
+    answer."""
+    rng = np.random.default_rng(22 + M)
+    N, P = 37, 300
     A, B, C, d = block_system(rng, N, P, M)
     expect = oracle.btsv(A, B, C, d, N, P, M, layout=0).reshape(N, P, M)
     A2, C2 = A.copy(), C.copy()
@@ -158,3 +160,36 @@ def test_block_autograd_against_dense():
     for g1, g2 in zip(leaves, ref):
         err = float((g1.grad - g2.grad).abs().max() / g2.grad.abs().max())
         assert err <= 1e-10, err
+
+
+@pytest.mark.parametrize("M", [2, 3, 4])
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-12), (np.float32, 1e-5)])
+@pytest.mark.parametrize("aligned", [True, False])
+def test_block_adjoint_register_kernels(M, dtype, tol, aligned):
+    """The one-thread-per-system adjoints (M = 2..4) over more systems than a
+    CTA holds, and with every array one element off a 16-byte boundary (the
+    M-lanes kernel for M = 2, 4)."""
+    rng = np.random.default_rng(70 + M)
+    N, P = 29, 333
+    A, B, C, d = block_system(rng, N, P, M)
+    w = rng.standard_normal((N, P, M))
+    u = oracle.btsv(A, B, C, d, N, P, M, layout=0).reshape(N, P, M)
+    g = oracle.btsv(A, B, C, w, N, P, M, layout=0, transpose=True).reshape(N, P, M)
+    exp_dA = -np.einsum("npi,npj->npij", g, np.concatenate([np.zeros((1, P, M)), u[:-1]]))
+    exp_dB = -np.einsum("npi,npj->npij", g, u)
+    exp_dC = -np.einsum("npi,npj->npij", g, np.concatenate([u[1:], np.zeros((1, P, M))]))
+
+    def dev(v):
+        if aligned:
+            return cuda(v, dtype)
+        flat = np.concatenate([[0.0], v.ravel()]).astype(dtype)
+        return torch.from_numpy(flat).cuda()[1:].view(v.shape)
+
+    A2, C2 = A.copy(), C.copy()
+    A2[0] = np.nan
+    C2[N - 1] = np.inf
+    dA, dB, dC, dd = block.btsv_adjoint(dev(A2), dev(B), dev(C2), dev(u), dev(w))
+    assert rel_err(dd.cpu().numpy(), g) <= tol
+    assert rel_err(dA[1:].cpu().numpy(), exp_dA[1:]) <= tol
+    assert rel_err(dB.cpu().numpy(), exp_dB) <= tol
+    assert rel_err(dC[:-1].cpu().numpy(), exp_dC[:-1]) <= tol

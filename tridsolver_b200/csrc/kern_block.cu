@@ -26,6 +26,11 @@
 // blocks.  With g the solution for the cotangent w and u the forward
 // solution: dA_n = -g_n u_{n-1}^T, dB_n = -g_n u_n^T, dC_n = -g_n u_{n+1}^T,
 // dd_n = g_n, formed in the backward sweep.
+//
+// For M = 2..4 a thread per system holds the whole block algebra in
+// registers instead (blocks read as 16-byte vectors where they allow it);
+// the M-lanes kernel takes those sizes only when M = 2 or 4 arrays are off a
+// 16-byte boundary.
 #include "trid_internal.cuh"
 
 namespace tridb200 {
@@ -606,6 +611,304 @@ __global__ void __launch_bounds__(128) block2_adj_kernel(BlkArgs<T> a) {
   }
 }
 
+// Forward for M = 3..4, one thread per system: the whole M x M algebra in
+// registers (Gauss-Jordan on [X | C | rhs] without pivoting, as the M-lanes
+// kernel), the next block row's loads in flight while the current one is
+// eliminated.
+template <typename T, int M>
+struct BlkMRow {
+  T A[M * M], B[M * M], C[M * M], d[M];
+};
+
+template <typename T, int K>
+__device__ __forceinline__ void blkm_ld(const T *p, T (&r)[K]) {
+  if constexpr (sizeof(T) == 8 && K % 2 == 0) {
+#pragma unroll
+    for (int j = 0; j < K; j += 2) {
+      const double2 u = __ldg(reinterpret_cast<const double2 *>(p + j));
+      r[j] = u.x;
+      r[j + 1] = u.y;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < K; ++j) r[j] = __ldg(p + j);
+  }
+}
+
+template <typename T, int K>
+__device__ __forceinline__ void blkm_st(T *p, const T (&r)[K]) {
+  if constexpr (sizeof(T) == 8 && K % 2 == 0) {
+#pragma unroll
+    for (int j = 0; j < K; j += 2)
+      *reinterpret_cast<double2 *>(p + j) = make_double2(r[j], r[j + 1]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < K; ++j) p[j] = r[j];
+  }
+}
+
+template <typename T, int M>
+__global__ void __launch_bounds__(128) blockm_kernel(BlkArgs<T> a) {
+  constexpr int MM = M * M;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.P) return;
+  const int64_t P = a.P;
+  const int N = a.N;
+  auto bx = [&](int n) { return ((int64_t)n * P + p) * MM; };
+  auto vx = [&](int n) { return ((int64_t)n * P + p) * M; };
+  auto fetch = [&](int n, BlkMRow<T, M> &s) {
+    if (n >= N) return;
+    blkm_ld<T, MM>(a.B + bx(n), s.B);
+    if (n > 0) {
+      blkm_ld<T, MM>(a.A + bx(n), s.A);
+    } else {
+#pragma unroll
+      for (int j = 0; j < MM; ++j) s.A[j] = T(0);
+    }
+    if (n < N - 1) {
+      blkm_ld<T, MM>(a.C + bx(n), s.C);
+    } else {
+#pragma unroll
+      for (int j = 0; j < MM; ++j) s.C[j] = T(0);
+    }
+    blkm_ld<T, M>(a.d + vx(n), s.d);
+  };
+  BlkMRow<T, M> nxt;
+  fetch(0, nxt);
+  T Cp[MM], dp[M];
+#pragma unroll
+  for (int j = 0; j < MM; ++j) Cp[j] = T(0);
+#pragma unroll
+  for (int j = 0; j < M; ++j) dp[j] = T(0);
+  for (int n = 0; n < N; ++n) {
+    BlkMRow<T, M> r = nxt;
+    fetch(n + 1, nxt);
+    // X = B - A C'_{n-1}, h = d - A d'_{n-1}; R = C
+    T X[MM], h[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      T hi = r.d[i];
+#pragma unroll
+      for (int k = 0; k < M; ++k) hi -= r.A[i * M + k] * dp[k];
+      h[i] = hi;
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        T x = r.B[i * M + j];
+#pragma unroll
+        for (int k = 0; k < M; ++k) x -= r.A[i * M + k] * Cp[k * M + j];
+        X[i * M + j] = x;
+      }
+    }
+    // Gauss-Jordan: X [C' | d'] = [C | h]
+#pragma unroll
+    for (int q = 0; q < M; ++q) {
+      const T inv = rcp(X[q * M + q]);
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        X[q * M + j] *= inv;
+        r.C[q * M + j] *= inv;
+      }
+      h[q] *= inv;
+#pragma unroll
+      for (int i = 0; i < M; ++i) {
+        if (i == q) continue;
+        const T f = X[i * M + q];
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+          X[i * M + j] -= f * X[q * M + j];
+          r.C[i * M + j] -= f * r.C[q * M + j];
+        }
+        h[i] -= f * h[q];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < MM; ++j) Cp[j] = r.C[j];
+#pragma unroll
+    for (int j = 0; j < M; ++j) dp[j] = h[j];
+    blkm_st<T, MM>(a.Cs + bx(n), Cp);
+    blkm_st<T, M>(a.ds + vx(n), dp);
+  }
+  // backward: x_{N-1} = d'_{N-1}; x_n = d'_n - C'_n x_{n+1}
+  T u[M];
+#pragma unroll
+  for (int j = 0; j < M; ++j) u[j] = dp[j];
+  blkm_st<T, M>(a.x + vx(N - 1), u);
+  T nc[MM], nd[M];
+  if (N >= 2) {
+    blkm_ld<T, MM>(a.Cs + bx(N - 2), nc);
+    blkm_ld<T, M>(a.ds + vx(N - 2), nd);
+  }
+  for (int n = N - 2; n >= 0; --n) {
+    T c[MM], dd[M];
+#pragma unroll
+    for (int j = 0; j < MM; ++j) c[j] = nc[j];
+#pragma unroll
+    for (int j = 0; j < M; ++j) dd[j] = nd[j];
+    if (n > 0) {
+      blkm_ld<T, MM>(a.Cs + bx(n - 1), nc);
+      blkm_ld<T, M>(a.ds + vx(n - 1), nd);
+    }
+    T v[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      T acc = dd[i];
+#pragma unroll
+      for (int k = 0; k < M; ++k) acc -= c[i * M + k] * u[k];
+      v[i] = acc;
+    }
+#pragma unroll
+    for (int j = 0; j < M; ++j) u[j] = v[j];
+    blkm_st<T, M>(a.x + vx(n), u);
+  }
+}
+
+// Adjoint for M = 3..4, one thread per system: the transposed block system
+// (sub-diagonal C_{n-1}^T, diagonal B_n^T, super-diagonal A_{n+1}^T, rhs w)
+// as in blockm_kernel, then g and the gradients in the backward sweep.
+template <typename T, int M>
+__global__ void __launch_bounds__(128) blockm_adj_kernel(BlkArgs<T> a) {
+  constexpr int MM = M * M;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.P) return;
+  const int64_t P = a.P;
+  const int N = a.N;
+  auto bx = [&](int n) { return ((int64_t)n * P + p) * MM; };
+  auto vx = [&](int n) { return ((int64_t)n * P + p) * M; };
+  // stage fields: A = C_{n-1}, B = B_n, C = A_{n+1} (all as stored)
+  auto fetch = [&](int n, BlkMRow<T, M> &s) {
+    if (n >= N) return;
+    blkm_ld<T, MM>(a.B + bx(n), s.B);
+    if (n > 0) {
+      blkm_ld<T, MM>(a.C + bx(n - 1), s.A);
+    } else {
+#pragma unroll
+      for (int j = 0; j < MM; ++j) s.A[j] = T(0);
+    }
+    if (n < N - 1) {
+      blkm_ld<T, MM>(a.A + bx(n + 1), s.C);
+    } else {
+#pragma unroll
+      for (int j = 0; j < MM; ++j) s.C[j] = T(0);
+    }
+    blkm_ld<T, M>(a.d + vx(n), s.d);
+  };
+  BlkMRow<T, M> nxt;
+  fetch(0, nxt);
+  T Cp[MM], dp[M];
+#pragma unroll
+  for (int j = 0; j < MM; ++j) Cp[j] = T(0);
+#pragma unroll
+  for (int j = 0; j < M; ++j) dp[j] = T(0);
+  for (int n = 0; n < N; ++n) {
+    BlkMRow<T, M> r = nxt;
+    fetch(n + 1, nxt);
+    // X = B^T - L C', h = w - L d' with L[i][k] = C_{n-1}[k][i]; R = A_{n+1}^T
+    T X[MM], h[M], R[MM];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      T hi = r.d[i];
+#pragma unroll
+      for (int k = 0; k < M; ++k) hi -= r.A[k * M + i] * dp[k];
+      h[i] = hi;
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        T x = r.B[j * M + i];
+#pragma unroll
+        for (int k = 0; k < M; ++k) x -= r.A[k * M + i] * Cp[k * M + j];
+        X[i * M + j] = x;
+        R[i * M + j] = r.C[j * M + i];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < M; ++q) {
+      const T inv = rcp(X[q * M + q]);
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        X[q * M + j] *= inv;
+        R[q * M + j] *= inv;
+      }
+      h[q] *= inv;
+#pragma unroll
+      for (int i = 0; i < M; ++i) {
+        if (i == q) continue;
+        const T f = X[i * M + q];
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+          X[i * M + j] -= f * X[q * M + j];
+          R[i * M + j] -= f * R[q * M + j];
+        }
+        h[i] -= f * h[q];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < MM; ++j) Cp[j] = R[j];
+#pragma unroll
+    for (int j = 0; j < M; ++j) dp[j] = h[j];
+    blkm_st<T, MM>(a.Cs + bx(n), Cp);
+    blkm_st<T, M>(a.ds + vx(n), dp);
+  }
+  // backward: g_{N-1} = d'_{N-1}; g_n = d'_n - C'_n g_{n+1}; gradients of row n
+  T g[M], un[M], uc[M];
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    g[j] = dp[j];
+    un[j] = T(0);
+  }
+  blkm_ld<T, M>(a.u + vx(N - 1), uc);
+  for (int n = N - 1; n >= 0; --n) {
+    T up[M];
+    if (n > 0) {
+      blkm_ld<T, M>(a.u + vx(n - 1), up);
+    } else {
+#pragma unroll
+      for (int j = 0; j < M; ++j) up[j] = T(0);
+    }
+    if (n < N - 1) {
+      T c[MM], dd[M];
+      blkm_ld<T, MM>(a.Cs + bx(n), c);
+      blkm_ld<T, M>(a.ds + vx(n), dd);
+      T v[M];
+#pragma unroll
+      for (int i = 0; i < M; ++i) {
+        T acc = dd[i];
+#pragma unroll
+        for (int k = 0; k < M; ++k) acc -= c[i * M + k] * g[k];
+        v[i] = acc;
+      }
+#pragma unroll
+      for (int j = 0; j < M; ++j) g[j] = v[j];
+    }
+    if (a.dd) blkm_st<T, M>(a.dd + vx(n), g);
+    T o[MM];
+    if (a.dA) {
+#pragma unroll
+      for (int i = 0; i < M; ++i)
+#pragma unroll
+        for (int j = 0; j < M; ++j) o[i * M + j] = -g[i] * up[j];
+      blkm_st<T, MM>(a.dA + bx(n), o);
+    }
+    if (a.dB) {
+#pragma unroll
+      for (int i = 0; i < M; ++i)
+#pragma unroll
+        for (int j = 0; j < M; ++j) o[i * M + j] = -g[i] * uc[j];
+      blkm_st<T, MM>(a.dB + bx(n), o);
+    }
+    if (a.dC) {
+#pragma unroll
+      for (int i = 0; i < M; ++i)
+#pragma unroll
+        for (int j = 0; j < M; ++j) o[i * M + j] = -g[i] * un[j];
+      blkm_st<T, MM>(a.dC + bx(n), o);
+    }
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      un[j] = uc[j];
+      uc[j] = up[j];
+    }
+  }
+}
+
 template <typename T, bool ADJ>
 cudaError_t launch_block(const BlkArgs<T> &a, int M, cudaStream_t st) {
   auto go = [&](auto kern, int m) {
@@ -629,6 +932,21 @@ cudaError_t launch_block(const BlkArgs<T> &a, int M, cudaStream_t st) {
         block2_adj_kernel<T, 4><<<dim3((unsigned)blocks), dim3(128), 0, st>>>(a);
       else
         block2_kernel<T, 4><<<dim3((unsigned)blocks), dim3(128), 0, st>>>(a);
+      return cudaGetLastError();
+    }
+    // M = 3, 4: one thread per system as well (16-byte accesses need M = 4
+    // and aligned arrays; M = 3 reads element by element)
+    if (M == 3 || (M == 4 && (bits & 15) == 0)) {
+      const int64_t blocks = (a.P + 127) / 128;
+      if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
+      const dim3 g((unsigned)blocks), b(128);
+      if constexpr (ADJ) {
+        if (M == 3) blockm_adj_kernel<T, 3><<<g, b, 0, st>>>(a);
+        else blockm_adj_kernel<T, 4><<<g, b, 0, st>>>(a);
+      } else {
+        if (M == 3) blockm_kernel<T, 3><<<g, b, 0, st>>>(a);
+        else blockm_kernel<T, 4><<<g, b, 0, st>>>(a);
+      }
       return cudaGetLastError();
     }
   }
