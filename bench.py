@@ -20,7 +20,8 @@ differentiation (16,384 x 1024 FP64: forward, forward + adjoint in one call
 and autograd forward + backward, times and their ratio to the forward solve,
 gradient error against central finite differences; rank 0 at N=1).
 
---suite: one JSON line per other workload (FP32 cube, long systems,
+--suite: one JSON line per other workload (FP32 cube, complex and
+FP32-storage / FP64-arithmetic cubes, long systems,
 variable-length batch, block systems, ADI steps and the ADI gradient);
 --scale f runs the batched workloads with a fraction f of their systems.
 
@@ -512,6 +513,30 @@ def run_suite(args):
         emit({"workload": f"FP32 256^3 solvedim {sd}", "ms": round(ms, 5),
               "gbs": round(20 * UNKNOWNS / (ms * 1e-3) / 1e9, 1)})
     del a, b, c, d
+
+    # complex128 / complex64 256^3 (5 elements of 16 / 8 B per unknown) and
+    # FP32 storage with FP64 arithmetic (20 B per unknown), each axis
+    def ccoeffs(shape, dtype):
+        rdt = torch.float64 if dtype == torch.complex128 else torch.float32
+        r = lambda: torch.rand(shape, dtype=rdt, device=dev, generator=gen) * 2 - 1
+        a, c = torch.complex(r(), r()), torch.complex(r(), r())
+        mod = a.abs() + c.abs() + 1.5 + 0.5 * r()
+        b = torch.polar(mod, torch.pi * r())
+        d = torch.complex(torch.randn(shape, dtype=rdt, device=dev, generator=gen),
+                          torch.randn(shape, dtype=rdt, device=dev, generator=gen))
+        return a, b, c, d
+
+    for name, dtype, fn, bpu in (("complex128", torch.complex128, tb.tridZmtsvStridedBatch, 80),
+                                 ("complex64", torch.complex64, tb.tridCmtsvStridedBatch, 40),
+                                 ("FP32 storage / FP64 arithmetic", torch.float32,
+                                  tb.tridSmtsvStridedBatchMixed, 20)):
+        a, b, c, d = (ccoeffs((UNKNOWNS,), dtype) if dtype.is_complex
+                      else coeffs((UNKNOWNS,), dtype))
+        for sd in range(3):
+            ms = timed(lambda: fn(a, b, c, d, None, 3, sd, DIMS, DIMS))
+            emit({"workload": f"{name} 256^3 solvedim {sd}", "ms": round(ms, 5),
+                  "gbs": round(bpu * UNKNOWNS / (ms * 1e-3) / 1e9, 1)})
+        del a, b, c, d
 
     sc = args.scale  # fraction of each workload's systems (1 = the configured sizes)
     assert 0 < sc <= 1, "--scale in (0, 1]"

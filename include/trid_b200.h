@@ -74,6 +74,52 @@ TRID_EXTERN_C tridStatus_t tridDmtsvStridedBatchInc(const double *a, const doubl
                                                     const double *c, double *d, double *u,
                                                     int ndim, int solvedim, int *dims, int *pads);
 
+/* ---- complex element types: the forms the reference declares but leaves
+ *      commented out (trid_cuda.h:39-52; trid_cuda.cu:546-600,
+ *      tridCmtsvStridedBatch / tridZmtsvStridedBatch and their Inc forms),
+ *      with the live 9-argument signature above.  Elements are interleaved
+ *      (re, im) pairs -- the layout of cuComplex / cuDoubleComplex,
+ *      std::complex and C99 _Complex -- aligned to their size (8 / 16 bytes).
+ *      Same algorithm in complex arithmetic, no pivoting: the rows must be
+ *      safe for Gaussian elimination without pivoting (e.g. diagonally
+ *      dominant in modulus). ---- */
+typedef struct {
+  float re, im;
+} tridComplexF;
+typedef struct {
+  double re, im;
+} tridComplexD;
+TRID_EXTERN_C tridStatus_t tridCmtsvStridedBatch(const tridComplexF *a, const tridComplexF *b,
+                                                 const tridComplexF *c, tridComplexF *d,
+                                                 tridComplexF *u, int ndim, int solvedim,
+                                                 int *dims, int *pads);
+TRID_EXTERN_C tridStatus_t tridCmtsvStridedBatchInc(const tridComplexF *a, const tridComplexF *b,
+                                                    const tridComplexF *c, tridComplexF *d,
+                                                    tridComplexF *u, int ndim, int solvedim,
+                                                    int *dims, int *pads);
+TRID_EXTERN_C tridStatus_t tridZmtsvStridedBatch(const tridComplexD *a, const tridComplexD *b,
+                                                 const tridComplexD *c, tridComplexD *d,
+                                                 tridComplexD *u, int ndim, int solvedim,
+                                                 int *dims, int *pads);
+TRID_EXTERN_C tridStatus_t tridZmtsvStridedBatchInc(const tridComplexD *a, const tridComplexD *b,
+                                                    const tridComplexD *c, tridComplexD *d,
+                                                    tridComplexD *u, int ndim, int solvedim,
+                                                    int *dims, int *pads);
+
+/* ---- FP32 storage, FP64 arithmetic (no reference counterpart): the
+ *      arguments of tridSmtsvStridedBatch[Inc]; every element is widened to
+ *      double on load, the solve runs in double and each result is rounded to
+ *      float once (Inc: u = float(double(u) + x)), so the FP32 result is the
+ *      correctly rounded FP64 solution up to the FP64 solve's own error. ---- */
+TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchMixed(const float *a, const float *b,
+                                                      const float *c, float *d, float *u,
+                                                      int ndim, int solvedim, int *dims,
+                                                      int *pads);
+TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchMixedInc(const float *a, const float *b,
+                                                         const float *c, float *d, float *u,
+                                                         int ndim, int solvedim, int *dims,
+                                                         int *pads);
+
 /* ---- per-array pads: replace trid_cuda.h:61-67 / :78-84
  *      (tridDmtsvStridedBatchPadded[Inc]); float forms are additions.
  *      opts is an optional algorithm hint (may be NULL); sync=1 waits for the

@@ -72,7 +72,8 @@ def _ipad(v):
 
 
 def _suffix(dtype):
-    return "f64" if np.dtype(dtype) == np.float64 else "f32"
+    return {np.dtype(np.float64): "f64", np.dtype(np.float32): "f32",
+            np.dtype(np.complex128): "c128", np.dtype(np.complex64): "c64"}[np.dtype(dtype)]
 
 
 # --------------------------------------------------------------------------- #
@@ -227,10 +228,13 @@ def run_adi_orig(nx, ny, nz, iters, workdir):
 # Dense FP64 LU oracle (numpy)                                                #
 # --------------------------------------------------------------------------- #
 def dense_solve_systems(a, b, c, d):
-    """Solve each row-system (shape [S, n]) by dense FP64 LU (numpy.linalg)."""
-    a, b, c, d = (np.asarray(x, dtype=np.float64) for x in (a, b, c, d))
+    """Solve each row-system (shape [S, n]) by dense FP64 LU (numpy.linalg);
+    complex inputs in complex128."""
+    cplx = any(np.iscomplexobj(x) for x in (a, b, c, d))
+    t = np.complex128 if cplx else np.float64
+    a, b, c, d = (np.asarray(x, dtype=t) for x in (a, b, c, d))
     S, n = b.shape
-    M = np.zeros((S, n, n))
+    M = np.zeros((S, n, n), dtype=t)
     idx = np.arange(n)
     M[:, idx, idx] = b
     if n > 1:

@@ -132,6 +132,18 @@ void oracle_trid_scalar_f32(const float *a, const float *b, const float *c,
 DEFINE_MTSV(double, f64)
 DEFINE_MTSV(float, f32)
 
+/* Complex element types: the same Thomas and N-D batch in C99 complex
+ * arithmetic (the reference declares tridC/ZmtsvStridedBatch over
+ * tridMultiDimBatchSolve<complexf/complexd> and leaves them commented out,
+ * scalar/src/cuda/trid_cuda.cu:546-600; its CPU Thomas, trid_cpu.cpp:360-401,
+ * is written for any element type).  Pinned by tests/test_oracle.py against
+ * the real functions above (zero imaginary parts) and against dense complex
+ * LU. */
+DEFINE_THOMAS(double _Complex, c128, 1.0)
+DEFINE_THOMAS(float _Complex, c64, 1.0F)
+DEFINE_MTSV(double _Complex, c128)
+DEFINE_MTSV(float _Complex, c64)
+
 /* ------------------------------------------------------------------------ */
 /* Variable-length packed batch: system s occupies rows                      */
 /* [offsets[s], offsets[s+1]) of every array, unit stride.  Each system is    */

@@ -12,8 +12,9 @@ RTOL = {np.float64: 1e-12, np.float32: 1e-5}
 
 
 def rel_err(x, ref):
-    x = np.asarray(x, dtype=np.float64)
-    ref = np.asarray(ref, dtype=np.float64)
+    x, ref = np.asarray(x), np.asarray(ref)
+    t = np.complex128 if np.iscomplexobj(x) or np.iscomplexobj(ref) else np.float64
+    x, ref = x.astype(t), ref.astype(t)
     return float(np.abs(x - ref).max() / max(np.abs(ref).max(), 1e-300))
 
 
@@ -23,6 +24,17 @@ def rand_coeffs(rng, size, dtype=np.float64):
     c = rng.uniform(-1, 1, size)
     b = np.abs(a) + np.abs(c) + rng.uniform(1, 2, size)
     d = rng.standard_normal(size)
+    return [x.astype(dtype) for x in (a, b, c, d)]
+
+
+def rand_complex_coeffs(rng, size, dtype=np.complex128):
+    """Complex rows diagonally dominant in modulus: a, c with components
+    U(-1,1), b = (|a|+|c|+U(1,2)) e^{i phi} with phi ~ U(0, 2 pi), d with
+    N(0,1) components."""
+    a = rng.uniform(-1, 1, size) + 1j * rng.uniform(-1, 1, size)
+    c = rng.uniform(-1, 1, size) + 1j * rng.uniform(-1, 1, size)
+    b = (np.abs(a) + np.abs(c) + rng.uniform(1, 2, size)) * np.exp(1j * rng.uniform(0, 2 * np.pi, size))
+    d = rng.standard_normal(size) + 1j * rng.standard_normal(size)
     return [x.astype(dtype) for x in (a, b, c, d)]
 
 

@@ -110,6 +110,22 @@ def test_null_and_misaligned_pointers_rejected():
     assert tb.tridSmtsvStridedBatch(p + 2, p, p, p, None, 1, 0, [8], [8]) == INVALID
 
 
+def test_complex_and_mixed_invalid_arguments_rejected():
+    p, _keep = _fake()
+    q = (p + 15) & ~15  # 16-byte aligned, inside the buffer
+    for fn in (tb.tridZmtsvStridedBatch, tb.tridCmtsvStridedBatch, tb.tridSmtsvStridedBatchMixed):
+        assert fn(q, q, q, q, None, 0, 0, [4], [4]) == INVALID
+        assert fn(q, q, q, q, None, 2, 0, [4, 4], [3, 4]) == INVALID
+        assert fn(q, q, q, None, None, 1, 0, [8], [8]) == INVALID
+    for fn in (tb.tridZmtsvStridedBatchInc, tb.tridCmtsvStridedBatchInc,
+               tb.tridSmtsvStridedBatchMixedInc):
+        assert fn(q, q, q, q, None, 1, 0, [8], [8]) == INVALID  # Inc needs u
+    # elements aligned to their size: 16 / 8 / 4 bytes
+    assert tb.tridZmtsvStridedBatch(q + 8, q, q, q, None, 1, 0, [8], [8]) == INVALID
+    assert tb.tridCmtsvStridedBatch(q, q, q, q + 4, None, 1, 0, [8], [8]) == INVALID
+    assert tb.tridSmtsvStridedBatchMixed(q, q + 2, q, q, None, 1, 0, [8], [8]) == INVALID
+
+
 def test_bad_opts_rejected_by_padded_and_compat():
     p, _keep = _fake()
     st = tb.tridDmtsvStridedBatchPadded(p, [8], p, [8], p, [8], p, [8], None, [8], 1, 0, [8],

@@ -116,6 +116,39 @@ def test_oracle_against_dense_lu():
         assert np.abs(sv(x) - xd).max() / np.abs(xd).max() < 1e-13
 
 
+@pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-13), (np.complex64, 2e-5)])
+def test_complex_oracle_against_dense_lu(dtype, tol):
+    """The complex restatement (same Thomas in complex arithmetic) against
+    dense complex LU on every axis, with pads."""
+    from helpers import rand_complex_coeffs
+    rng = np.random.default_rng(17)
+    dims, pads = [13, 6, 4], [15, 6, 5]
+    for solvedim in range(3):
+        a, b, c, d = rand_complex_coeffs(rng, int(np.prod(pads)), dtype)
+        x = oracle.mtsv(a, b, c, d, dims=dims, pads=pads, solvedim=solvedim)
+        sv = lambda v: oracle.systems_view(v, dims, solvedim, pads)
+        xd = oracle.dense_solve_systems(sv(a), sv(b), sv(c), sv(d))
+        assert np.abs(sv(x) - xd).max() / np.abs(xd).max() < tol
+        u = (rng.standard_normal(a.size) + 1j * rng.standard_normal(a.size)).astype(dtype)
+        ui = oracle.mtsv(a, b, c, d, u=u, dims=dims, pads=pads, solvedim=solvedim, inc=True)
+        assert np.abs(sv(ui) - sv(u) - xd).max() / np.abs(xd).max() < 2 * tol
+
+
+@pytest.mark.parametrize("rdt,cdt", [(np.float64, np.complex128), (np.float32, np.complex64)])
+def test_complex_oracle_reduces_to_real_oracle(rdt, cdt):
+    """With zero imaginary parts the complex restatement gives the real one's
+    answer (which the golden fixtures and the reference CPU build pin)."""
+    rng = np.random.default_rng(5)
+    dims = [40, 7, 3]
+    a, b, c, d, _ = rand_system(rng, int(np.prod(dims)), rdt)
+    tol = 1e-15 if rdt == np.float64 else 1e-6
+    for solvedim in range(3):
+        xr = oracle.mtsv(a, b, c, d, dims=dims, solvedim=solvedim)
+        xc = oracle.mtsv(*(v.astype(cdt) for v in (a, b, c, d)), dims=dims, solvedim=solvedim)
+        assert np.abs(xc.imag).max() == 0
+        assert np.abs(xc.real - xr).max() / np.abs(xr).max() <= tol
+
+
 def test_oracle_ignores_a0_and_cn():
     """a[0] and c[n-1] of every system are never read (trid_cpu.cpp:360-401)."""
     rng = np.random.default_rng(3)

@@ -22,6 +22,8 @@ from ._lib import STATUS_NAMES, TridError, compat_lib, lib  # noqa: F401
 from .scalar import (  # noqa: F401
     initTridMultiDimBatchSolve,
     solve,
+    tridCmtsvStridedBatch,
+    tridCmtsvStridedBatchInc,
     tridDmtsvStridedBatch,
     tridDmtsvStridedBatchAdjoint,
     tridSmtsvStridedBatchAdjoint,
@@ -35,6 +37,10 @@ from .scalar import (  # noqa: F401
     tridSmtsvStridedBatchInc,
     tridSmtsvStridedBatchPadded,
     tridSmtsvStridedBatchPaddedInc,
+    tridSmtsvStridedBatchMixed,
+    tridSmtsvStridedBatchMixedInc,
+    tridZmtsvStridedBatch,
+    tridZmtsvStridedBatchInc,
     set_method,
 )
 from .autograd import TridSolve, trid_solve  # noqa: F401

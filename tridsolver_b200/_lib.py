@@ -69,6 +69,12 @@ _MAIN_ONLY = {
     "tridDmtsvStridedBatch": (c_int, _SCALAR9),
     "tridSmtsvStridedBatchInc": (c_int, _SCALAR9),
     "tridDmtsvStridedBatchInc": (c_int, _SCALAR9),
+    "tridCmtsvStridedBatch": (c_int, _SCALAR9),
+    "tridCmtsvStridedBatchInc": (c_int, _SCALAR9),
+    "tridZmtsvStridedBatch": (c_int, _SCALAR9),
+    "tridZmtsvStridedBatchInc": (c_int, _SCALAR9),
+    "tridSmtsvStridedBatchMixed": (c_int, _SCALAR9),
+    "tridSmtsvStridedBatchMixedInc": (c_int, _SCALAR9),
 }
 _COMPAT_ONLY = {
     "tridSmtsvStridedBatch": (c_int, _SCALAR11),

@@ -1,0 +1,393 @@
+// Strided-batch solves over element types beyond FP32/FP64 (sm_100a).
+//
+//  * complex<float>, complex<double>: interleaved (re, im) pairs, the layout
+//    of cuComplex / cuDoubleComplex, std::complex and C99 _Complex.  The
+//    reference declares these forms and leaves them commented out
+//    (scalar/include/trid_cuda.h:39-52, scalar/src/cuda/trid_cuda.cu:468-600,
+//    tridMultiDimBatchSolve<complexf/complexd>); the algorithm is the real
+//    one in complex arithmetic, without pivoting.
+//  * FP32 storage with FP64 arithmetic ("mixed"): every load widens to
+//    double, the whole solve runs in double and each result is rounded to
+//    float once (Inc: u = float(double(u) + x)).
+//
+// S is the storage type, T the arithmetic type.  The solvers are the
+// partitioned Thomas building blocks of partition.cuh instantiated for T:
+//
+//  ext_x_kernel       axis 0 (unit stride), n <= 32*M: one warp per system,
+//                     lane t owns rows [t*M, t*M+M).
+//  ext_strided_kernel axes >= 1, n <= 32*M: a CTA owns SB adjacent systems
+//                     (SB*sizeof(S) = 128 B rows for the complex types up to
+//                     256 rows, 64 B otherwise) x 32 chunks; the interface
+//                     rows go through shared memory to SB warps, one
+//                     interface system each.
+//  ext_thomas_kernel  any n: one thread per system, Thomas with c'/d' in
+//                     library scratch laid out [row][system] (in T).
+#include <cstring>
+
+#include "partition.cuh"
+#include "trid_b200.h"
+
+namespace tridb200 {
+
+// ------------------------------------------------------------ complex T --
+template <typename R>
+struct Cx {
+  R x, y;
+  Cx() = default;
+  __host__ __device__ constexpr Cx(R re) : x(re), y(R(0)) {}
+  __host__ __device__ constexpr Cx(R re, R im) : x(re), y(im) {}
+};
+
+template <typename R>
+__device__ __forceinline__ Cx<R> operator+(const Cx<R> &p, const Cx<R> &q) {
+  return {p.x + q.x, p.y + q.y};
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> operator-(const Cx<R> &p, const Cx<R> &q) {
+  return {p.x - q.x, p.y - q.y};
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> operator-(const Cx<R> &p) {
+  return {-p.x, -p.y};
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> operator*(const Cx<R> &p, const Cx<R> &q) {
+  return {p.x * q.x - p.y * q.y, p.x * q.y + p.y * q.x};
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> &operator*=(Cx<R> &p, const Cx<R> &q) {
+  p = p * q;
+  return p;
+}
+
+// 1/z by Smith's scaling (R. L. Smith, "Algorithm 116: Complex division",
+// CACM 5(8), 1962): divide through by the larger component so that no
+// intermediate squares the magnitude.
+template <typename R>
+__device__ __forceinline__ Cx<R> rcp(const Cx<R> &z) {
+  if (fabs(z.x) >= fabs(z.y)) {
+    const R r = z.y * rcp(z.x);
+    const R t = rcp(z.x + z.y * r);
+    return {t, -r * t};
+  }
+  const R r = z.x * rcp(z.y);
+  const R t = rcp(z.x * r + z.y);
+  return {r * t, -t};
+}
+
+// warp shuffles of a complex value (found by argument-dependent lookup from
+// the partition.cuh templates)
+template <typename R>
+__device__ __forceinline__ Cx<R> __shfl_down_sync(unsigned m, const Cx<R> &v, unsigned s,
+                                                  int w = 32) {
+  return {::__shfl_down_sync(m, v.x, s, w), ::__shfl_down_sync(m, v.y, s, w)};
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> __shfl_up_sync(unsigned m, const Cx<R> &v, unsigned s,
+                                                int w = 32) {
+  return {::__shfl_up_sync(m, v.x, s, w), ::__shfl_up_sync(m, v.y, s, w)};
+}
+
+// ------------------------------------------------- storage <-> arithmetic --
+template <typename S, typename T>
+struct Elem;
+template <>
+struct Elem<float, double> {
+  static __device__ __forceinline__ double ld(const float *p) { return (double)__ldg(p); }
+  static __device__ __forceinline__ double ldw(const float *p) { return (double)*p; }
+  static __device__ __forceinline__ void st(float *p, double v) { *p = (float)v; }
+};
+template <>
+struct Elem<float2, Cx<float>> {
+  static __device__ __forceinline__ Cx<float> ld(const float2 *p) {
+    const float2 v = __ldg(p);
+    return {v.x, v.y};
+  }
+  static __device__ __forceinline__ Cx<float> ldw(const float2 *p) {
+    const float2 v = *p;
+    return {v.x, v.y};
+  }
+  static __device__ __forceinline__ void st(float2 *p, Cx<float> v) { *p = make_float2(v.x, v.y); }
+};
+template <>
+struct Elem<double2, Cx<double>> {
+  static __device__ __forceinline__ Cx<double> ld(const double2 *p) {
+    const double2 v = __ldg(p);
+    return {v.x, v.y};
+  }
+  static __device__ __forceinline__ Cx<double> ldw(const double2 *p) {
+    const double2 v = *p;
+    return {v.x, v.y};
+  }
+  static __device__ __forceinline__ void st(double2 *p, Cx<double> v) {
+    *p = make_double2(v.x, v.y);
+  }
+};
+
+// x -> d (INC = 0) or u += x (INC = 1)
+template <typename S, typename T, int INC>
+__device__ __forceinline__ void ext_out(S *d, S *u, T x) {
+  using E = Elem<S, T>;
+  if (INC)
+    E::st(u, E::ldw(u) + x);
+  else
+    E::st(d, x);
+}
+
+// ------------------------------------------------------------- kernels --
+template <typename S, typename T, int M, int INC>
+__global__ void __launch_bounds__(128) ext_x_kernel(Geom g, const S *__restrict__ a,
+                                                    const S *__restrict__ b,
+                                                    const S *__restrict__ c, S *__restrict__ d,
+                                                    S *__restrict__ u) {
+  using E = Elem<S, T>;
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int64_t sys = (int64_t)blockIdx.x * (blockDim.x / kWarp) + (threadIdx.x / kWarp);
+  if (sys >= g.nsys) return;  // uniform per warp
+  int64_t off[5];
+  system_offsets(g, sys, off);
+  const int n = g.n;
+  const int r0 = lane * M;
+  T al[M], be[M], ga[M], de[M];
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int r = r0 + j;
+    if (r < n) {
+      al[j] = (r == 0) ? T(0) : E::ld(a + off[kA] + r);
+      be[j] = E::ld(b + off[kB] + r);
+      ga[j] = (r == n - 1) ? T(0) : E::ld(c + off[kC] + r);
+      de[j] = E::ldw(d + off[kD] + r);
+    } else {
+      al[j] = T(0);
+      be[j] = T(1);
+      ga[j] = T(0);
+      de[j] = T(0);
+    }
+  }
+  Row<T> F, L;
+  chunk_reduce<T, M>(al, be, ga, de, F, L);
+  T xF, xL;
+  warp_interface_solve(F, L, xF, xL, lane);
+  chunk_backsub<T, M>(al, ga, de, xF, xL);
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int r = r0 + j;
+    if (r < n) ext_out<S, T, INC>(d + off[kD] + r, INC ? u + off[kU] + r : nullptr, de[j]);
+  }
+}
+
+template <typename S, typename T, int M, int SB, int INC>
+__global__ void __launch_bounds__(SB * kWarp) ext_strided_kernel(Geom g, const S *__restrict__ a,
+                                                                 const S *__restrict__ b,
+                                                                 const S *__restrict__ c,
+                                                                 S *__restrict__ d,
+                                                                 S *__restrict__ u) {
+  using E = Elem<S, T>;
+  // interface rows, [component][chunk][system] (+1 pad against bank conflicts)
+  __shared__ T red[8][kWarp][SB + 1];
+  __shared__ T sol[2][kWarp][SB + 1];
+  const int tid = threadIdx.x;
+  const int sl = tid % SB;  // system within the tile (fastest: coalesced rows)
+  const int t = tid / SB;   // chunk
+  const int64_t sys = (int64_t)blockIdx.x * SB + sl;
+  const bool valid = sys < g.nsys;
+  int64_t off[5] = {0, 0, 0, 0, 0};
+  if (valid) system_offsets(g, sys, off);
+  const int n = g.n;
+  const int r0 = t * M;
+  const int64_t sa = g.stride[kA], sb = g.stride[kB], sc = g.stride[kC], sd = g.stride[kD];
+  T al[M], be[M], ga[M], de[M];
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int r = r0 + j;
+    if (valid && r < n) {
+      al[j] = (r == 0) ? T(0) : E::ld(a + off[kA] + r * sa);
+      be[j] = E::ld(b + off[kB] + r * sb);
+      ga[j] = (r == n - 1) ? T(0) : E::ld(c + off[kC] + r * sc);
+      de[j] = E::ldw(d + off[kD] + r * sd);
+    } else {
+      al[j] = T(0);
+      be[j] = T(1);
+      ga[j] = T(0);
+      de[j] = T(0);
+    }
+  }
+  Row<T> F, L;
+  chunk_reduce<T, M>(al, be, ga, de, F, L);
+  red[0][t][sl] = F.a;
+  red[1][t][sl] = F.b;
+  red[2][t][sl] = F.c;
+  red[3][t][sl] = F.d;
+  red[4][t][sl] = L.a;
+  red[5][t][sl] = L.b;
+  red[6][t][sl] = L.c;
+  red[7][t][sl] = L.d;
+  __syncthreads();
+  {
+    const int w = tid / kWarp;  // this warp solves the interface system of tile system w
+    const int lane = tid & (kWarp - 1);
+    const Row<T> F2{red[0][lane][w], red[1][lane][w], red[2][lane][w], red[3][lane][w]};
+    const Row<T> L2{red[4][lane][w], red[5][lane][w], red[6][lane][w], red[7][lane][w]};
+    T xF, xL;
+    warp_interface_solve(F2, L2, xF, xL, lane);
+    sol[0][lane][w] = xF;
+    sol[1][lane][w] = xL;
+  }
+  __syncthreads();
+  chunk_backsub<T, M>(al, ga, de, sol[0][t][sl], sol[1][t][sl]);
+  if (!valid) return;
+  const int64_t su = g.stride[kU];
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int r = r0 + j;
+    if (r < n)
+      ext_out<S, T, INC>(d + off[kD] + r * sd, INC ? u + off[kU] + r * su : nullptr, de[j]);
+  }
+}
+
+// Thomas in the reference's operation order (scalar/src/cpu/trid_cpu.cpp:
+// 360-401); a[0] and c[n-1] are never read
+template <typename S, typename T, int INC>
+__global__ void __launch_bounds__(128) ext_thomas_kernel(Geom g, const S *__restrict__ a,
+                                                         const S *__restrict__ b,
+                                                         const S *__restrict__ c,
+                                                         S *__restrict__ d, S *__restrict__ u,
+                                                         T *__restrict__ work, int64_t s0,
+                                                         int64_t ns) {
+  using E = Elem<S, T>;
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ns) return;
+  int64_t off[5];
+  system_offsets(g, s0 + k, off);
+  const int64_t sa = g.stride[kA], sb = g.stride[kB], sc = g.stride[kC], sd = g.stride[kD],
+                su = g.stride[kU];
+  const int n = g.n;
+  T *c2 = work + k;
+  T *d2 = work + (int64_t)n * ns + k;
+  const S *ap = a + off[kA];
+  const S *bp = b + off[kB];
+  const S *cp = c + off[kC];
+  S *dp = d + off[kD];
+  S *up = INC ? u + off[kU] : nullptr;
+
+  T bb = rcp(E::ld(bp));
+  T cc = (n > 1) ? bb * E::ld(cp) : T(0);
+  T dd = bb * E::ldw(dp);
+  c2[0] = cc;
+  d2[0] = dd;
+  for (int i = 1; i < n; ++i) {
+    const T aa = E::ld(ap + i * sa);
+    bb = E::ld(bp + i * sb) - aa * cc;
+    dd = E::ldw(dp + i * sd) - aa * dd;
+    bb = rcp(bb);
+    cc = (i < n - 1) ? bb * E::ld(cp + i * sc) : T(0);
+    dd = bb * dd;
+    c2[(int64_t)i * ns] = cc;
+    d2[(int64_t)i * ns] = dd;
+  }
+  ext_out<S, T, INC>(dp + (int64_t)(n - 1) * sd, INC ? up + (int64_t)(n - 1) * su : nullptr, dd);
+  for (int i = n - 2; i >= 0; --i) {
+    dd = d2[(int64_t)i * ns] - c2[(int64_t)i * ns] * dd;
+    ext_out<S, T, INC>(dp + (int64_t)i * sd, INC ? up + (int64_t)i * su : nullptr, dd);
+  }
+}
+
+// ------------------------------------------------------------ launchers --
+// Largest chunk (rows per lane) of the partitioned kernels: 16 for 8-byte
+// arithmetic, 8 for complex<double> (16 rows of 16 bytes per array exceed the
+// register file at one CTA per SM).
+template <typename T>
+constexpr int ext_max_chunk() {
+  return sizeof(T) >= 16 ? 8 : 16;
+}
+
+template <typename S, typename T, int INC>
+cudaError_t launch_ext(const Geom &g, int solvedim, const S *a, const S *b, const S *c, S *d,
+                       S *u, cudaStream_t st) {
+  int M = 2;
+  while (32 * M < g.n && M < ext_max_chunk<T>()) M *= 2;
+  if (32 * M >= g.n) {
+    if (solvedim == 0) {
+      const int64_t blocks = (g.nsys + 3) / 4;
+      if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
+      const dim3 grid((unsigned)blocks), block(128);
+      switch (M) {
+        case 2: ext_x_kernel<S, T, 2, INC><<<grid, block, 0, st>>>(g, a, b, c, d, u); break;
+        case 4: ext_x_kernel<S, T, 4, INC><<<grid, block, 0, st>>>(g, a, b, c, d, u); break;
+        case 8: ext_x_kernel<S, T, 8, INC><<<grid, block, 0, st>>>(g, a, b, c, d, u); break;
+        default:
+          if constexpr (ext_max_chunk<T>() >= 16)
+            ext_x_kernel<S, T, 16, INC><<<grid, block, 0, st>>>(g, a, b, c, d, u);
+          break;
+      }
+      return cudaGetLastError();
+    }
+    // SB systems per CTA: 8 for 16-byte T and for 16-row chunks (whose 64
+    // register-resident values per thread need 256-thread CTAs), else 16
+    constexpr int SB = sizeof(T) >= 16 ? 8 : 16;
+    auto go = [&](auto kern, int sb) {
+      const int64_t blocks = (g.nsys + sb - 1) / sb;
+      if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
+      kern<<<dim3((unsigned)blocks), dim3(sb * kWarp), 0, st>>>(g, a, b, c, d, u);
+      return cudaGetLastError();
+    };
+    switch (M) {
+      case 2: return go(ext_strided_kernel<S, T, 2, SB, INC>, SB);
+      case 4: return go(ext_strided_kernel<S, T, 4, SB, INC>, SB);
+      case 8: return go(ext_strided_kernel<S, T, 8, SB, INC>, SB);
+      default:
+        if constexpr (ext_max_chunk<T>() >= 16) return go(ext_strided_kernel<S, T, 16, 8, INC>, 8);
+        return cudaErrorInvalidValue;
+    }
+  }
+  // Thomas with c'/d' in scratch, in batches of systems bounded to ~1 GiB
+  const size_t per_sys = (size_t)2 * g.n * sizeof(T);
+  int64_t ws = (int64_t)(((size_t)1 << 30) / per_sys);
+  ws = ws < 1 ? 1 : (ws > g.nsys ? g.nsys : ws);
+  T *work = (T *)scratch(per_sys * (size_t)ws, 0);
+  if (!work) return cudaErrorMemoryAllocation;
+  for (int64_t s0 = 0; s0 < g.nsys; s0 += ws) {
+    const int64_t ns = (g.nsys - s0 < ws) ? (g.nsys - s0) : ws;
+    ext_thomas_kernel<S, T, INC><<<dim3((unsigned)((ns + 127) / 128)), dim3(128), 0, st>>>(
+        g, a, b, c, d, u, work, s0, ns);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+tridStatus_t make_geom(int ndim, int solvedim, const int *dims, const int *const pads[5],
+                       bool inc, Geom &g);
+
+template <typename S, typename T, int INC>
+static tridStatus_t solve_ext(const void *a, const void *b, const void *c, void *d, void *u,
+                              int ndim, int solvedim, const int *dims, const int *pads) {
+  const int *p[5] = {pads, pads, pads, pads, pads};
+  Geom g;
+  const tridStatus_t st = make_geom(ndim, solvedim, dims, p, INC != 0, g);
+  if (st != TRID_STATUS_SUCCESS) return st;
+  auto ok = [](const void *q) { return q != nullptr && ((uintptr_t)q % sizeof(S)) == 0; };
+  if (!ok(a) || !ok(b) || !ok(c) || !ok(d) || (INC && !ok(u))) return TRID_STATUS_INVALID_VALUE;
+  if (g.n == 0 || g.nsys == 0) return TRID_STATUS_SUCCESS;
+  const cudaError_t e = launch_ext<S, T, INC>(g, solvedim, (const S *)a, (const S *)b,
+                                             (const S *)c, (S *)d, INC ? (S *)u : nullptr,
+                                             current_stream());
+  if (e == cudaErrorMemoryAllocation) return TRID_STATUS_ALLOC_FAILED;
+  return e == cudaSuccess ? TRID_STATUS_SUCCESS : TRID_STATUS_EXECUTION_FAILED;
+}
+
+}  // namespace tridb200
+
+using namespace tridb200;
+
+#define TRID_EXT_ABI(NAME, ST, S, T, INC)                                                    \
+  extern "C" tridStatus_t NAME(const ST *a, const ST *b, const ST *c, ST *d, ST *u, int ndim, \
+                               int solvedim, int *dims, int *pads) {                          \
+    return solve_ext<S, T, INC>(a, b, c, d, u, ndim, solvedim, dims, pads);                   \
+  }
+TRID_EXT_ABI(tridCmtsvStridedBatch, tridComplexF, float2, Cx<float>, 0)
+TRID_EXT_ABI(tridCmtsvStridedBatchInc, tridComplexF, float2, Cx<float>, 1)
+TRID_EXT_ABI(tridZmtsvStridedBatch, tridComplexD, double2, Cx<double>, 0)
+TRID_EXT_ABI(tridZmtsvStridedBatchInc, tridComplexD, double2, Cx<double>, 1)
+TRID_EXT_ABI(tridSmtsvStridedBatchMixed, float, float, double, 0)
+TRID_EXT_ABI(tridSmtsvStridedBatchMixedInc, float, float, double, 1)

@@ -64,6 +64,14 @@ tridSmtsvStridedBatch = _scalar9("tridSmtsvStridedBatch")
 tridDmtsvStridedBatch = _scalar9("tridDmtsvStridedBatch")
 tridSmtsvStridedBatchInc = _scalar9("tridSmtsvStridedBatchInc")
 tridDmtsvStridedBatchInc = _scalar9("tridDmtsvStridedBatchInc")
+# complex element types (the reference's commented-out tridC/ZmtsvStridedBatch,
+# trid_cuda.cu:546-600) and FP32 storage with FP64 arithmetic
+tridCmtsvStridedBatch = _scalar9("tridCmtsvStridedBatch")
+tridCmtsvStridedBatchInc = _scalar9("tridCmtsvStridedBatchInc")
+tridZmtsvStridedBatch = _scalar9("tridZmtsvStridedBatch")
+tridZmtsvStridedBatchInc = _scalar9("tridZmtsvStridedBatchInc")
+tridSmtsvStridedBatchMixed = _scalar9("tridSmtsvStridedBatchMixed")
+tridSmtsvStridedBatchMixedInc = _scalar9("tridSmtsvStridedBatchMixedInc")
 tridSmtsvStridedBatchPadded = _padded("tridSmtsvStridedBatchPadded")
 tridDmtsvStridedBatchPadded = _padded("tridDmtsvStridedBatchPadded")
 tridSmtsvStridedBatchPaddedInc = _padded("tridSmtsvStridedBatchPaddedInc")
@@ -141,11 +149,13 @@ def set_method(method=0, chunk=0, sys_per_cta=0):
         raise TridError(st, "tridSetMethod")
 
 
-def solve(a, b, c, d, dim=-1, u=None, inc=False):
+def solve(a, b, c, d, dim=-1, u=None, inc=False, fp64_arithmetic=False):
     """Solve the tridiagonal systems along torch dimension ``dim``.
 
     a, b, c, d (and u for ``inc``) are contiguous CUDA tensors of one shape
-    and dtype (float32 or float64).  Without ``inc`` the solution overwrites
+    and dtype (float32, float64, complex64 or complex128).
+    ``fp64_arithmetic`` (float32 only) solves in FP64 and rounds each result
+    to float32 once.  Without ``inc`` the solution overwrites
     ``d`` (returned); with ``inc`` it is added to ``u`` (returned) and ``d``
     is left unchanged.  Torch's dimension k is the library's axis ndim-1-k
     (the last torch dimension is the unit-stride axis 0).
@@ -162,12 +172,18 @@ def solve(a, b, c, d, dim=-1, u=None, inc=False):
     dim = dim % ndim
     dims = list(reversed(shape))
     solvedim = ndim - 1 - dim
-    if d.dtype == torch.float64:
-        fn = tridDmtsvStridedBatchInc if inc else tridDmtsvStridedBatch
-    elif d.dtype == torch.float32:
-        fn = tridSmtsvStridedBatchInc if inc else tridSmtsvStridedBatch
-    else:
-        raise TypeError("float32 or float64 only")
+    fns = {
+        torch.float64: (tridDmtsvStridedBatch, tridDmtsvStridedBatchInc),
+        torch.float32: ((tridSmtsvStridedBatchMixed, tridSmtsvStridedBatchMixedInc)
+                        if fp64_arithmetic else (tridSmtsvStridedBatch, tridSmtsvStridedBatchInc)),
+        torch.complex128: (tridZmtsvStridedBatch, tridZmtsvStridedBatchInc),
+        torch.complex64: (tridCmtsvStridedBatch, tridCmtsvStridedBatchInc),
+    }
+    if d.dtype not in fns:
+        raise TypeError("float32, float64, complex64 or complex128 only")
+    if fp64_arithmetic and d.dtype != torch.float32:
+        raise TypeError("fp64_arithmetic applies to float32 tensors")
+    fn = fns[d.dtype][1 if inc else 0]
     st = fn(a, b, c, d, u, ndim, solvedim, dims, dims)
     if st != 0:
         raise TridError(st, fn.__name__)
