@@ -35,11 +35,13 @@ def dev(x):
     return torch.from_numpy(np.ascontiguousarray(x)).cuda()
 
 
-def geometry(n, solvedim):
-    """dims with n along solvedim; padded axes 0 and 2."""
-    dims = [37, 5, 3]
+def geometry(n, solvedim, rows16=False):
+    """dims with n along solvedim; padded axes 0 and 2.  rows16: axis 0 of 48
+    systems padded to 52 (whole 16-system tiles, rows on 16-byte boundaries:
+    the strided axes take 16-byte copies)."""
+    dims = [48 if rows16 else 37, 5, 3]
     dims[solvedim] = n
-    pads = [dims[0] + 2, dims[1], dims[2] + 1]
+    pads = [dims[0] + (4 if rows16 else 2), dims[1], dims[2] + 1]
     return dims, pads
 
 
@@ -53,10 +55,13 @@ def outside(dims, pads):
 @pytest.mark.parametrize("n", [1, 2, 3, 31, 64, 129, 256, 300, 512, 700])
 @pytest.mark.parametrize("solvedim", [0, 1, 2])
 @pytest.mark.parametrize("inc", [False, True])
-def test_complex_strided(kind, n, solvedim, inc):
+@pytest.mark.parametrize("rows16", [False, True])
+def test_complex_strided(kind, n, solvedim, inc, rows16):
+    if rows16 and solvedim == 0:
+        pytest.skip("axis 0 has no tiles of systems")
     ndt, f, finc, tol = CPLX[kind]
     rng = np.random.default_rng(1000 * n + 10 * solvedim + inc + (7 if kind == "c" else 0))
-    dims, pads = geometry(n, solvedim)
+    dims, pads = geometry(n, solvedim, rows16)
     size = int(np.prod(pads))
     a, b, c, d = rand_complex_coeffs(rng, size, ndt)
     u = (rng.standard_normal(size) + 1j * rng.standard_normal(size)).astype(ndt)
@@ -77,9 +82,12 @@ def test_complex_strided(kind, n, solvedim, inc):
 @pytest.mark.parametrize("n", [1, 2, 5, 64, 200, 256, 400, 512, 1000])
 @pytest.mark.parametrize("solvedim", [0, 1, 2])
 @pytest.mark.parametrize("inc", [False, True])
-def test_mixed_strided(n, solvedim, inc):
+@pytest.mark.parametrize("rows16", [False, True])
+def test_mixed_strided(n, solvedim, inc, rows16):
+    if rows16 and solvedim == 0:
+        pytest.skip("axis 0 has no tiles of systems")
     rng = np.random.default_rng(77 * n + 3 * solvedim + inc)
-    dims, pads = geometry(n, solvedim)
+    dims, pads = geometry(n, solvedim, rows16)
     size = int(np.prod(pads))
     a, b, c, d = rand_coeffs(rng, size, np.float32)
     u = rng.standard_normal(size).astype(np.float32)

@@ -15,7 +15,9 @@
 //
 //  ext_x_kernel       axis 0 (unit stride), n <= 32*M: one warp per system,
 //                     lane t owns rows [t*M, t*M+M).
-//  ext_strided_kernel axes >= 1, n <= 32*M: a CTA owns SB adjacent systems
+//  ext_stream_kernel  axes >= 1, n <= 32*8: persistent, tiles streamed
+//                     through shared memory by cp.async (below).
+//  ext_strided_kernel axes >= 1, n <= 32*M (longer chunks): a CTA owns SB adjacent systems
 //                     (SB*sizeof(S) = 128 B rows for the complex types up to
 //                     256 rows, 64 B otherwise) x 32 chunks; the interface
 //                     rows go through shared memory to SB warps, one
@@ -25,6 +27,7 @@
 #include <cstring>
 
 #include "partition.cuh"
+#include "tma.cuh"
 #include "trid_b200.h"
 
 namespace tridb200 {
@@ -96,6 +99,7 @@ struct Elem<float, double> {
   static __device__ __forceinline__ double ld(const float *p) { return (double)__ldg(p); }
   static __device__ __forceinline__ double ldw(const float *p) { return (double)*p; }
   static __device__ __forceinline__ void st(float *p, double v) { *p = (float)v; }
+  static __device__ __forceinline__ double cv(float v) { return (double)v; }
 };
 template <>
 struct Elem<float2, Cx<float>> {
@@ -108,6 +112,7 @@ struct Elem<float2, Cx<float>> {
     return {v.x, v.y};
   }
   static __device__ __forceinline__ void st(float2 *p, Cx<float> v) { *p = make_float2(v.x, v.y); }
+  static __device__ __forceinline__ Cx<float> cv(float2 v) { return {v.x, v.y}; }
 };
 template <>
 struct Elem<double2, Cx<double>> {
@@ -122,6 +127,7 @@ struct Elem<double2, Cx<double>> {
   static __device__ __forceinline__ void st(double2 *p, Cx<double> v) {
     *p = make_double2(v.x, v.y);
   }
+  static __device__ __forceinline__ Cx<double> cv(double2 v) { return {v.x, v.y}; }
 };
 
 // x -> d (INC = 0) or u += x (INC = 1)
@@ -245,6 +251,157 @@ __global__ void __launch_bounds__(SB * kWarp) ext_strided_kernel(Geom g, const S
   }
 }
 
+// Element-wise asynchronous global -> shared copies of 4, 8 or 16 bytes
+// (cp.async; 16-byte copies bypass L1)
+template <int B>
+__device__ __forceinline__ void cp_async_elem(void *dst, const void *src) {
+  if constexpr (B == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src),
+                 "n"(B)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Strided axes, persistent (one CTA per SM): tiles of SB adjacent systems x n
+// rows of every array stream into shared memory by per-element cp.async
+// (consecutive threads take consecutive systems of a row: coalesced), each
+// thread copies its chunk rows into registers, the buffer is released and
+// the next tile's copies are issued before the current tile is solved (as
+// ext_strided_kernel), so the copies overlap the arithmetic.
+// VEC: every tile is SB consecutive systems of one axis-0 row with 16-byte
+// aligned rows (dims[0] a multiple of SB, row strides multiples of 16 bytes),
+// so the copies move 16 bytes (16/sizeof(S) systems) each.
+template <typename S, typename T, int M, int SB, int INC, bool VEC>
+__global__ void __launch_bounds__(SB * kWarp, 1) ext_stream_kernel(Geom g, const S *__restrict__ a,
+                                                                   const S *__restrict__ b,
+                                                                   const S *__restrict__ c,
+                                                                   S *__restrict__ d,
+                                                                   S *__restrict__ u,
+                                                                   int64_t ntiles) {
+  using E = Elem<S, T>;
+  constexpr int NA = INC ? 5 : 4;
+  extern __shared__ __align__(16) unsigned char ext_smem[];
+  // per array, the tile's system offsets (-1: past the last system); two
+  // sets, the next tile's written while the current one is in use
+  __shared__ int64_t soff[2][NA][SB];
+  const int n = g.n;
+  const size_t tsz = (size_t)n * SB;  // [row][system] per array
+  S *tile = reinterpret_cast<S *>(ext_smem);
+  T *red = reinterpret_cast<T *>(tile + NA * tsz);  // [8][32][SB+1]
+  T *sol = red + 8 * kWarp * (SB + 1);               // [2][32][SB+1]
+  const S *src[5] = {a, b, c, d, u};
+  const int tid = threadIdx.x;
+  const int sl = tid % SB;
+  const int t = tid / SB;
+  auto offsets = [&](int64_t blk, int buf) {
+    if (tid < SB) {
+      const int64_t s = blk * SB + tid;
+      int64_t off[5] = {-1, -1, -1, -1, -1};
+      if (s < g.nsys) system_offsets(g, s, off);
+#pragma unroll
+      for (int q = 0; q < NA; ++q) soff[buf][q][tid] = s < g.nsys ? off[q] : -1;
+    }
+  };
+  auto issue = [&](int buf) {
+    if constexpr (VEC) {
+      constexpr int V = 16 / (int)sizeof(S);  // systems per copy
+      constexpr int PR = SB / V;              // copies per row
+#pragma unroll
+      for (int q = 0; q < NA; ++q) {
+        const int64_t base = soff[buf][q][0];
+        const int64_t str = g.stride[q];
+        for (int i = tid; i < n * PR; i += SB * kWarp) {
+          const int r = i / PR, v = i % PR;
+          cp_async_elem<16>(tile + q * tsz + (size_t)r * SB + v * V, src[q] + base + r * str + v * V);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < NA; ++q) {
+        const int64_t base = soff[buf][q][sl];
+        if (base < 0) continue;
+        const int64_t str = g.stride[q];
+        for (int r = t; r < n; r += kWarp)
+          cp_async_elem<(int)sizeof(S)>(tile + q * tsz + (size_t)r * SB + sl,
+                                        src[q] + base + r * str);
+      }
+    }
+    cp_async_commit();
+  };
+  auto R = [&](int comp, int chunk, int s) -> T & {
+    return red[((size_t)comp * kWarp + chunk) * (SB + 1) + s];
+  };
+
+  int64_t blk = blockIdx.x;
+  if (blk >= ntiles) return;
+  offsets(blk, 0);
+  __syncthreads();
+  issue(0);
+  int buf = 0;
+  const int r0 = t * M;
+  const int64_t so = INC ? g.stride[kU] : g.stride[kD];
+  S *const out = INC ? u : d;
+  for (; blk < ntiles; blk += gridDim.x) {
+    const int64_t nxt = blk + gridDim.x;
+    if (nxt < ntiles) offsets(nxt, buf ^ 1);
+    cp_async_wait_all();
+    __syncthreads();  // every thread's copies of this tile have landed
+    const int64_t obase = soff[buf][INC ? kU : kD][sl];
+    const bool valid = obase >= 0;
+    T al[M], be[M], ga[M], de[M], uo[INC ? M : 1];
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int r = r0 + j;
+      const bool in = valid && r < n;
+      const size_t o = (size_t)(r < n ? r : n - 1) * SB + sl;
+      al[j] = (in && r != 0) ? E::cv(tile[o]) : T(0);
+      be[j] = in ? E::cv(tile[tsz + o]) : T(1);
+      ga[j] = (in && r != n - 1) ? E::cv(tile[2 * tsz + o]) : T(0);
+      de[j] = in ? E::cv(tile[3 * tsz + o]) : T(0);
+      if constexpr (INC) uo[j] = in ? E::cv(tile[4 * tsz + o]) : T(0);
+    }
+    __syncthreads();  // the tile is free: the next one streams in meanwhile
+    if (nxt < ntiles) issue(buf ^ 1);
+
+    Row<T> F, L;
+    chunk_reduce<T, M>(al, be, ga, de, F, L);
+    R(0, t, sl) = F.a;
+    R(1, t, sl) = F.b;
+    R(2, t, sl) = F.c;
+    R(3, t, sl) = F.d;
+    R(4, t, sl) = L.a;
+    R(5, t, sl) = L.b;
+    R(6, t, sl) = L.c;
+    R(7, t, sl) = L.d;
+    __syncthreads();
+    {
+      const int w = tid / kWarp;
+      const int lane = tid & (kWarp - 1);
+      const Row<T> F2{R(0, lane, w), R(1, lane, w), R(2, lane, w), R(3, lane, w)};
+      const Row<T> L2{R(4, lane, w), R(5, lane, w), R(6, lane, w), R(7, lane, w)};
+      T xF, xL;
+      warp_interface_solve(F2, L2, xF, xL, lane);
+      sol[(0 * kWarp + lane) * (SB + 1) + w] = xF;
+      sol[(1 * kWarp + lane) * (SB + 1) + w] = xL;
+    }
+    __syncthreads();
+    chunk_backsub<T, M>(al, ga, de, sol[(0 * kWarp + t) * (SB + 1) + sl],
+                        sol[(1 * kWarp + t) * (SB + 1) + sl]);
+    if (valid) {
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        const int r = r0 + j;
+        if (r < n) E::st(out + obase + r * so, INC ? uo[INC ? j : 0] + de[j] : de[j]);
+      }
+    }
+    buf ^= 1;
+  }
+}
+
 // Thomas in the reference's operation order (scalar/src/cpu/trid_cpu.cpp:
 // 360-401); a[0] and c[n-1] are never read
 template <typename S, typename T, int INC>
@@ -296,6 +453,9 @@ __global__ void __launch_bounds__(128) ext_thomas_kernel(Geom g, const S *__rest
 // Largest chunk (rows per lane) of the partitioned kernels: 16 for 8-byte
 // arithmetic, 8 for complex<double> (16 rows of 16 bytes per array exceed the
 // register file at one CTA per SM).
+// dynamic shared memory of the streamed kernel: tile plus interface rows
+constexpr size_t kExtStreamSmem = 200 * 1024;
+
 template <typename T>
 constexpr int ext_max_chunk() {
   return sizeof(T) >= 16 ? 8 : 16;
@@ -325,6 +485,45 @@ cudaError_t launch_ext(const Geom &g, int solvedim, const S *a, const S *b, cons
     // SB systems per CTA: 8 for 16-byte T and for 16-row chunks (whose 64
     // register-resident values per thread need 256-thread CTAs), else 16
     constexpr int SB = sizeof(T) >= 16 ? 8 : 16;
+    if (M <= 8) {
+      // streamed tiles, one CTA per SM
+      constexpr int NA = INC ? 5 : 4;
+      const size_t smem = (size_t)NA * g.n * SB * sizeof(S) + (size_t)10 * kWarp * (SB + 1) * sizeof(T);
+      int dev = 0, sms = 0;
+      if (smem <= kExtStreamSmem && cudaGetDevice(&dev) == cudaSuccess &&
+          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess) {
+        const int64_t ntiles = (g.nsys + SB - 1) / SB;
+        const unsigned grid = (unsigned)(ntiles < sms ? ntiles : sms);
+        auto go = [&](auto kern) {
+          cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem);
+          if (e != cudaSuccess) return e;
+          kern<<<dim3(grid), dim3(SB * kWarp), smem, st>>>(g, a, b, c, d, u, ntiles);
+          return cudaGetLastError();
+        };
+        // 16-byte copies: whole tiles in one row, 16-byte aligned bases and
+        // row strides (elements narrower than 16 bytes only)
+        bool vec = sizeof(S) < 16 && g.odims[0] % SB == 0;
+        const void *ptrs[5] = {a, b, c, d, u};
+        constexpr int64_t kV = 16 / (int64_t)sizeof(S);
+        for (int q = 0; q < NA && vec; ++q) {
+          vec = ((uintptr_t)ptrs[q] & 15) == 0 && g.stride[q] % kV == 0;
+          for (int k = 1; k < g.nod && vec; ++k) vec = g.ocum[q][k] % kV == 0;
+        }
+        if (vec) {
+          switch (M) {
+            case 2: return go(ext_stream_kernel<S, T, 2, SB, INC, true>);
+            case 4: return go(ext_stream_kernel<S, T, 4, SB, INC, true>);
+            default: return go(ext_stream_kernel<S, T, 8, SB, INC, true>);
+          }
+        }
+        switch (M) {
+          case 2: return go(ext_stream_kernel<S, T, 2, SB, INC, false>);
+          case 4: return go(ext_stream_kernel<S, T, 4, SB, INC, false>);
+          default: return go(ext_stream_kernel<S, T, 8, SB, INC, false>);
+        }
+      }
+    }
     auto go = [&](auto kern, int sb) {
       const int64_t blocks = (g.nsys + sb - 1) / sb;
       if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
