@@ -506,13 +506,17 @@ def run_suite(args):
         d = torch.randn(shape, dtype=dtype, device=dev, generator=gen)
         return a, b, c, d
 
+    def want(name):
+        return args.only is None or args.only in name
+
     # FP32 256^3, each axis (20 B per unknown)
-    a, b, c, d = coeffs((UNKNOWNS,), torch.float32)
-    for sd in range(3):
-        ms = timed(lambda: tb.tridSmtsvStridedBatch(a, b, c, d, None, 3, sd, DIMS, DIMS))
-        emit({"workload": f"FP32 256^3 solvedim {sd}", "ms": round(ms, 5),
-              "gbs": round(20 * UNKNOWNS / (ms * 1e-3) / 1e9, 1)})
-    del a, b, c, d
+    if want("FP32 256^3"):
+        a, b, c, d = coeffs((UNKNOWNS,), torch.float32)
+        for sd in range(3):
+            ms = timed(lambda: tb.tridSmtsvStridedBatch(a, b, c, d, None, 3, sd, DIMS, DIMS))
+            emit({"workload": f"FP32 256^3 solvedim {sd}", "ms": round(ms, 5),
+                  "gbs": round(20 * UNKNOWNS / (ms * 1e-3) / 1e9, 1)})
+        del a, b, c, d
 
     # complex128 / complex64 256^3 (5 elements of 16 / 8 B per unknown) and
     # FP32 storage with FP64 arithmetic (20 B per unknown), each axis
@@ -530,6 +534,8 @@ def run_suite(args):
                                  ("complex64", torch.complex64, tb.tridCmtsvStridedBatch, 40),
                                  ("FP32 storage / FP64 arithmetic", torch.float32,
                                   tb.tridSmtsvStridedBatchMixed, 20)):
+        if not want(name):
+            continue
         a, b, c, d = (ccoeffs((UNKNOWNS,), dtype) if dtype.is_complex
                       else coeffs((UNKNOWNS,), dtype))
         for sd in range(3):
@@ -537,6 +543,8 @@ def run_suite(args):
             emit({"workload": f"{name} 256^3 solvedim {sd}", "ms": round(ms, 5),
                   "gbs": round(bpu * UNKNOWNS / (ms * 1e-3) / 1e9, 1)})
         del a, b, c, d
+    if args.only is not None:  # the remaining workloads are not selectable
+        return
 
     sc = args.scale  # fraction of each workload's systems (1 = the configured sizes)
     assert 0 < sc <= 1, "--scale in (0, 1]"
@@ -679,6 +687,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--suite", action="store_true",
                     help="instead: one JSON line per other workload of the path (1 GPU)")
+    ap.add_argument("--only", default=None,
+                    help="--suite: run only the cube workloads whose name contains this "
+                         "(e.g. 'complex128', 'FP32 storage')")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="--suite: fraction of each workload's systems (profiling runs)")
     args = ap.parse_args()
