@@ -15,17 +15,16 @@
 //
 //  ext_x_kernel       axis 0 (unit stride), n <= 32*M: one warp per system,
 //                     lane t owns rows [t*M, t*M+M).
-//  ext_stream_kernel  axes >= 1, n <= 32*8: persistent, tiles streamed
-//                     through shared memory by cp.async (below).
-//  ext_strided_kernel axes >= 1, n <= 32*M (longer chunks): a CTA owns SB adjacent systems
-//                     (SB*sizeof(S) = 128 B rows for the complex types up to
-//                     256 rows, 64 B otherwise) x 32 chunks; the interface
-//                     rows go through shared memory to SB warps, one
-//                     interface system each.
-//  ext_thomas_kernel  any n: one thread per system, Thomas with c'/d' in
-//                     library scratch laid out [row][system] (in T).
-#include <cstring>
-
+//  ext_stream_kernel  axes >= 1, n <= 256 (tile within 200 KB of shared
+//                     memory): persistent, one CTA per SM; tiles of SB
+//                     systems x n rows stream through shared memory by
+//                     cp.async while the previous tile is solved.
+//  ext_strided_kernel the other axes >= 1 cases up to 512 rows: a CTA owns
+//                     SB adjacent systems x 32 chunks; the interface rows go
+//                     through shared memory to one warp per system.
+//  ext_thomas_kernel  longer systems: one thread per system, Thomas with
+//                     c'/d' in library scratch laid out [row][system] (in T).
+// The longest chunk is 16 rows for 8-byte T and 8 for complex<double>.
 #include "partition.cuh"
 #include "tma.cuh"
 #include "trid_b200.h"
