@@ -126,6 +126,22 @@ def test_complex_and_mixed_invalid_arguments_rejected():
     assert tb.tridSmtsvStridedBatchMixed(q, q + 2, q, q, None, 1, 0, [8], [8]) == INVALID
 
 
+def test_solve_rejects_unsupported_dtypes_on_the_host():
+    """solve() checks the element type before any pointer or CUDA call:
+    float16 and fp64_arithmetic on non-float32 tensors raise TypeError."""
+    torch = pytest.importorskip("torch")
+    h = torch.ones(2, 8, dtype=torch.float16)
+    with pytest.raises(TypeError):
+        tb.solve(h, h, h, h)
+    for dt in (torch.float64, torch.complex64, torch.complex128):
+        x = torch.ones(2, 8, dtype=dt)
+        with pytest.raises(TypeError):
+            tb.solve(x, x, x, x, fp64_arithmetic=True)
+    x = torch.ones(2, 8, dtype=torch.complex128)  # supported type, host tensor
+    with pytest.raises(ValueError):
+        tb.solve(x, x, x, x)
+
+
 def test_bad_opts_rejected_by_padded_and_compat():
     p, _keep = _fake()
     st = tb.tridDmtsvStridedBatchPadded(p, [8], p, [8], p, [8], p, [8], None, [8], 1, 0, [8],
