@@ -142,6 +142,29 @@ def test_solve_rejects_unsupported_dtypes_on_the_host():
         tb.solve(x, x, x, x)
 
 
+def test_component_modules_reject_other_element_types():
+    """block, varlen and ADI take float32/float64 only: a complex or float16
+    tensor raises TypeError on the host instead of reaching the FP32 entry
+    point."""
+    torch = pytest.importorskip("torch")
+    from tridsolver_b200 import adi, block, varlen
+    for dt in (torch.complex128, torch.float16):
+        A = torch.ones(3, 2, 2, 2, dtype=dt)
+        d = torch.ones(3, 2, 2, dtype=dt)
+        with pytest.raises(TypeError):
+            block.btsv(A, A, A, d)
+        with pytest.raises(TypeError):
+            block.btsv_adjoint(A, A, A, d, d)
+        v = torch.ones(8, dtype=dt)
+        with pytest.raises(TypeError):
+            varlen.solve_varlen(v, v, v, v, torch.tensor([0, 8]))
+    A64, d32 = torch.ones(3, 2, 2, 2, dtype=torch.float64), torch.ones(3, 2, 2)
+    with pytest.raises(TypeError):  # mixed element types
+        block.btsv(A64, A64, A64, d32)
+    with pytest.raises(TypeError):
+        adi.ADI((4, 4, 4), 1.0, dtype=torch.complex128, device="cpu")
+
+
 def test_bad_opts_rejected_by_padded_and_compat():
     p, _keep = _fake()
     st = tb.tridDmtsvStridedBatchPadded(p, [8], p, [8], p, [8], p, [8], None, [8], 1, 0, [8],

@@ -51,6 +51,8 @@ class ADI:
         self.kind = coeffs
         self.a, self.b, self.c = COEFFS[coeffs][0](self.lam)
         self.da, self.db, self.dc = COEFFS[coeffs][1]
+        if dtype not in (torch.float32, torch.float64):
+            raise TypeError("ADI runs in float32 or float64")
         self.dtype = dtype
         self.work = torch.empty((2,) + tuple(shape), dtype=dtype, device=device)
         self._graph = None
@@ -58,6 +60,8 @@ class ADI:
 
     # ------------------------------------------------------------ forward --
     def step(self, u, nsteps=1):
+        if u.dtype != self.dtype:
+            raise TypeError(f"u is {u.dtype}, this ADI runs in {self.dtype}")
         L = lib()
         _bind_stream(L)
         fn = L.tridDadiSteps if self.dtype == torch.float64 else L.tridSadiSteps
@@ -88,6 +92,8 @@ class ADI:
         return u
 
     def _solve(self, rhs, out, axis, stencil=0, transpose=0, inc=0):
+        if rhs.dtype != self.dtype or out.dtype != self.dtype:
+            raise TypeError(f"arrays must be {self.dtype}")
         L = lib()
         _bind_stream(L)
         fn = L.tridDadiSolve if self.dtype == torch.float64 else L.tridSadiSolve

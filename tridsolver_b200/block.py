@@ -11,7 +11,7 @@ import ctypes
 import torch
 
 from ._lib import TridError, c_int, lib, register, vp
-from .scalar import _bind_stream, _ptr
+from .scalar import _bind_stream, _ptr, _real_dtype
 
 _BT = [vp, vp, vp, vp, vp, c_int, c_int, c_int, vp, vp]
 _BTA = [vp, vp, vp, vp, vp, vp, vp, vp, vp, c_int, c_int, c_int]
@@ -32,10 +32,11 @@ def _shape(A, d):
 def btsv(A, B, C, d, x=None, Cstar=None, dstar=None):
     """Solve the block systems; returns x (new tensor unless given)."""
     N, P, M = _shape(A, d)
+    dt = _real_dtype(A, B, C, d, x, Cstar, dstar)
     x = torch.empty_like(d) if x is None else x
     L = lib()
     _bind_stream(L)
-    fn = L.tridDbtsvBatch if d.dtype == torch.float64 else L.tridSbtsvBatch
+    fn = L.tridDbtsvBatch if dt == torch.float64 else L.tridSbtsvBatch
     st = fn(_ptr(A), _ptr(B), _ptr(C), _ptr(d), _ptr(x), N, P, M, _ptr(Cstar), _ptr(dstar))
     if st != 0:
         raise TridError(st, fn.__name__)
@@ -45,10 +46,11 @@ def btsv(A, B, C, d, x=None, Cstar=None, dstar=None):
 def btsv_adjoint(A, B, C, u, w, need=(True, True, True, True)):
     """Gradients (dA, dB, dC, dd) of a loss with dL/dx = w at the solution u."""
     N, P, M = _shape(A, u)
+    dt = _real_dtype(A, B, C, u, w)
     outs = [torch.empty_like(t) if k else None for k, t in zip(need, (A, B, C, u))]
     L = lib()
     _bind_stream(L)
-    fn = L.tridDbtsvBatchAdjoint if u.dtype == torch.float64 else L.tridSbtsvBatchAdjoint
+    fn = L.tridDbtsvBatchAdjoint if dt == torch.float64 else L.tridSbtsvBatchAdjoint
     st = fn(_ptr(A), _ptr(B), _ptr(C), _ptr(u), _ptr(w), *[_ptr(o) for o in outs], N, P, M)
     if st != 0:
         raise TridError(st, fn.__name__)

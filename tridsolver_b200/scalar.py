@@ -30,6 +30,15 @@ def _ptr(x):
     raise TypeError(f"expected a CUDA tensor or a device pointer, got {type(x)}")
 
 
+def _real_dtype(*tensors):
+    """The common element type of the given tensors (None entries skipped),
+    float32 or float64; anything else raises TypeError before any call."""
+    dts = {t.dtype for t in tensors if t is not None}
+    if len(dts) != 1 or next(iter(dts)) not in (torch.float32, torch.float64):
+        raise TypeError(f"float32 or float64 tensors of one dtype only, got {sorted(map(str, dts))}")
+    return next(iter(dts))
+
+
 def _bind_stream(L):
     if torch is not None and torch.cuda.is_available() and torch.cuda.is_initialized():
         L.tridSetStream(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))

@@ -10,7 +10,7 @@ import ctypes
 import torch
 
 from ._lib import TridError, c_int, lib, register, vp
-from .scalar import _bind_stream, _ptr
+from .scalar import _bind_stream, _ptr, _real_dtype
 
 c_ll = ctypes.c_longlong
 register({
@@ -21,13 +21,14 @@ register({
 
 
 def solve_varlen(a, b, c, d, offsets, total=None):
+    dt = _real_dtype(a, b, c, d)
     if offsets.dtype != torch.int64 or not offsets.is_cuda:
         raise TypeError("offsets: int64 CUDA tensor of nsys+1 entries")
     nsys = offsets.numel() - 1
     total = d.numel() if total is None else int(total)
     L = lib()
     _bind_stream(L)
-    fn = L.tridDmtsvVarlenBatch if d.dtype == torch.float64 else L.tridSmtsvVarlenBatch
+    fn = L.tridDmtsvVarlenBatch if dt == torch.float64 else L.tridSmtsvVarlenBatch
     st = fn(_ptr(a), _ptr(b), _ptr(c), _ptr(d), _ptr(offsets), nsys, total)
     if st != 0:
         raise TridError(st, fn.__name__)
