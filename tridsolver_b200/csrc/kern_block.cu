@@ -620,6 +620,9 @@ struct BlkMRow {
   T A[M * M], B[M * M], C[M * M], d[M];
 };
 
+// K consecutive values at p: 16-byte accesses for FP64 when K is even (the
+// M = 4 blocks and vectors, whose arrays the dispatch requires to be 16-byte
+// aligned), one value at a time otherwise (M = 3, FP32).
 template <typename T, int K>
 __device__ __forceinline__ void blkm_ld(const T *p, T (&r)[K]) {
   if constexpr (sizeof(T) == 8 && K % 2 == 0) {
