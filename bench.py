@@ -315,8 +315,8 @@ def measure_differentiation(torch, tb, steps, seed=99):
     forward solve, the forward + adjoint in one call
     (tridDmtsvStridedBatchFwdAdj: x and the gradients w.r.t. a, b, c, d) and
     the autograd path (trid_solve forward + backward), and checks the
-    gradients against central finite differences (h = 1e-6) on 16 sampled
-    entries.  Every array is 134 MB (> L2), so no flush between launches."""
+    gradients against central finite differences (h = 1e-6) on 64 sampled
+    entries (16 of each of a, b, c, d).  Every array is 134 MB (> L2), so no flush between launches."""
     S, n = 16384, 1024
     gen = torch.Generator(device="cuda").manual_seed(seed)
     a = torch.rand(S, n, dtype=torch.float64, device="cuda", generator=gen) * 2 - 1
@@ -367,7 +367,7 @@ def measure_differentiation(torch, tb, steps, seed=99):
     h = 1e-6
     errs, gmax = [], 0.0
     coefs = (a, b, c, d)
-    for k in range(16):
+    for k in range(64):
         which, s_, i = k % 4, int(rng.integers(S)), int(rng.integers(1, n - 1))
         rows = [t[s_:s_ + 1].clone() for t in coefs]
         vals = []
@@ -392,7 +392,7 @@ def measure_differentiation(torch, tb, steps, seed=99):
         "ratio_autograd_over_fwd": round(times["autograd"] / times["fwd"], 3),
         "target_ratio": 2.2,
         "grad_err_vs_fd": float(f"{max(errs) / max(1.0, gmax):.3e}"),
-        "fd": "central, h=1e-6, 16 sampled entries of a, b, c, d; error relative to max(1, max|g|)",
+        "fd": "central, h=1e-6, 64 sampled entries of a, b, c, d; error relative to max(1, max|g|)",
         "bytes_per_unknown": {"fwd": 40, "fwd_adj": 80, "autograd": "40 + 16 (copy of d) + 72"},
     }
 
