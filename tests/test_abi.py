@@ -246,3 +246,25 @@ def test_tuning_table_roundtrip(tmp_path):
     bad.write_text("f16 0 1 1 0 0\n")
     assert L.tridLoadTuningTable(str(bad).encode()) == INVALID
     assert L.tridLoadTuningTable(None) == 0
+
+
+@pytest.mark.parametrize("header", sorted(h for h in os.listdir(INCLUDE) if h.endswith(".h")))
+@pytest.mark.parametrize("lang,compiler,std", [("c", "gcc", "c99"), ("c++", "g++", "c++17")])
+def test_headers_compile_for_c_and_cxx_callers(tmp_path, header, lang, compiler, std):
+    """Each public header compiles on its own as C99 and C++17 (a caller
+    includes trid_b200.h or, for the 11-argument forms, trid_b200_cudacompat.h,
+    never both); the complex element types are interleaved (re, im) pairs of
+    8 / 16 bytes."""
+    import shutil
+    if shutil.which(compiler) is None:
+        pytest.skip(f"{compiler} not installed")
+    src = tmp_path / ("check.c" if lang == "c" else "check.cpp")
+    text = f'#include "{header}"\n'
+    if header == "trid_b200.h":
+        kw = "_Static_assert" if lang == "c" else "static_assert"
+        text += (f"{kw}(sizeof(tridComplexF) == 8, \"complex<float>\");\n"
+                 f"{kw}(sizeof(tridComplexD) == 16, \"complex<double>\");\n")
+    src.write_text(text)
+    r = subprocess.run([compiler, f"-std={std}", "-Wall", "-Werror", "-fsyntax-only", "-I", INCLUDE,
+                        "-x", lang, str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
