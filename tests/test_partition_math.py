@@ -9,7 +9,10 @@ warp_interface_solve, chunk_backsub), lane shuffles written as array shifts.
 Checked against the oracle's Thomas (the reference's operation order,
 trid_cpu.cpp:360-401) for every chunk size the kernels use, for lengths that
 fill the 32 chunks partly (identity rows past n) and for a PCR cut short
-(`span`: only the chunks holding rows take part).
+(`span`: only the chunks holding rows take part); and the two facts the
+adjoint and forward+adjoint kernels build on: the continuant recurrence
+(chunk_reduce_cont) gives the Thomas pivots, and the transposed system reuses
+them (chunk_reduce_given).
 """
 
 import numpy as np
@@ -34,6 +37,65 @@ def chunk_reduce(al, be, ga, de):
     al[:, 1] *= r
     for j in range(2, M - 1):
         r = 1.0 / (be[:, j] - al[:, j] * ga[:, j - 1])
+        de[:, j] = (de[:, j] - al[:, j] * de[:, j - 1]) * r
+        al[:, j] = -(al[:, j] * al[:, j - 1]) * r
+        ga[:, j] = ga[:, j] * r
+    D, A, C = de[:, M - 2].copy(), al[:, M - 2].copy(), ga[:, M - 2].copy()
+    L = (-al[:, M - 1] * A, be[:, M - 1] - al[:, M - 1] * C, ga[:, M - 1].copy(),
+         de[:, M - 1] - al[:, M - 1] * D)
+    for j in range(M - 3, 0, -1):
+        D = de[:, j] - ga[:, j] * D
+        A = al[:, j] - ga[:, j] * A
+        C = -ga[:, j] * C
+    F = (al[:, 0].copy(), be[:, 0] - ga[:, 0] * A, -ga[:, 0] * C, de[:, 0] - ga[:, 0] * D)
+    return F, L
+
+
+def interior_pivots(al, be, ga):
+    """Reciprocal Thomas pivots 1/p_j (j = 1..M-2) of each chunk's interior,
+    p_1 = b_1, p_j = b_j - a_j c_{j-1} / p_{j-1} (chunk_reduce_pivots)."""
+    M = al.shape[1]
+    rp = np.zeros_like(al)
+    p = be[:, 1].copy()
+    rp[:, 1] = 1.0 / p
+    for j in range(2, M - 1):
+        p = be[:, j] - al[:, j] * ga[:, j - 1] / p
+        rp[:, j] = 1.0 / p
+    return rp
+
+
+def pow2_inv_exponent(x):
+    """2^-e for x = m 2^e with m in [1, 2) (x normal, nonzero), else 1."""
+    m, k = np.frexp(x)
+    return np.where((x != 0) & np.isfinite(x), np.ldexp(1.0, 1 - k), 1.0)
+
+
+def continuant_pivots(al, be, ga):
+    """The same pivots from the continuant recurrence q_j = b_j q_{j-1} -
+    (a_j c_{j-1}) q_{j-2}, 1/p_j = q_{j-1} / q_j, the pair rescaled by a power
+    of two every 4 rows (chunk_reduce_cont)."""
+    M = al.shape[1]
+    rp = np.zeros_like(al)
+    qm2, qm1 = np.ones(al.shape[0]), be[:, 1].copy()
+    rp[:, 1] = 1.0 / be[:, 1]
+    for j in range(2, M - 1):
+        q = be[:, j] * qm1 - (al[:, j] * ga[:, j - 1]) * qm2
+        rp[:, j] = qm1 / q
+        qm2, qm1 = qm1, q
+        if j % 4 == 0:
+            sc = pow2_inv_exponent(q)
+            qm1, qm2 = qm1 * sc, qm2 * sc
+    return rp
+
+
+def chunk_reduce_given(al, be, ga, de, rp):
+    """chunk_reduce with the interior's reciprocal pivots given."""
+    M = al.shape[1]
+    ga[:, 1] *= rp[:, 1]
+    de[:, 1] *= rp[:, 1]
+    al[:, 1] *= rp[:, 1]
+    for j in range(2, M - 1):
+        r = rp[:, j]
         de[:, j] = (de[:, j] - al[:, j] * de[:, j - 1]) * r
         al[:, j] = -(al[:, j] * al[:, j - 1]) * r
         ga[:, j] = ga[:, j] * r
@@ -100,13 +162,17 @@ def chunk_backsub(al, ga, de, xF, xL):
     return de
 
 
-def partition_solve(a, b, c, d, M, span=W):
-    n = a.size
-    rows = W * M
+def chunks(a, b, c, d, M):
+    n, rows = a.size, W * M
     al, be, ga, de = np.zeros(rows), np.ones(rows), np.zeros(rows), np.zeros(rows)
     al[1:n], be[:n], ga[:n - 1], de[:n] = a[1:], b, c[:-1], d  # a_0, c_{n-1} never read
-    al, be, ga, de = (v.reshape(W, M) for v in (al, be, ga, de))
-    F, L = chunk_reduce(al, be, ga, de)
+    return [v.reshape(W, M) for v in (al, be, ga, de)]
+
+
+def partition_solve(a, b, c, d, M, span=W, rp=None):
+    n = a.size
+    al, be, ga, de = chunks(a, b, c, d, M)
+    F, L = chunk_reduce(al, be, ga, de) if rp is None else chunk_reduce_given(al, be, ga, de, rp)
     xF, xL = interface_solve(F, L, span)
     return chunk_backsub(al, ga, de, xF, xL).ravel()[:n]
 
@@ -124,3 +190,27 @@ def test_partitioned_thomas_matches_oracle(M, fill):
     span = 1 << int(np.ceil(np.log2(max(1, -(-n // M)))))
     xs = partition_solve(a, b, c, d, M, span=max(span, 2))
     assert np.abs(xs - expect).max() / np.abs(expect).max() < 1e-13
+
+
+@pytest.mark.parametrize("M", [4, 8, 16])
+def test_continuant_pivots_and_transpose_reuse(M):
+    """The continuant pivots equal the Thomas pivots, and the transposed
+    system (sub-diagonal c_{i-1}, super-diagonal a_{i+1}) solved with the
+    forward chunks' pivots matches the oracle's solve of the transpose: the
+    pivots depend on a_j c_{j-1} only."""
+    n = W * M
+    rng = np.random.default_rng(M)
+    a, b, c, d = rand_coeffs(rng, n)
+    al, be, ga, _ = chunks(a, b, c, d, M)
+    rp = interior_pivots(al, be, ga)
+    rc = continuant_pivots(al, be, ga)
+    assert np.abs(rc[:, 1:M - 1] - rp[:, 1:M - 1]).max() / np.abs(rp).max() < 1e-14
+    x = partition_solve(a, b, c, d, M, rp=rc)
+    expect = oracle.mtsv(a, b, c, d, dims=[n], solvedim=0)
+    assert np.abs(x - expect).max() / np.abs(expect).max() < 1e-13
+    at, ct = np.zeros(n), np.zeros(n)
+    at[1:], ct[:-1] = c[:-1], a[1:]
+    w = rng.standard_normal(n)
+    g = partition_solve(at, b, ct, w, M, rp=rc)
+    gexp = oracle.mtsv(at, b, ct, w, dims=[n], solvedim=0)
+    assert np.abs(g - gexp).max() / np.abs(gexp).max() < 1e-13
