@@ -82,7 +82,9 @@ TRID_EXTERN_C tridStatus_t tridDmtsvStridedBatchInc(const double *a, const doubl
  *      std::complex and C99 _Complex -- aligned to their size (8 / 16 bytes).
  *      Same algorithm in complex arithmetic, no pivoting: the rows must be
  *      safe for Gaussian elimination without pivoting (e.g. diagonally
- *      dominant in modulus). ---- */
+ *      dominant in modulus).  These and the Mixed forms below choose their
+ *      kernels by length and axis alone (tridSetMethod and the tuning table
+ *      apply to the real forms). ---- */
 typedef struct {
   float re, im;
 } tridComplexF;
