@@ -12,7 +12,9 @@ fill the 32 chunks partly (identity rows past n) and for a PCR cut short
 (`span`: only the chunks holding rows take part); and the two facts the
 adjoint and forward+adjoint kernels build on: the continuant recurrence
 (chunk_reduce_cont) gives the Thomas pivots, and the transposed system reuses
-them (chunk_reduce_given).
+them (chunk_reduce_given).  The long-system level on top (warp_block_basis,
+block_rows: blocks of 32 chunks reduced to two rows each, the block system
+solved at the next level) is checked the same way.
 """
 
 import numpy as np
@@ -214,3 +216,103 @@ def test_continuant_pivots_and_transpose_reuse(M):
     g = partition_solve(at, b, ct, w, M, rp=rc)
     gexp = oracle.mtsv(at, b, ct, w, dims=[n], solvedim=0)
     assert np.abs(g - gexp).max() / np.abs(gexp).max() < 1e-13
+
+
+def interface_solve_n(F, L, dF, dL):
+    """warp_interface_solve_n: the interface elimination with several
+    right-hand sides (dF, dL: [NR, W])."""
+    fa, fb, fc, _ = F
+    la, lb, lc, _ = L
+    lane = np.arange(W)
+    ifb = 1.0 / fb
+    nfa, nfi, nfc = down(fa, 1, 0.0), down(ifb, 1, 1.0), down(fc, 1, 0.0)
+    nfd = np.stack([down(v, 1, 0.0) for v in dF])
+    p, q = la * ifb, lc * nfi
+    ra, rb, rc = -p * fa, lb - p * fc - q * nfa, -q * nfc
+    rd = dL - p * dF - q * nfd
+    s = 1
+    while s < W:
+        ib = 1.0 / rb
+        sa, sc = ra * ib, rc * ib
+        k1 = np.where(lane >= s, ra, 0.0)
+        k2 = np.where(lane + s < W, rc, 0.0)
+        ua, uc, da, dc = up(sa, s), up(sc, s), down(sa, s, 0.0), down(sc, s, 0.0)
+        sd = rd * ib
+        rd = rd - k1 * np.stack([up(v, s) for v in sd]) - k2 * np.stack([down(v, s, 0.0) for v in sd])
+        ra, rc = -k1 * ua, -k2 * dc
+        rb = rb - k1 * uc - k2 * da
+        s <<= 1
+    xL = rd / rb
+    lprev = np.stack([up(v, 1) for v in xL])
+    xF = (dF - np.where(lane > 0, fa * lprev, 0.0) - fc * xL) * ifb
+    return xF, xL
+
+
+def block_basis(F, L):
+    """warp_block_basis: lane 0's F row and lane 31's L row replaced by
+    identity rows; right-hand sides (d, e_{F^B}, e_{L^B}) give every interface
+    unknown as P + F^B UF + L^B UL ([3, W] for the F and L unknowns)."""
+    F3 = [v.copy() for v in F]
+    L3 = [v.copy() for v in L]
+    dF = np.stack([F[3], np.zeros(W), np.zeros(W)])
+    dL = np.stack([L[3], np.zeros(W), np.zeros(W)])
+    F3[0][0], F3[1][0], F3[2][0] = 0.0, 1.0, 0.0
+    dF[:, 0] = (0.0, 1.0, 0.0)
+    L3[0][-1], L3[1][-1], L3[2][-1] = 0.0, 1.0, 0.0
+    dL[:, -1] = (0.0, 0.0, 1.0)
+    return interface_solve_n(F3, L3, dF, dL)
+
+
+def block_rows(F, L, bF, bL):
+    """The block's two reduced rows (block_rows) from lane 0's F row, lane
+    31's L row and the basis."""
+    fa, fb, fc, fd = (v[0] for v in F)
+    la, lb, lc, ld = (v[-1] for v in L)
+    l0P, l0F, l0L = bL[:, 0]
+    f31P, f31F, f31L = bF[:, -1]
+    FB = (fa, fb + fc * l0F, fc * l0L, fd - fc * l0P)
+    LB = (la * f31F, lb + la * f31L, lc, ld - la * f31P)
+    return FB, LB
+
+
+def blocked_solve(a, b, c, d, M):
+    """Blocks of 32*M rows: chunk reduction, block basis and block rows per
+    block, the block system (2 rows per block) by the oracle's Thomas, then
+    the interface unknowns from the basis and the chunk interiors."""
+    n = a.size
+    B = -(-n // (W * M))
+    rows = B * W * M
+    al, be, ga, de = np.zeros(rows), np.ones(rows), np.zeros(rows), np.zeros(rows)
+    al[1:n], be[:n], ga[:n - 1], de[:n] = a[1:], b, c[:-1], d
+    blocks = []
+    ra, rb, rc, rd = (np.zeros(2 * B) for _ in range(4))
+    for k in range(B):
+        sl = slice(k * W * M, (k + 1) * W * M)
+        ch = [v[sl].reshape(W, M).copy() for v in (al, be, ga, de)]
+        F, L = chunk_reduce(*ch)
+        bF, bL = block_basis(F, L)
+        FB, LB = block_rows(F, L, bF, bL)
+        ra[2 * k], rb[2 * k], rc[2 * k], rd[2 * k] = FB
+        ra[2 * k + 1], rb[2 * k + 1], rc[2 * k + 1], rd[2 * k + 1] = LB
+        blocks.append((ch, bF, bL))
+    xb = oracle.mtsv(ra, rb, rc, rd, dims=[2 * B], solvedim=0)
+    out = []
+    for k, (ch, bF, bL) in enumerate(blocks):
+        fB, lB = xb[2 * k], xb[2 * k + 1]
+        xF = bF[0] + fB * bF[1] + lB * bF[2]
+        xL = bL[0] + fB * bL[1] + lB * bL[2]
+        out.append(chunk_backsub(ch[0], ch[2], ch[3], xF, xL).ravel())
+    return np.concatenate(out)[:n]
+
+
+@pytest.mark.parametrize("M", [4, 8])
+@pytest.mark.parametrize("nblocks,ragged", [(1, 0), (3, 0), (5, 77), (9, 255)])
+def test_blocked_partition_matches_oracle(M, nblocks, ragged):
+    """The long-system method (warp_block_basis + block_rows, the block
+    system solved at the next level): whole and ragged last blocks."""
+    n = nblocks * W * M - ragged
+    rng = np.random.default_rng(n + M)
+    a, b, c, d = rand_coeffs(rng, n)
+    expect = oracle.mtsv(a, b, c, d, dims=[n], solvedim=0)
+    x = blocked_solve(a, b, c, d, M)
+    assert np.abs(x - expect).max() / np.abs(expect).max() < 1e-13
