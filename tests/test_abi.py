@@ -165,6 +165,21 @@ def test_component_modules_reject_other_element_types():
         adi.ADI((4, 4, 4), 1.0, dtype=torch.complex128, device="cpu")
 
 
+def test_complex_and_mixed_empty_problems_are_noops():
+    """A zero extent returns SUCCESS before any CUDA call (host buffers stand
+    in for device pointers and are left untouched)."""
+    p, keep = _fake()
+    q = (p + 15) & ~15
+    before = list(keep)
+    for fn in (tb.tridZmtsvStridedBatch, tb.tridCmtsvStridedBatch, tb.tridSmtsvStridedBatchMixed):
+        assert fn(q, q, q, q, None, 2, 0, [0, 10], [0, 10]) == 0
+        assert fn(q, q, q, q, None, 2, 1, [10, 0], [10, 0]) == 0
+    for fn in (tb.tridZmtsvStridedBatchInc, tb.tridCmtsvStridedBatchInc,
+               tb.tridSmtsvStridedBatchMixedInc):
+        assert fn(q, q, q, q, q, 3, 2, [4, 4, 0], [4, 4, 0]) == 0
+    assert list(keep) == before
+
+
 def test_bad_opts_rejected_by_padded_and_compat():
     p, _keep = _fake()
     st = tb.tridDmtsvStridedBatchPadded(p, [8], p, [8], p, [8], p, [8], None, [8], 1, 0, [8],
