@@ -14,7 +14,9 @@ adjoint and forward+adjoint kernels build on: the continuant recurrence
 (chunk_reduce_cont) gives the Thomas pivots, and the transposed system reuses
 them (chunk_reduce_given).  The long-system level on top (warp_block_basis,
 block_rows: blocks of 32 chunks reduced to two rows each, the block system
-solved at the next level) is checked the same way.
+solved at the next level) is checked the same way, and so is the
+one-CTA-per-system form whose block system is solved by the odd-even step
+plus PCR over the warps.
 """
 
 import numpy as np
@@ -115,7 +117,7 @@ def chunk_reduce_given(al, be, ga, de, rp):
 def down(v, s, fill):
     """__shfl_down_sync by s (lanes past the end keep `fill`)."""
     out = np.full_like(v, fill)
-    out[:W - s] = v[s:]
+    out[:v.size - s] = v[s:]
     return out
 
 
@@ -123,25 +125,28 @@ def up(v, s):
     """__shfl_up_sync by s (lanes below s read lane 0's value; every use is
     masked there)."""
     out = np.empty_like(v)
-    out[s:] = v[:W - s]
+    out[s:] = v[:v.size - s]
     out[:s] = v[:s]
     return out
 
 
 def interface_solve(F, L, span=W):
+    """warp_interface_solve over len(F[0]) lanes (32 for a warp; the number
+    of warps for the one-CTA kernel's block system)."""
     fa, fb, fc, fd = F
     la, lb, lc, ld = L
-    lane = np.arange(W)
+    nl = fa.size
+    lane = np.arange(nl)
     ifb = 1.0 / fb
     nfa, nfi, nfc, nfd = down(fa, 1, 0.0), down(ifb, 1, 1.0), down(fc, 1, 0.0), down(fd, 1, 0.0)
     p, q = la * ifb, lc * nfi
     ra, rb, rc, rd = -p * fa, lb - p * fc - q * nfa, -q * nfc, ld - p * fd - q * nfd
     s = 1
-    while s < W and s < span:
+    while s < nl and s < span:
         ib = 1.0 / rb
         sa, sc, sd = ra * ib, rc * ib, rd * ib
         k1 = np.where(lane >= s, ra, 0.0)
-        k2 = np.where(lane + s < W, rc, 0.0)
+        k2 = np.where(lane + s < nl, rc, 0.0)
         ua, uc, ud = up(sa, s), up(sc, s), up(sd, s)
         da, dc, dd = down(sa, s, 0.0), down(sc, s, 0.0), down(sd, s, 0.0)
         ra, rc = -k1 * ua, -k2 * dc
@@ -315,4 +320,46 @@ def test_blocked_partition_matches_oracle(M, nblocks, ragged):
     a, b, c, d = rand_coeffs(rng, n)
     expect = oracle.mtsv(a, b, c, d, dims=[n], solvedim=0)
     x = blocked_solve(a, b, c, d, M)
+    assert np.abs(x - expect).max() / np.abs(expect).max() < 1e-13
+
+
+def cta_solve(a, b, c, d, M, warps):
+    """The one-CTA-per-system form (513..4096 rows): a block of 32 chunks per
+    warp with its basis and two rows, the 2*warps-row block system solved by
+    the same odd-even step plus PCR over the warps (lanes = warps), then every
+    warp's interface unknowns and chunk interiors."""
+    n = a.size
+    rows = warps * W * M
+    assert n <= rows
+    al, be, ga, de = np.zeros(rows), np.ones(rows), np.zeros(rows), np.zeros(rows)
+    al[1:n], be[:n], ga[:n - 1], de[:n] = a[1:], b, c[:-1], d
+    blocks, FBs, LBs = [], [], []
+    for k in range(warps):
+        sl = slice(k * W * M, (k + 1) * W * M)
+        ch = [v[sl].reshape(W, M).copy() for v in (al, be, ga, de)]
+        F, L = chunk_reduce(*ch)
+        bF, bL = block_basis(F, L)
+        FB, LB = block_rows(F, L, bF, bL)
+        FBs.append(FB)
+        LBs.append(LB)
+        blocks.append((ch, bF, bL))
+    FBw = tuple(np.array([r[i] for r in FBs]) for i in range(4))
+    LBw = tuple(np.array([r[i] for r in LBs]) for i in range(4))
+    fB, lB = interface_solve(FBw, LBw)
+    out = []
+    for k, (ch, bF, bL) in enumerate(blocks):
+        xF = bF[0] + fB[k] * bF[1] + lB[k] * bF[2]
+        xL = bL[0] + fB[k] * bL[1] + lB[k] * bL[2]
+        out.append(chunk_backsub(ch[0], ch[2], ch[3], xF, xL).ravel())
+    return np.concatenate(out)[:n]
+
+
+@pytest.mark.parametrize("warps", [2, 4, 8])
+@pytest.mark.parametrize("short", [0, 100])
+def test_one_cta_block_system_by_pcr_over_warps(warps, short):
+    n = warps * W * 16 - short
+    rng = np.random.default_rng(warps * 7 + short)
+    a, b, c, d = rand_coeffs(rng, n)
+    expect = oracle.mtsv(a, b, c, d, dims=[n], solvedim=0)
+    x = cta_solve(a, b, c, d, 16, warps)
     assert np.abs(x - expect).max() / np.abs(expect).max() < 1e-13
