@@ -171,7 +171,8 @@ def chunk_backsub(al, ga, de, xF, xL):
 
 def chunks(a, b, c, d, M):
     n, rows = a.size, W * M
-    al, be, ga, de = np.zeros(rows), np.ones(rows), np.zeros(rows), np.zeros(rows)
+    t = np.result_type(a, b, c, d)
+    al, be, ga, de = (np.zeros(rows, t), np.ones(rows, t), np.zeros(rows, t), np.zeros(rows, t))
     al[1:n], be[:n], ga[:n - 1], de[:n] = a[1:], b, c[:-1], d  # a_0, c_{n-1} never read
     return [v.reshape(W, M) for v in (al, be, ga, de)]
 
@@ -362,4 +363,18 @@ def test_one_cta_block_system_by_pcr_over_warps(warps, short):
     a, b, c, d = rand_coeffs(rng, n)
     expect = oracle.mtsv(a, b, c, d, dims=[n], solvedim=0)
     x = cta_solve(a, b, c, d, 16, warps)
+    assert np.abs(x - expect).max() / np.abs(expect).max() < 1e-13
+
+
+@pytest.mark.parametrize("M", [4, 8])
+def test_partitioned_thomas_in_complex_arithmetic(M):
+    """The same equations in complex arithmetic (the complex kernels
+    instantiate partition.cuh for a complex type) against the complex
+    oracle."""
+    from helpers import rand_complex_coeffs
+    n = W * M - 5
+    rng = np.random.default_rng(M + 100)
+    a, b, c, d = rand_complex_coeffs(rng, n)
+    expect = oracle.mtsv(a, b, c, d, dims=[n], solvedim=0)
+    x = partition_solve(a, b, c, d, M)
     assert np.abs(x - expect).max() / np.abs(expect).max() < 1e-13
