@@ -230,9 +230,12 @@ TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchSplitFinish(const float *a, cons
  * array of nsys+1 int64 values and total = offsets[nsys] (the number of
  * rows, passed so that the call needs no device-to-host read).  Each system's
  * first a and last c are never read.  The solution overwrites d.  Systems of
- * up to 8192 rows; one persistent launch (after a one-CTA prefix pass) with
- * length-bucketed work items.  Malformed offsets and longer systems are
- * skipped and reported by tridGetDeviceErrors (bits 4 and 8). */
+ * up to 8192 rows; one persistent launch (after three short preparation
+ * launches) with length-bucketed work items.  Malformed offsets and longer
+ * systems are skipped and reported by tridGetDeviceErrors (bits 4 and 8).
+ * Offsets must increase monotonically: where they do not, valid-looking
+ * systems may overlap, and those whose work items would not fit in the
+ * tables sized for monotone offsets are skipped as malformed (bit 4). */
 TRID_EXTERN_C tridStatus_t tridDmtsvVarlenBatch(const double *a, const double *b, const double *c,
                                                 double *d, const long long *offsets,
                                                 long long nsys, long long total);
@@ -258,9 +261,11 @@ TRID_EXTERN_C tridStatus_t tridSmtsvVarlenBatch(const float *a, const float *b, 
  * first call before any stream capture.  Every call uses the same array and
  * leaves its contents behind (the next call clears what must start at zero),
  * so calls that overlap on the GPU -- concurrent streams or threads on one
- * device -- race and must be serialised by the caller.  Malformed offsets
- * and over-long systems are skipped as in tridDmtsvVarlenBatch but are not
- * reported through tridGetDeviceErrors. */
+ * device -- race and must be serialised by the caller.  Malformed offsets,
+ * over-long systems and finish waits that gave up are skipped as in
+ * tridDmtsvVarlenBatch and recorded in an error word inside the same array,
+ * which tridGetDeviceErrors reads and clears together with the library's
+ * word (bits 1, 4 and 8; that call allocates nothing either). */
 TRID_EXTERN_C tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const double *b,
                                                        const double *c, double *d,
                                                        const long long *offsets, long long nsys,
@@ -346,8 +351,9 @@ TRID_EXTERN_C tridStatus_t tridSetMethod(int method, int chunk, int sys_per_cta)
 /* Error bits recorded on the current device by kernels whose bounded waits
  * gave up (1 = a TMA/mbarrier wait timed out; 2 = a bulk-copy shared-memory
  * operand was misaligned and the copy was skipped; 4 = malformed varlen
- * offsets; 8 = a varlen system longer than supported); reading clears them.  Blocks
- * until the device is idle. */
+ * offsets; 8 = a varlen system longer than supported); reading clears them.
+ * Covers the allocation-free varlen solve's word too.  Allocates nothing;
+ * blocks until the device is idle. */
 TRID_EXTERN_C tridStatus_t tridGetDeviceErrors(unsigned *flags);
 
 /* Load an autotuning table written by tridsolver_b200.autotune (text lines

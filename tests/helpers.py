@@ -45,3 +45,22 @@ def dev(x):
 def host(t):
     torch.cuda.synchronize()
     return t.cpu().numpy()
+
+
+def overlapping_varlen_problem(seed, ngood=600, npairs=400, extra=8192):
+    """A variable-length batch whose offsets stop increasing: ngood ordinary
+    systems packed in rows [0, G), then npairs of systems alternating between
+    [G, G + extra] (valid-looking, every one overlapping the others) and
+    [G + extra, G] (decreasing).  The valid-looking ones would need about
+    npairs * extra / 256 work items, far more than the tables sized for
+    monotone offsets hold, so the solver must skip the ones past its capacity
+    and flag bit 4, while the ngood systems stay solved.  Returns the FP64
+    arrays, the offsets and G."""
+    rng = np.random.default_rng(seed)
+    lens = np.floor(np.exp(rng.uniform(np.log(8), np.log(2048), ngood))).astype(np.int64)
+    good = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    G = int(good[-1])
+    tail = np.array([G + extra if k % 2 == 0 else G for k in range(2 * npairs)], dtype=np.int64)
+    off = np.concatenate([good, tail])
+    a, b, c, d = rand_coeffs(rng, G + extra)
+    return (a, b, c, d), off, G

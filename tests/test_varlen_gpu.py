@@ -15,7 +15,7 @@ import tridsolver_b200 as tb  # noqa: E402
 from tridsolver_b200.varlen import solve_varlen  # noqa: E402
 from oracle import oracle  # noqa: E402
 
-from helpers import rand_coeffs  # noqa: E402
+from helpers import overlapping_varlen_problem, rand_coeffs  # noqa: E402
 
 
 def run(lens, dtype=np.float64, seed=0):
@@ -80,3 +80,26 @@ def test_rejects_and_flags():
     torch.cuda.synchronize()
     tb.lib().tridGetDeviceErrors(ctypes.byref(flags))
     assert flags.value & 4
+
+
+def test_non_monotone_offsets_past_capacity_are_skipped():
+    """Offsets that stop increasing can ask for many more work items than the
+    tables hold; the systems past the capacity are skipped and flagged (bit
+    4), nothing is written out of bounds, and the ordinary systems before
+    them are solved."""
+    flags = ctypes.c_uint()
+    tb.lib().tridGetDeviceErrors(ctypes.byref(flags))  # clear
+    (a, b, c, d), off, G = overlapping_varlen_problem(21)
+    expect = oracle.varlen(a[:G], b[:G], c[:G], d[:G], off[:601])
+    t = [torch.from_numpy(x).cuda() for x in (a, b, c, d)]
+    solve_varlen(*t, torch.from_numpy(off).cuda())
+    got = t[3].cpu().numpy()
+    for s in range(600):
+        o, n = off[s], off[s + 1] - off[s]
+        ref = expect[o:o + n]
+        err = np.abs(got[o:o + n] - ref).max() / max(np.abs(ref).max(), 1e-300)
+        assert err <= 1e-12, (s, n, err)
+    assert np.isfinite(got).all()
+    tb.lib().tridGetDeviceErrors(ctypes.byref(flags))
+    assert flags.value & 4
+    assert not flags.value & 1  # no finish wait gave up

@@ -6,7 +6,10 @@ synchronisation of cudaMalloc/cudaFree); its scratch is a fixed array
 compiled into the library.  Checked through the C ABI against the allocating
 entry point tridDmtsvVarlenBatch on the same inputs, for two calls in a row
 (the second call must not be disturbed by what the first left in the shared
-array), and for the size limit.  This file is named to be collected last.
+array), for the size limit, and for the error word inside the array:
+offsets that stop increasing make it skip systems, which
+tridGetDeviceErrors must report (and then clear).  This file is named to be
+collected last.
 """
 
 import ctypes
@@ -20,6 +23,8 @@ torch = pytest.importorskip("torch")
 
 import tridsolver_b200.varlen  # noqa: E402,F401  (registers the signatures)
 from tridsolver_b200 import lib  # noqa: E402
+
+from helpers import overlapping_varlen_problem  # noqa: E402
 
 TOL = 1e-12  # FP64 relative max-norm, as for every FP64 solve
 
@@ -60,3 +65,23 @@ def test_no_alloc_rejects_problems_beyond_its_fixed_scratch():
     # 10 M systems need far more than the 32 MiB the array holds
     st = _call("tridDmtsvVarlenBatchNoAlloc", a, a, a, a, off, 10_000_000, 8)
     assert st == 3  # TRID_STATUS_INVALID_VALUE
+
+
+def test_no_alloc_reports_skipped_systems():
+    L = lib()
+    flags = ctypes.c_uint()
+    assert L.tridGetDeviceErrors(ctypes.byref(flags)) == 0  # clear both words
+    (a, b, c, d), off, G = overlapping_varlen_problem(22, ngood=300, npairs=200)
+    a, b, c, d = [torch.from_numpy(x).cuda() for x in (a, b, c, d)]
+    off_t = torch.from_numpy(off).cuda()
+    nsys, total = off.size - 1, d.numel()
+    d_ref, d_new = d.clone(), d.clone()
+    assert _call("tridDmtsvVarlenBatch", a, b, c, d_ref, off_t, nsys, total) == 0
+    assert L.tridGetDeviceErrors(ctypes.byref(flags)) == 0 and flags.value & 4
+    assert _call("tridDmtsvVarlenBatchNoAlloc", a, b, c, d_new, off_t, nsys, total) == 0
+    assert L.tridGetDeviceErrors(ctypes.byref(flags)) == 0
+    assert flags.value & 4, flags.value  # recorded in the static array's word
+    assert L.tridGetDeviceErrors(ctypes.byref(flags)) == 0 and flags.value == 0  # cleared
+    # the ordinary systems (rows [0, G)) match the allocating entry point
+    err = float((d_new[:G] - d_ref[:G]).abs().max() / d_ref[:G].abs().max())
+    assert err <= TOL, err

@@ -73,6 +73,13 @@ unsigned *device_error_flags() {
   return g_err[dev];
 }
 
+unsigned *device_error_flags_if_present() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  return (int)g_err.size() > dev ? g_err[dev] : nullptr;
+}
+
 struct TuneEntry {
   int dtype_bytes, axis, nmax, method, chunk, spc;
 };
@@ -675,13 +682,23 @@ extern "C" tridStatus_t tridSetMethod(int method, int chunk, int sys_per_cta) {
   return TRID_STATUS_SUCCESS;
 }
 
+// Reads and clears both error words of the current device: the library's
+// (made by the first kernel that needs it) and the allocation-free varlen
+// solve's (inside its static array).  Allocates nothing: a word that does not
+// exist yet has recorded nothing.
 extern "C" tridStatus_t tridGetDeviceErrors(unsigned *flags) {
   if (!flags) return TRID_STATUS_INVALID_VALUE;
-  unsigned *p = device_error_flags();
-  if (!p) return TRID_STATUS_ALLOC_FAILED;
-  if (cudaMemcpy(flags, p, sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess ||
-      cudaMemset(p, 0, sizeof(unsigned)) != cudaSuccess)
-    return TRID_STATUS_EXECUTION_FAILED;
+  unsigned acc = 0;
+  unsigned *words[2] = {device_error_flags_if_present(), noalloc_error_word()};
+  for (unsigned *p : words) {
+    if (!p) continue;
+    unsigned v = 0;
+    if (cudaMemcpy(&v, p, sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemset(p, 0, sizeof(unsigned)) != cudaSuccess)
+      return TRID_STATUS_EXECUTION_FAILED;
+    acc |= v;
+  }
+  *flags = acc;
   return TRID_STATUS_SUCCESS;
 }
 

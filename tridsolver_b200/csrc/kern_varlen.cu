@@ -32,6 +32,12 @@
 // per-system counters.
 // Malformed offsets (decreasing or past `total`) and systems longer than
 // 8192 rows are skipped and recorded in the device error word (bits 4 and 8).
+// The item tables hold `cap` = nsys + total/256 + 1 entries, which bounds the
+// items of any offsets that increase monotonically.  Offsets that do not
+// (e.g. 0, T, 0, T, ...: every other system valid and T rows long) can ask
+// for more; a system whose items would end past `cap` is skipped whole
+// (its table entries read -1) and recorded as malformed (bit 4), so no table,
+// block-row or queue access ever leaves the scratch.
 #include <mutex>
 
 #include "partition.cuh"
@@ -74,14 +80,19 @@ __device__ __forceinline__ int64_t vl_fitems(int64_t len) {
 //          the item tables item_sys/fitem_sys for each of its items.
 constexpr int kPrepThreads = 256;
 
+// Items of system s, each count clamped to cap + 1 so that the prefix sums
+// stay far from int64 overflow whatever the offsets hold (a system with more
+// than cap items is skipped by the fill anyway).
 __device__ __forceinline__ void vl_counts(const int64_t *offsets, int64_t nsys, int64_t total,
-                                          int64_t s, int64_t &ni, int64_t &nf) {
+                                          int64_t cap, int64_t s, int64_t &ni, int64_t &nf) {
   ni = nf = 0;
   if (s >= nsys) return;
   int64_t len = offsets[s + 1] - offsets[s];
   if (vl_bad(offsets[s], offsets[s + 1], total)) len = 0;
   ni = vl_items(len > 0 ? len : 1);
   nf = vl_fitems(len);
+  if (ni > cap + 1) ni = cap + 1;
+  if (nf > cap + 1) nf = cap + 1;
 }
 
 // inclusive sum over the CTA of v (blockDim.x == kPrepThreads); returns it
@@ -102,11 +113,12 @@ __device__ __forceinline__ int64_t vl_cta_scan(int64_t v, int64_t *warp_tot) {
 
 __global__ void __launch_bounds__(kPrepThreads) varlen_prep_count(const int64_t *__restrict__ offsets,
                                                                   int64_t nsys, int64_t total,
+                                                                  int64_t cap,
                                                                   int64_t *__restrict__ bsum) {
   __shared__ int64_t wt[kPrepThreads / 32];
   const int64_t s = (int64_t)blockIdx.x * kPrepThreads + threadIdx.x;
   int64_t ni, nf;
-  vl_counts(offsets, nsys, total, s, ni, nf);
+  vl_counts(offsets, nsys, total, cap, s, ni, nf);
   const int64_t ci = vl_cta_scan(ni, wt);
   const int64_t cf = vl_cta_scan(nf, wt);
   if (threadIdx.x == kPrepThreads - 1) {
@@ -157,36 +169,49 @@ __global__ void __launch_bounds__(1024) varlen_prep_scan(int64_t *__restrict__ b
 }
 
 __global__ void __launch_bounds__(kPrepThreads) varlen_prep_fill(
-    const int64_t *__restrict__ offsets, int64_t nsys, int64_t total,
+    const int64_t *__restrict__ offsets, int64_t nsys, int64_t total, int64_t cap,
     const int64_t *__restrict__ bsum, int64_t *__restrict__ item_off,
     int64_t *__restrict__ fitem_off, int *__restrict__ item_sys, int *__restrict__ fitem_sys,
-    unsigned *__restrict__ sys_count) {
+    unsigned *__restrict__ sys_count, unsigned *__restrict__ err) {
   __shared__ int64_t wt[kPrepThreads / 32];
   const int64_t s = (int64_t)blockIdx.x * kPrepThreads + threadIdx.x;
   int64_t ni, nf;
-  vl_counts(offsets, nsys, total, s, ni, nf);
+  vl_counts(offsets, nsys, total, cap, s, ni, nf);
   const int64_t ri = bsum[2 * blockIdx.x] + vl_cta_scan(ni, wt) - ni;
   const int64_t rf = bsum[2 * blockIdx.x + 1] + vl_cta_scan(nf, wt) - nf;
   if (s >= nsys) return;
   item_off[s] = ri;
   fitem_off[s] = rf;
   sys_count[s] = 0u;
-  for (int64_t k = 0; k < ni; ++k) item_sys[ri + k] = (int)s;
-  for (int64_t k = 0; k < nf; ++k) fitem_sys[rf + k] = (int)s;
+  // A system whose items end past the tables' capacity (only non-monotone
+  // offsets get there) is skipped whole: its entries below cap read -1.
+  const bool fits = ri + ni <= cap && rf + nf <= cap;
+  if (!fits) atomicOr(err, kErrBadOffsets);
+  const int tag = fits ? (int)s : -1;
+  for (int64_t k = ri; k < ri + ni && k < cap; ++k) item_sys[k] = tag;
+  for (int64_t k = rf; k < rf + nf && k < cap; ++k) fitem_sys[k] = tag;
 }
 
-// the three preparation launches; bsum holds 2*ceil(nsys/256) int64
+// Capacity of the item tables: enough for any monotone offsets
+// (sum over systems of max(1, ceil(len/256)) <= nsys + total/256).
+static inline int64_t varlen_cap(int64_t nsys, int64_t total) {
+  return nsys + total / kVLBlock + 1;
+}
+
+// the three preparation launches; bsum holds 2*ceil(nsys/256) int64, the
+// item tables cap = varlen_cap(nsys, total) entries each
 static cudaError_t launch_varlen_prep(const int64_t *offsets, int64_t nsys, int64_t total,
                                       int64_t *bsum, int64_t *item_off, int64_t *fitem_off,
                                       int *item_sys, int *fitem_sys, unsigned *sys_count,
-                                      unsigned long long *queue, cudaStream_t st) {
+                                      unsigned long long *queue, unsigned *err, cudaStream_t st) {
   const int64_t nb = (nsys + kPrepThreads - 1) / kPrepThreads;
   if (nb > 0x7fffffff) return cudaErrorInvalidValue;
-  varlen_prep_count<<<(unsigned)nb, kPrepThreads, 0, st>>>(offsets, nsys, total, bsum);
+  const int64_t cap = varlen_cap(nsys, total);
+  varlen_prep_count<<<(unsigned)nb, kPrepThreads, 0, st>>>(offsets, nsys, total, cap, bsum);
   varlen_prep_scan<<<1, 1024, 0, st>>>(bsum, nb, nsys, item_off, fitem_off, queue);
-  varlen_prep_fill<<<(unsigned)nb, kPrepThreads, 0, st>>>(offsets, nsys, total, bsum, item_off,
-                                                          fitem_off, item_sys, fitem_sys,
-                                                          sys_count);
+  varlen_prep_fill<<<(unsigned)nb, kPrepThreads, 0, st>>>(offsets, nsys, total, cap, bsum,
+                                                          item_off, fitem_off, item_sys,
+                                                          fitem_sys, sys_count, err);
   return cudaGetLastError();
 }
 
@@ -197,10 +222,11 @@ struct VLArgs {
   const int64_t *offsets;
   const int64_t *item_off;   // reduce-queue prefix, nsys+1
   const int64_t *fitem_off;  // finish-queue prefix, nsys+1
-  const int *item_sys;       // system of every reduce item
-  const int *fitem_sys;      // system of every finish item
+  const int *item_sys;       // system of every reduce item (-1: skipped)
+  const int *fitem_sys;      // system of every finish item (-1: skipped)
   int64_t nsys;
   int64_t total;
+  int64_t cap;               // entries of item_sys / fitem_sys / block rows
   unsigned *sys_count;
   unsigned long long *queue;  // [0] reduce queue, [1] finish queue
   T *rows;       // per reduce item: the block's 8 row values; later its 2 unknowns
@@ -334,8 +360,10 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
   extern __shared__ __align__(16) unsigned char vl_dyn[];
   const int lane = threadIdx.x & (kWarp - 1);
   T *reg = reinterpret_cast<T *>(vl_dyn) + (size_t)(threadIdx.x / kWarp) * 4 * kVLRegion;
-  const int64_t nitems = A.item_off[A.nsys];
-  const int64_t nf = A.fitem_off[A.nsys];
+  // the prefixes can pass cap only for non-monotone offsets; the systems past
+  // it were skipped by the preparation
+  const int64_t nitems = A.item_off[A.nsys] < A.cap ? A.item_off[A.nsys] : A.cap;
+  const int64_t nf = A.fitem_off[A.nsys] < A.cap ? A.fitem_off[A.nsys] : A.cap;
   // Both queues are software-pipelined: lane 0 claims the next item one
   // iteration ahead and, while the current item's rows are in flight, looks
   // up the next item's rows and warms L2 with them.
@@ -343,6 +371,7 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
                   const int64_t *toff, bool long_only) {
     if (lane != 0 || (int64_t)nx >= nlimit) return;
     const int64_t s2 = tsys[nx];
+    if (s2 < 0) return;
     const int64_t lo2 = A.offsets[s2], hi2 = A.offsets[s2 + 1];
     if (vl_bad(lo2, hi2, A.total) || hi2 == lo2) return;
     int64_t first = lo2, cnt = hi2 - lo2;
@@ -361,6 +390,7 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
     if (lane == 0) nit = atomicAdd(&A.queue[0], 1ull);
     auto between = [&]() { warm(nit, nitems, A.item_sys, A.item_off, false); };
     const int64_t s = A.item_sys[it];
+    if (s < 0) continue;  // skipped by the preparation (past cap)
     const int64_t lo = A.offsets[s], hi = A.offsets[s + 1];
     const int64_t len = hi - lo;
     if (vl_bad(lo, hi, A.total)) {
@@ -427,6 +457,7 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
     if ((int64_t)fi >= nf) break;
     if (lane == 0) nfi = atomicAdd(&A.queue[1], 1ull);
     const int64_t s = A.fitem_sys[fi];
+    if (s < 0) continue;  // skipped by the preparation (past cap)
     // the system's reduce items were all taken by running warps: its mark
     // comes; poll a bounded number of times
     int ok = 0;
@@ -494,7 +525,7 @@ cudaError_t launch_varlen(const T *a, const T *b, const T *c, T *d, const int64_
                           int64_t nsys, int64_t total, unsigned *err, cudaStream_t st) {
   // scratch: item_off and fitem_off (nsys+1 each), sys_count, queues, block
   // rows (8 per item), item_sys and fitem_sys (one int per item each)
-  const int64_t max_items = nsys + total / kVLBlock + 1;
+  const int64_t max_items = varlen_cap(nsys, total);
   const size_t b_off = sizeof(int64_t) * (size_t)(nsys + 1);
   const size_t b_cnt = sizeof(unsigned) * (size_t)(nsys + 1);
   const size_t b_q = 64;
@@ -514,6 +545,7 @@ cudaError_t launch_varlen(const T *a, const T *b, const T *c, T *d, const int64_
   A.offsets = offsets;
   A.nsys = nsys;
   A.total = total;
+  A.cap = max_items;
   A.item_off = (int64_t *)w;
   A.fitem_off = (int64_t *)(w + al(b_off));
   A.sys_count = (unsigned *)(w + 2 * al(b_off));
@@ -527,7 +559,7 @@ cudaError_t launch_varlen(const T *a, const T *b, const T *c, T *d, const int64_
   if (e != cudaSuccess) return e;
   e = launch_varlen_prep(offsets, nsys, total, bsum, (int64_t *)A.item_off,
                          (int64_t *)A.fitem_off, (int *)A.item_sys, (int *)A.fitem_sys,
-                         A.sys_count, A.queue, st);
+                         A.sys_count, A.queue, err, st);
   if (e != cudaSuccess) return e;
   varlen_kernel<T><<<dim3((unsigned)grid), dim3(kVLWarps * 32), varlen_smem_bytes<T>(), st>>>(A);
   return cudaGetLastError();
@@ -608,13 +640,24 @@ static void *noalloc_scratch_address() {
   return g_noalloc_ptr[dev];
 }
 
+// The allocation-free solve's error word (the first bytes of the static
+// array) on the current device, or nullptr when no allocation-free solve has
+// run there yet (the word is then still zero).  Read and cleared by
+// tridGetDeviceErrors.
+unsigned *noalloc_error_word() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  return (unsigned *)g_noalloc_ptr[dev];
+}
+
 // Bytes of work space a solve of nsys systems / total rows needs (0 when it
 // does not fit in the static array).
 static size_t noalloc_layout(int64_t nsys, int64_t total, size_t off[5]) {
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-  const int64_t max_items = nsys + total / kVLBlock + 1;
+  const int64_t max_items = varlen_cap(nsys, total);
   size_t at = 0;
-  off[0] = at;  // error word
+  off[0] = at;  // error word (read and cleared by tridGetDeviceErrors)
   at += 256;
   off[1] = at;  // item_off and fitem_off, nsys+1 int64 each
   at += 2 * al(sizeof(int64_t) * (size_t)(nsys + 1));
@@ -653,6 +696,7 @@ extern "C" tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const doubl
   A.offsets = (const int64_t *)offsets;
   A.nsys = nsys;
   A.total = total;
+  A.cap = varlen_cap(nsys, total);
   A.err = (unsigned *)(w + off[0]);
   A.item_off = (int64_t *)(w + off[1]);
   A.fitem_off = (int64_t *)(w + off[1] + (off[2] - off[1]) / 2);
@@ -662,7 +706,7 @@ extern "C" tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const doubl
   int64_t *bsum = nullptr;
   {
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const int64_t max_items = nsys + total / kVLBlock + 1;
+    const int64_t max_items = A.cap;
     A.item_sys = (const int *)(w + off[4] + al(sizeof(double) * 8 * (size_t)max_items));
     A.fitem_sys = A.item_sys + al(sizeof(int) * (size_t)max_items) / sizeof(int);
     bsum = (int64_t *)(w + off[4] + al(sizeof(double) * 8 * (size_t)max_items) +
@@ -674,7 +718,7 @@ extern "C" tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const doubl
   if (varlen_grid<double>(grid) != cudaSuccess) return TRID_STATUS_EXECUTION_FAILED;
   if (launch_varlen_prep(A.offsets, nsys, total, bsum, (int64_t *)A.item_off,
                          (int64_t *)A.fitem_off, (int *)A.item_sys, (int *)A.fitem_sys,
-                         A.sys_count, A.queue, st) != cudaSuccess)
+                         A.sys_count, A.queue, A.err, st) != cudaSuccess)
     return TRID_STATUS_EXECUTION_FAILED;
   varlen_kernel<double><<<dim3((unsigned)grid), dim3(kVLWarps * 32), varlen_smem_bytes<double>(),
                           st>>>(A);

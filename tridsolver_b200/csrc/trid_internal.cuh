@@ -121,6 +121,12 @@ void *scratch(size_t bytes, int level = 0);
 // Per-device word of error bits set by kernels whose bounded waits gave up
 // (read and cleared by tridGetDeviceErrors).  nullptr if it cannot be made.
 unsigned *device_error_flags();
+// The same word when it exists already on the current device (nullptr if no
+// kernel has needed it yet); never allocates.
+unsigned *device_error_flags_if_present();
+// The allocation-free varlen solve's own error word on the current device
+// (kern_varlen.cu), nullptr until that entry point has run there.
+unsigned *noalloc_error_word();
 
 // Kernel launchers (return cudaSuccess or the launch error).
 template <typename T, int INC>
