@@ -169,7 +169,7 @@ TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchAdjoint(const float *a, const fl
  * x = A^{-1} d and, for the cotangent w = dL/dx, the gradients of the
  * adjoint above at that x (dd = A^{-T} w, da, db, dc), in one call.  For
  * solvedim 0 and n <= 4096 one kernel does both (every input read once,
- * methods 5/6 below); otherwise the forward solve and the adjoint run one
+ * method 6 below); otherwise the forward solve and the adjoint run one
  * after the other.  x
  * may alias d and dd may alias w; no other output may alias an input. */
 TRID_EXTERN_C tridStatus_t tridDmtsvStridedBatchFwdAdj(const double *a, const double *b,
@@ -328,19 +328,13 @@ TRID_EXTERN_C const char *tridGetStatusString(tridStatus_t status);
  *              one persistent CTA per SM, the next tile's copy in flight
  *              while the current one is solved
  *   method 3 = method 2 with plain loads only
- *   method 4 = strided axes: two-sided (twisted) Thomas, rows staged by TMA,
- *              c'/d' in shared memory (falls back to method 2 where the
- *              layout or length does not allow it; axis 0 uses method 2)
- *   method 5 = axis 0: one warp per system, the system staged in shared
- *              memory and cut into 32 chunks of ceil(n/32) rows (from 65
- *              rows up to what 227 KB of shared memory holds: in FP64 about
- *              7200 rows forward, 5700 adjoint, 4100 forward + adjoint)
+ *   methods 4 and 5 are not used (INVALID_VALUE)
  *   method 6 = axis 0: one CTA per system, one block of 32*chunk rows per
  *              warp (chunk 4, 8 or 16; up to 4096 rows)
- *              (methods 5/6 act as method 3 on the other axes and where their
- *              limits exclude the system; by default axis-0 systems of
- *              513..4096 rows take method 6 with chunk 16, as do the adjoint
- *              and the forward + adjoint call from 65 rows)
+ *              (method 6 acts as method 3 on the other axes and past 4096
+ *              rows; by default axis-0 systems of 513..4096 rows take
+ *              method 6 with chunk 16, as do the adjoint and the forward +
+ *              adjoint call from 65 rows)
  *   chunk      : rows per thread for methods 2/3 (2, 4, 8 or 16; 0 = automatic)
  *   sys_per_cta: systems per CTA for methods 2/3 on strided axes (4, 8, 16 or
  *                32; 0 = auto; 32 applies to the FP32 streamed tiles, and

@@ -4,7 +4,7 @@ The reference's file-driven Catch2 tests (scalar/test/test_cpu.cpp:88-110,
 scalar/test/test_cuda.cu:58-82) load text fixtures written by
 scalar/test/gen_testcases.py:95-109.  Those files are not shipped with the
 reference, so this script imports that generator from a checkout of the
-reference (``--reference``, default ``/root/reference``), runs its ``main()``
+reference (``--reference``, default ``$TRID_REFERENCE_DIR``), runs its ``main()``
 exactly as shipped (numpy seed 1, same call order, so every fixture draws the
 same random stream as the original), parses the text files the generator
 wrote (column-major, values rounded to 15 / 6 decimals exactly as the
@@ -81,8 +81,11 @@ def crop(dims, solvedim, keep, arrays):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("TRID_REFERENCE_DIR"),
+                    help="reference checkout (default: $TRID_REFERENCE_DIR)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("name the reference checkout with --reference or TRID_REFERENCE_DIR")
     gen_path = os.path.join(args.reference, "scalar", "test", "gen_testcases.py")
     spec = importlib.util.spec_from_file_location("ref_gen_testcases", gen_path)
     mod = importlib.util.module_from_spec(spec)

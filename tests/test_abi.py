@@ -216,10 +216,13 @@ def test_method_override_and_query():
     tb.set_method(1)
     assert L.tridQueryMethod(8, 0, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
     assert m.value == 1
-    tb.set_method(5)
+    tb.set_method(6)
     assert L.tridQueryMethod(8, 0, 1024, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
-    assert m.value == 5
+    assert m.value == 6
     tb.set_method(0)
+    for removed in (4, 5):  # methods that no longer exist
+        with pytest.raises(tb.TridError):
+            tb.set_method(removed)
     with pytest.raises(tb.TridError):
         tb.set_method(2, chunk=3)
     with pytest.raises(tb.TridError):

@@ -59,7 +59,7 @@ def test_fused_one_kernel(n, dtype):
     run_fused(dtype, [n, 7], 0, seed=n)
 
 
-@pytest.mark.parametrize("method", [(5, 0), (6, 4), (6, 8), (6, 16)])
+@pytest.mark.parametrize("method", [(6, 4), (6, 8), (6, 16)])
 @pytest.mark.parametrize("n", [65, 66, 100, 257, 511, 1000, 1024, 1025, 2500, 4096])
 def test_fused_forced_kernel(method, n):
     tb.set_method(*method)
@@ -135,18 +135,18 @@ def test_one_kernel_adjoint(n):
     run_adjoint(np.float32, [n, 6], 0, seed=n + 3)
 
 
-@pytest.mark.parametrize("method", [5, 6])
+@pytest.mark.parametrize("method", [6])
 @pytest.mark.parametrize("n", [65, 97, 300, 1024, 1031, 3000, 5000, 7000])
 @pytest.mark.parametrize("inc", [False, True])
 def test_forced_kernel_forward(method, n, inc):
-    """Methods 5/6 forced: where their limits exclude the system (6 past
-    4096 rows) the call still returns the solution through another kernel."""
+    """Method 6 forced: where its limit excludes the system (past 4096
+    rows) the call still returns the solution through another kernel."""
     from test_scalar_gpu import run_case
     run_case(np.random.default_rng(n + method), np.float64, [n, 4], 0, inc=inc,
              method=(method, 0, 0))
 
 
-@pytest.mark.parametrize("method", [(5, 0), (6, 4), (6, 16)])
+@pytest.mark.parametrize("method", [(6, 4), (6, 16)])
 @pytest.mark.parametrize("n", [65, 300, 1024, 1031, 5000])
 def test_forced_kernel_adjoint(method, n):
     from test_adjoint_gpu import run_adjoint

@@ -154,21 +154,6 @@ def test_forced_methods(method, solvedim):
 
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
-@pytest.mark.parametrize("dims,solvedim,pads", [
-    ([64, 256, 3], 1, None),          # TMA two-sided Thomas, full tiles
-    ([40, 33, 5], 1, [44, 33, 5]),    # partial x tile, odd n, padded
-    ([48, 6, 7], 2, None),            # n=7 < stage rows: falls back
-    ([32, 5, 300], 2, None),          # odd n, z
-    ([16, 1, 2], 2, None),            # n = 2
-    ([16, 4, 4, 9, 2], 3, None),      # rank 5
-])
-@pytest.mark.parametrize("inc", [False, True])
-def test_method4_twisted_thomas(dtype, dims, solvedim, pads, inc):
-    run_case(np.random.default_rng(sum(dims)), dtype, dims, solvedim, pads=pads, inc=inc,
-             method=(4, 0, 0))
-
-
-@pytest.mark.parametrize("dtype", [np.float64, np.float32])
 @pytest.mark.parametrize("n", [16, 48, 64, 200, 256, 512])
 @pytest.mark.parametrize("inc", [False, True])
 def test_x_tma_staged(dtype, n, inc):

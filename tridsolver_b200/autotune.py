@@ -16,9 +16,6 @@ Candidates (see tridSetMethod in include/trid_b200.h):
                         axes, 4/8/16 systems per CTA (and 32 for method 2;
                         128 bytes of systems, 16 FP64 / 32 FP32, is the
                         streamed persistent kernel)
-    method 4            strided axes: two-sided Thomas with a TMA stage ring
-    method 5            axis 0, longer systems: one warp per system, staged in
-                        shared memory
     method 6, chunk     axis 0, longer systems: one CTA per system, 4/8/16
                         rows per thread (up to 4096 rows)
     (method 2 above 512 rows on axis 0 also means the blocked partition:
@@ -72,10 +69,7 @@ def candidates(axis, n):
                     out.append((2, ch, spc))
                     out.append((3, ch, spc))
                 out.append((2, ch, 32))
-    if axis > 0:
-        out.append((4, 0, 0))
-    elif n > 64:
-        out.append((5, 0, 0))
+    if axis == 0 and n > 64:
         if n <= 4096:
             for ch in (4, 8, 16):
                 out.append((6, ch, 0))

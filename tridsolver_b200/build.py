@@ -27,14 +27,14 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                      "-I", os.path.join(ROOT, "include")]
 
 # sources shared by both libraries
-COMMON = ["kern_scalar.cu", "kern_xtma.cu", "kern_stma.cu", "kern_sptma.cu", "kern_general.cu", "kern_block.cu", "kern_varlen.cu", "kern_adi.cu", "kern_xcta.cu", "kern_xwarp.cu", "kern_split.cu", "tma_host.cu"]
-EXTRA = []  # filled as components are added (block, adjoint, varlen, adi)
+COMMON = ["kern_scalar.cu", "kern_xtma.cu", "kern_sptma.cu", "kern_general.cu", "kern_block.cu",
+          "kern_varlen.cu", "kern_adi.cu", "kern_xcta.cu", "kern_split.cu", "tma_host.cu"]
 MAIN = ["api_scalar.cu", "kern_ext.cu"]
 COMPAT = [("api_scalar.cu", ["-DTRID_CUDACOMPAT"]), ("api_compat.cu", [])]
 
 LIBS = {
-    "libtridb200.so": [(s, []) for s in COMMON + EXTRA + MAIN],
-    "libtridb200_cudacompat.so": [(s, []) for s in COMMON + EXTRA] + COMPAT,
+    "libtridb200.so": [(s, []) for s in COMMON + MAIN],
+    "libtridb200_cudacompat.so": [(s, []) for s in COMMON] + COMPAT,
 }
 
 
@@ -77,12 +77,19 @@ def build(verbose=False):
     for lib, objs in LIBS.items():
         out = os.path.join(HERE, lib)
         obj_paths = [_obj_name(s, d) for s, d in objs]
-        if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(o) for o in obj_paths):
+        # the object list of the last link: a changed list relinks too
+        stamp = os.path.join(BUILD, lib + ".objs")
+        listed = "\n".join(obj_paths)
+        same = os.path.exists(stamp) and open(stamp).read() == listed
+        if same and os.path.exists(out) and \
+                os.path.getmtime(out) >= max(os.path.getmtime(o) for o in obj_paths):
             continue
         cmd = [nvcc()] + ARCH + ["-shared", "-o", out] + obj_paths
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed for {lib}:\n{r.stdout}\n{r.stderr}")
+        with open(stamp, "w") as f:
+            f.write(listed)
     return [os.path.join(HERE, lib) for lib in LIBS]
 
 

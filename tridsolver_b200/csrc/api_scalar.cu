@@ -102,7 +102,8 @@ static tridStatus_t parse_tuning_table(const char *path, std::vector<TuneEntry> 
     e.dtype_bytes = (strcmp(dt, "f64") == 0) ? 8 : (strcmp(dt, "f32") == 0 ? 4 : 0);
     const bool chunk_ok = e.chunk == 0 || e.chunk == 2 || e.chunk == 4 || e.chunk == 8 || e.chunk == 16;
     const bool spc_ok = e.spc == 0 || e.spc == 4 || e.spc == 8 || e.spc == 16 || e.spc == 32;
-    if (e.dtype_bytes == 0 || e.method < 1 || e.method > 6 || e.axis < 0 || e.axis > 3 ||
+    if (e.dtype_bytes == 0 || e.method < 1 || e.method > 6 || e.method == 4 || e.method == 5 ||
+        e.axis < 0 || e.axis > 3 ||
         !chunk_ok || !spc_ok) {
       fclose(f);
       return TRID_STATUS_INVALID_VALUE;
@@ -285,16 +286,11 @@ static int axis_class(const Geom &g, int solvedim, int elem_bytes) {
   return bytes <= 65536 ? 1 : (bytes <= (1 << 20) ? 2 : 3);
 }
 
-// Axis-0 systems solved whole by one warp (method 5) or one CTA (method 6,
-// and the default up to 4096 rows) each.  cudaErrorNotSupported when neither
-// applies.
+// Axis-0 systems solved whole by one CTA each (method 6, and the default up
+// to 4096 rows).  cudaErrorNotSupported when it does not apply.
 template <typename T, int MODE>
 static cudaError_t launch_x_whole(const Geom &g, const XArgs<T> &A, const MethodChoice &m,
                                   cudaStream_t st) {
-  if (m.method == 5) {
-    const cudaError_t e = launch_xwarp<T, MODE>(g, A, st);
-    if (e != cudaErrorNotSupported) return e;
-  }
   if (g.n <= 4096) return launch_xcta<T, MODE>(g, A, m.method == 6 ? m.chunk : 0, st);
   return cudaErrorNotSupported;
 }
@@ -319,19 +315,12 @@ static tridStatus_t solve_level(const T *a, const T *b, const T *c, T *d, T *u, 
   const MethodChoice m = choose_method((int)sizeof(T), axis, g.n, opt);
   const bool fits = g.n <= 32 * m.chunk;
   cudaError_t e = cudaErrorNotSupported;
-  if (m.method == 4 && axis >= 1) {
-    unsigned *err = device_error_flags();
-    if (!err) return TRID_STATUS_ALLOC_FAILED;
-    e = launch_strided_tma<T, INC>(g, dims, pads, ndim, solvedim, a, b, c, d, u, err, stream);
-  }
-  if (e != cudaErrorNotSupported) {
-    // done (or failed) by the method-4 kernel
-  } else if (m.method >= 2 && axis == 0 && (!fits || m.method >= 5) &&
+  if (m.method >= 2 && axis == 0 && (!fits || m.method == 6) &&
              (e = launch_x_whole<T, INC ? kXcFwdInc : kXcFwd>(
                   g, XArgs<T>{a, b, c, d, nullptr, nullptr, INC ? u : d, nullptr, nullptr, nullptr,
                               nullptr},
                   m, stream)) != cudaErrorNotSupported) {
-    // one warp or one CTA per system: done (or failed) above
+    // one CTA per system: done (or failed) above
   } else if (m.method >= 2 && !fits) {
     GenArgs<T> A = {};
     A.a = a;
@@ -405,7 +394,7 @@ tridStatus_t solve_adjoint(const T *a, const T *b, const T *c, const T *u, const
   MethodChoice m = choose_method((int)sizeof(T), axis, g.n, 0);
   if (m.chunk == 0) m.chunk = 8;
   if (m.spc == 0) m.spc = 8;
-  if (axis == 0 && (g.n > 64 || m.method >= 5)) {
+  if (axis == 0 && (g.n > 64 || m.method == 6)) {
     const cudaError_t e = launch_x_whole<T, kXcAdj>(
         g, XArgs<T>{a, b, c, nullptr, w, u, nullptr, ga, gb, gc, gd}, m, stream);
     if (e != cudaErrorNotSupported)
@@ -672,7 +661,7 @@ extern "C" const char *tridGetStatusString(tridStatus_t s) {
 }
 
 extern "C" tridStatus_t tridSetMethod(int method, int chunk, int sys_per_cta) {
-  if (method < 0 || method > 6) return TRID_STATUS_INVALID_VALUE;
+  if (method < 0 || method > 6 || method == 4 || method == 5) return TRID_STATUS_INVALID_VALUE;
   if (chunk != 0 && chunk != 2 && chunk != 4 && chunk != 8 && chunk != 16)
     return TRID_STATUS_INVALID_VALUE;
   if (sys_per_cta != 0 && sys_per_cta != 4 && sys_per_cta != 8 && sys_per_cta != 16 &&

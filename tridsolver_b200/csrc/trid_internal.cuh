@@ -140,10 +140,6 @@ cudaError_t launch_xsolve_tma(const Geom &g, const int *const pads[5], int ndim,
                               const T *b, const T *c, T *d, T *u, int chunk, unsigned *err,
                               cudaStream_t st);
 template <typename T, int INC>
-cudaError_t launch_strided_tma(const Geom &g, const int *dims, const int *const pads[5],
-                               int ndim, int solvedim, const T *a, const T *b, const T *c, T *d,
-                               T *u, unsigned *err, cudaStream_t st);
-template <typename T, int INC>
 cudaError_t launch_strided_part_tma(const Geom &g, const int *dims, const int *const pads[5],
                                     int ndim, int solvedim, const T *a, const T *b, const T *c,
                                     T *d, T *u, int chunk, int spc, bool prefetch,
@@ -178,10 +174,6 @@ struct XArgs {
 };
 template <typename T, int MODE>
 cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, int chunk, cudaStream_t st);
-// one-warp-per-system partition in shared memory on axis 0 (kern_xwarp.cu)
-template <typename T, int MODE>
-cudaError_t launch_xwarp(const Geom &g, const XArgs<T> &A, cudaStream_t st);
-
 template <typename T, int INC>
 cudaError_t launch_generic(const Geom &g, const T *a, const T *b, const T *c, T *d, T *u,
                            T *work, int64_t work_systems, cudaStream_t st);
