@@ -5,29 +5,42 @@
 One step = three solves of the 256^3 FP64 cube (65,536 systems of n=256),
 along solvedim 0, 1 and 2 in turn (tridDmtsvStridedBatch through the C ABI),
 on inputs resident in HBM.  Inputs: a_i, c_i ~ U(-1,1), b_i = |a_i|+|c_i|+U(1,2),
-d ~ N(0,1), seeded (synthetic stand-in for the workload's distribution).
+d ~ N(0,1), a_0 = c_{n-1} = 0 along every axis, seeded (synthetic stand-in
+for the workload's distribution).
 
 Metric: solve GB/s = algorithmic bytes (read a,b,c,d + write x = 40 B per
 unknown) / time, whole job (all ranks).  Each array is 134 MB, so every launch
 streams 671 MB (> 126 MB L2): no L2 flush is needed between steps.
 
-Extra keys: roofline (dominant kernel vs the measured HBM copy bandwidth),
-cpu_baseline (the reference CPU solver compiled from the reference sources,
-all host threads, on the same cube), e2e (the same solves through the C ABI
-from pinned host buffers, host<->device copies inside the timed region),
-clocks (nvidia-smi samples during the timed region), gpu_launches,
-differentiation (16,384 x 1024 FP64: forward, forward + adjoint in one call
-and autograd forward + backward, times and their ratio to the forward solve,
-gradient error against central finite differences; rank 0 at N=1).
+Extra keys (rank 0, one GPU):
+  roofline      the dominant kernel vs the measured HBM copy bandwidth
+  e2e           the same solves through the C ABI from pinned host buffers,
+                host<->device copies inside the timed region
+  clocks        nvidia-smi samples during the timed region
+  differentiation  16,384 x 1024 FP64: forward, forward + adjoint in one call
+                and autograd forward + backward, times and their ratio to the
+                forward solve, gradient error against central differences
+  workloads     the other configurations of the path, each timed with CUDA
+                events and checked on sampled systems against the oracle:
+                FP32 cube per axis, 2,048 x 65,536 long systems, the
+                200,000-system variable-length batch, block M = 2/4/8
+                forward and adjoint, ADI 64^3 x 10 and 128^3 x 100 (CUDA
+                graph), the checkpointed 200-step ADI gradient
+  reference_gpu the reference's own GPU library (scalar/src/cuda/trid_cuda.cu
+                built for sm_100a into oracle/_ref) on the same cube, per
+                axis and algorithm option, next to ours
+  cpu_baseline  the reference's CPU solver (oracle/_ref) on the same cube:
+                best of 5 steps on the physical cores (OMP_PROC_BIND=close),
+                on every logical thread, and on one thread
 
---suite: one JSON line per other workload (FP32 cube, complex and
-FP32-storage / FP64-arithmetic cubes, long systems,
-variable-length batch, block systems, ADI steps and the ADI gradient);
---scale f runs the batched workloads with a fraction f of their systems.
+--suite: one JSON line per workload instead (profiling runs; --scale f runs
+the batched workloads with a fraction f of their systems, --only selects
+workloads by name).
 
 --impl reference: times the reference's own CPU implementation of the path
-(scalar/src/cpu/trid_cpu.cpp built into oracle/_ref) on the same workload
-with every host thread; with N>1 only rank 0 runs it.
+(scalar/src/cpu/trid_cpu.cpp built into oracle/_ref) on the same cube with
+the same measurement as cpu_baseline (each step timed alone, the best step
+reported, physical cores, OMP_PROC_BIND=close); with N>1 only rank 0 runs it.
 """
 
 import argparse
@@ -74,6 +87,10 @@ def make_inputs(seed=1234):
     c = rng.uniform(-1, 1, UNKNOWNS)
     b = np.abs(a) + np.abs(c) + rng.uniform(1, 2, UNKNOWNS)
     d = rng.standard_normal(UNKNOWNS)
+    # a_0 = c_{n-1} = 0 along every axis (the first / last plane of each)
+    A, C = a.reshape(N, N, N), c.reshape(N, N, N)
+    A[0, :, :] = A[:, 0, :] = A[:, :, 0] = 0
+    C[-1, :, :] = C[:, -1, :] = C[:, :, -1] = 0
     return a, b, c, d
 
 
@@ -150,29 +167,106 @@ def read_traffic():
     return out
 
 
-def cpu_baseline_ref(a, b, c, d, reps=2):
-    """The reference CPU solver (oracle/_ref) on the full cube, all threads."""
-    import ctypes
+def host_cpu_info():
+    """Host threads this process may use, the physical cores among them and
+    the CPU model (from lscpu)."""
+    try:
+        cpus = sorted(os.sched_getaffinity(0))
+    except AttributeError:  # pragma: no cover
+        cpus = list(range(os.cpu_count() or 1))
+    cores, model = set(), None
+    try:
+        out = subprocess.run(["lscpu", "-p=CPU,CORE,SOCKET"], capture_output=True, text=True,
+                             timeout=10).stdout
+        allowed = set(cpus)
+        for line in out.splitlines():
+            if line.startswith("#"):
+                continue
+            f = line.split(",")
+            if len(f) >= 3 and f[0].isdigit() and int(f[0]) in allowed:
+                cores.add((f[2], f[1]))
+        info = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in info.splitlines():
+            if line.startswith("Model name:"):
+                model = line.split(":", 1)[1].strip()
+    except (OSError, subprocess.SubprocessError):
+        pass
+    physical = len(cores) if cores else len(cpus)
+    return {"nproc": len(cpus), "physical_cores": physical, "model": model}
 
+
+class RefCPU:
+    """The reference CPU solver (scalar/src/cpu/trid_cpu.cpp compiled
+    unmodified into oracle/_ref, OpenMP) on the 256^3 cube: one step = the
+    three solves, solvedim 0 through its correct scalar path (misaligned
+    pointers), 1 and 2 through its vector paths."""
+
+    def __init__(self, a, b, c, d):
+        import ctypes
+
+        from oracle import oracle
+
+        os.environ.setdefault("OMP_PROC_BIND", "close")
+        self.ct = ctypes
+        lib = oracle.ref_lib()
+        self.f = lib.tridDmtsvStridedBatch
+        self.f.restype = ctypes.c_int
+        self.dims = (ctypes.c_int * 3)(*DIMS)
+        self.placed = {al: [oracle._placed(x, al) for x in (a, b, c, d)] for al in (False, True)}
+        try:  # the OpenMP runtime the reference library was linked with
+            self.gomp = ctypes.CDLL("libgomp.so.1")
+        except OSError:  # pragma: no cover
+            self.gomp = None
+
+    def set_threads(self, n):
+        if self.gomp is not None:
+            self.gomp.omp_set_num_threads(int(n))
+
+    def step(self):
+        for sd in range(3):
+            arrs = self.placed[sd > 0]
+            st = self.f(*[x.ctypes.data_as(self.ct.c_void_p) for x in arrs], None, 3, sd,
+                        self.dims, self.dims)
+            assert st == 0
+
+    def time_steps(self, steps, warmup=1):
+        for _ in range(warmup):
+            self.step()
+        out = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            self.step()
+            out.append(time.perf_counter() - t0)
+        return out
+
+
+def cpu_baseline_entry(a, b, c, d):
+    """The reference CPU solver on the same cube: best of 5 steps on the
+    physical cores, on every logical thread, and best of 3 on one thread."""
     from oracle import oracle
 
-    lib = oracle.ref_lib()
-    f = lib.tridDmtsvStridedBatch
-    f.restype = ctypes.c_int
-    dims = (ctypes.c_int * 3)(*DIMS)
-    best = None
-    placed = {}
-    for aligned in (False, True):
-        placed[aligned] = [oracle._placed(x, aligned) for x in (a, b, c, d)]
-    for _ in range(reps + 1):
-        t0 = time.perf_counter()
-        for sd in range(3):
-            arrs = placed[sd > 0]
-            st = f(*[x.ctypes.data_as(ctypes.c_void_p) for x in arrs], None, 3, sd, dims, dims)
-            assert st == 0
-        dt = time.perf_counter() - t0
-        best = dt if best is None else min(best, dt)
-    return best
+    host = host_cpu_info()
+    if not oracle.ref_available():
+        return {"value": None, "unit": "GB/s", "cores": None, "kind": "reference",
+                "sample": "reference CPU build missing", "host": host}
+    ref = RefCPU(a, b, c, d)
+    gbs = lambda sec: round(3 * BYTES_PER_SOLVE / sec / 1e9, 3)
+    runs = {}
+    for label, threads, reps in (("physical", host["physical_cores"], 5),
+                                 ("logical", host["nproc"], 5), ("one", 1, 3)):
+        if label == "logical" and threads == host["physical_cores"]:
+            continue
+        ref.set_threads(threads)
+        t = ref.time_steps(reps)
+        runs[label] = {"threads": threads, "best_ms": round(min(t) * 1e3, 2),
+                       "mean_ms": round(sum(t) / len(t) * 1e3, 2), "gbs": gbs(min(t))}
+    ref.set_threads(host["physical_cores"])
+    main = runs["physical"]
+    return {"value": main["gbs"], "unit": "GB/s", "cores": main["threads"], "kind": "reference",
+            "sample": "full 256^3 cube, solvedim 0,1,2 once each per step; best of 5 steps after "
+                      "one warm-up (OMP_PROC_BIND=close); 1 thread best of 3",
+            "ms_per_step": main["best_ms"], "runs": runs, "host": host,
+            "omp_proc_bind": os.environ.get("OMP_PROC_BIND")}
 
 
 def run_ours(args):
@@ -301,6 +395,13 @@ def run_ours(args):
     }
     if rank == 0 and world == 1:
         result["differentiation"] = measure_differentiation(torch, tb, max(3, min(args.steps, 20)))
+        if not args.no_workloads:
+            result["reference_gpu"] = measure_reference_gpu(torch, ta, tb_, tc,
+                                                            torch.from_numpy(d0).cuda(), per_axis,
+                                                            max(3, min(args.steps, 10)))
+            del ta, tb_, tc, td
+            torch.cuda.empty_cache()
+            result["workloads"] = measure_workloads(torch, tb, max(3, min(args.steps, 10)))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline_entry(a, b, c, d0)
     if dist:
@@ -397,23 +498,6 @@ def measure_differentiation(torch, tb, steps, seed=99):
     }
 
 
-def cpu_baseline_entry(a, b, c, d):
-    from oracle import oracle
-
-    threads = os.cpu_count()
-    if oracle.ref_available():
-        sec = cpu_baseline_ref(a, b, c, d)
-        kind = "reference"
-        sample = "full 256^3 cube, solvedim 0,1,2 once each, best of 2 after one warm-up"
-    else:
-        sec = None
-        kind = "port"
-        sample = "reference CPU build missing"
-    return {"value": round(3 * BYTES_PER_SOLVE / sec / 1e9, 3) if sec else None, "unit": "GB/s",
-            "cores": threads, "kind": kind, "sample": sample,
-            "ms_per_step": round(sec * 1e3, 2) if sec else None}
-
-
 def run_reference(args):
     rank, world, _ = env_rank()
     if rank != 0:
@@ -423,62 +507,62 @@ def run_reference(args):
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
         return
-    import ctypes
-
-    a, b, c, d = make_inputs(1234)
-    lib = oracle.ref_lib()
-    f = lib.tridDmtsvStridedBatch
-    f.restype = ctypes.c_int
-    dims = (ctypes.c_int * 3)(*DIMS)
-    placed = {al: [oracle._placed(x, al) for x in (a, b, c, d)] for al in (False, True)}
-
-    def step():
-        for sd in range(3):
-            arrs = placed[sd > 0]
-            f(*[x.ctypes.data_as(ctypes.c_void_p) for x in arrs], None, 3, sd, dims, dims)
-
-    for _ in range(args.warmup):
-        step()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        step()
-    sec = (time.perf_counter() - t0) / args.steps
-    value = 3 * BYTES_PER_SOLVE / sec / 1e9
-    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    host = host_cpu_info()
+    ref = RefCPU(*make_inputs(1234))
+    ref.set_threads(host["physical_cores"])
+    times = ref.time_steps(args.steps, warmup=args.warmup)
+    best = min(times)
+    value = 3 * BYTES_PER_SOLVE / best / 1e9
+    sample = (f"full 256^3 cube per step (solvedim 0,1,2), each of {args.steps} steps timed alone "
+              f"after {args.warmup} warm-up steps, the best reported; "
+              f"{host['physical_cores']} OpenMP threads (physical cores), OMP_PROC_BIND=close")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": round(best * 1e3, 3), "mean_ms_per_step": round(sum(times) / len(times) * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": {"workload": WORKLOAD, "dims": DIMS, "solves_per_step": 3,
                    "implementation": "reference scalar/src/cpu/trid_cpu.cpp (OpenMP), "
                                      "solvedim 0 via its scalar path"},
-        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads,
-                         "kind": "reference", "sample": "full 256^3 cube per step"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": host["physical_cores"],
+                         "kind": "reference", "sample": sample, "host": host},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }))
 
 
-def run_suite(args):
-    """The other workloads of the path, one JSON line each (GPU, N=1):
-    FP32 cube per axis, long systems, variable-length batch, block systems
-    (forward and adjoint), ADI steps (eager and CUDA graph) and the
-    checkpointed ADI gradient.  Algorithmic bytes per workload are stated in
-    each line; inputs are seeded synthetic data of the workload's shapes and
-    distributions; every timing is CUDA events around K launches after 2
-    warm-up launches, inputs larger than L2 unless stated."""
-    import torch
+def _parity(got, ref, tol, checked, what):
+    got = np.asarray(got)
+    ref = np.asarray(ref)
+    t = np.complex128 if np.iscomplexobj(got) or np.iscomplexobj(ref) else np.float64
+    err = float(np.abs(got.astype(t) - ref.astype(t)).max() / max(np.abs(ref.astype(t)).max(), 1e-300))
+    return {"checked": checked, "against": what, "max_rel_err": float(f"{err:.3e}"),
+            "tol": tol, "ok": bool(err <= tol)}
 
-    import tridsolver_b200 as tb
+
+def measure_workloads(torch, tb, K, sc=1.0, only=None, emit=None):
+    """The other configurations of the path, each timed with CUDA events
+    around K launches after 2 warm-up launches (inputs larger than L2 unless
+    stated) and checked on sampled systems against the oracle (the plain-C
+    restatement of the reference, test infrastructure only: it runs after
+    the timing, on copies).  Returns one dict per workload; `emit` (if given)
+    receives each as soon as it is measured.  `sc` scales the batched
+    workloads' system counts (profiling runs), `only` keeps the workloads
+    whose name contains it."""
+    from oracle import oracle
+
+    import tridsolver_b200.scalar as tbs
     from tridsolver_b200.adi import ADI
     from tridsolver_b200.block import btsv, btsv_adjoint
     from tridsolver_b200.varlen import solve_varlen
 
+    assert 0 < sc <= 1, "scale in (0, 1]"
     peak, peak_kind = measured_peak()
-    K = max(3, min(args.steps, 10))
     dev = torch.device("cuda")
     gen = torch.Generator(device="cuda").manual_seed(2024)
+    rng = np.random.default_rng(2024)
+    out = []
 
     def timed(fn, reps=K):
         for _ in range(2):
@@ -493,11 +577,15 @@ def run_suite(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps
 
-    def emit(d):
-        d["peak_gbs_" + peak_kind] = peak
+    def add(d):
         if "gbs" in d:
             d["frac_of_" + peak_kind] = round(d["gbs"] / peak, 4)
-        print(json.dumps(d), flush=True)
+        out.append(d)
+        if emit:
+            emit(d)
+
+    def want(name):
+        return only is None or only in name
 
     def coeffs(shape, dtype):
         a = torch.rand(shape, dtype=dtype, device=dev, generator=gen) * 2 - 1
@@ -506,20 +594,6 @@ def run_suite(args):
         d = torch.randn(shape, dtype=dtype, device=dev, generator=gen)
         return a, b, c, d
 
-    def want(name):
-        return args.only is None or args.only in name
-
-    # FP32 256^3, each axis (20 B per unknown)
-    if want("FP32 256^3"):
-        a, b, c, d = coeffs((UNKNOWNS,), torch.float32)
-        for sd in range(3):
-            ms = timed(lambda: tb.tridSmtsvStridedBatch(a, b, c, d, None, 3, sd, DIMS, DIMS))
-            emit({"workload": f"FP32 256^3 solvedim {sd}", "ms": round(ms, 5),
-                  "gbs": round(20 * UNKNOWNS / (ms * 1e-3) / 1e9, 1)})
-        del a, b, c, d
-
-    # complex128 / complex64 256^3 (5 elements of 16 / 8 B per unknown) and
-    # FP32 storage with FP64 arithmetic (20 B per unknown), each axis
     def ccoeffs(shape, dtype):
         rdt = torch.float64 if dtype == torch.complex128 else torch.float32
         r = lambda: torch.rand(shape, dtype=rdt, device=dev, generator=gen) * 2 - 1
@@ -530,152 +604,309 @@ def run_suite(args):
                           torch.randn(shape, dtype=rdt, device=dev, generator=gen))
         return a, b, c, d
 
-    for name, dtype, fn, bpu in (("complex128", torch.complex128, tb.tridZmtsvStridedBatch, 80),
-                                 ("complex64", torch.complex64, tb.tridCmtsvStridedBatch, 40),
-                                 ("FP32 storage / FP64 arithmetic", torch.float32,
-                                  tb.tridSmtsvStridedBatchMixed, 20)):
+    def cube_parity(arrs, x, sd, tol, what, widen=False):
+        """64 systems of the cube, solved by the oracle, against x."""
+        pick = rng.choice(N * N, 64, replace=False)
+        hs = [oracle.systems_view(t.cpu().numpy(), DIMS, sd)[pick] for t in arrs + [x]]
+        if widen:
+            hs = [h.astype(np.float64) for h in hs[:4]] + [hs[4]]
+        # the 64 systems back to back (row s = system s), solved along axis 0
+        rows = [np.ascontiguousarray(h).ravel() for h in hs[:4]]
+        ref = oracle.mtsv(*rows, dims=[N, 64], solvedim=0).reshape(64, N)
+        if widen:
+            ref = ref.astype(np.float32)
+        return _parity(hs[4], ref, tol, 64, what)
+
+    # ---- cubes: FP32, complex128, complex64, FP32 storage / FP64 arithmetic
+    cubes = (("FP32 256^3", torch.float32, tb.tridSmtsvStridedBatch, 20, 1e-5, False),
+             ("complex128 256^3", torch.complex128, tb.tridZmtsvStridedBatch, 80, 1e-12, False),
+             ("complex64 256^3", torch.complex64, tb.tridCmtsvStridedBatch, 40, 1e-5, False),
+             ("FP32 storage / FP64 arithmetic 256^3", torch.float32,
+              tb.tridSmtsvStridedBatchMixed, 20, 2.5e-7, True))
+    for name, dtype, fn, bpu, tol, widen in cubes:
         if not want(name):
             continue
-        a, b, c, d = (ccoeffs((UNKNOWNS,), dtype) if dtype.is_complex
-                      else coeffs((UNKNOWNS,), dtype))
+        a, b, c, d = ccoeffs((UNKNOWNS,), dtype) if dtype.is_complex else coeffs((UNKNOWNS,), dtype)
         for sd in range(3):
-            ms = timed(lambda: fn(a, b, c, d, None, 3, sd, DIMS, DIMS))
-            emit({"workload": f"{name} 256^3 solvedim {sd}", "ms": round(ms, 5),
-                  "gbs": round(bpu * UNKNOWNS / (ms * 1e-3) / 1e9, 1)})
+            x = d.clone()
+            ms = timed(lambda: fn(a, b, c, x, None, 3, sd, DIMS, DIMS))
+            x.copy_(d)
+            assert fn(a, b, c, x, None, 3, sd, DIMS, DIMS) == 0
+            what = ("oracle Thomas in FP64 on the FP32 inputs, rounded to FP32" if widen
+                    else "oracle Thomas (reference operation order)")
+            add({"workload": f"{name} solvedim {sd}", "ms": round(ms, 5),
+                 "gbs": round(bpu * UNKNOWNS / (ms * 1e-3) / 1e9, 1),
+                 "bytes_per_unknown": bpu,
+                 "parity": cube_parity([a, b, c, d], x, sd, tol, what, widen)})
+            del x
         del a, b, c, d
-    if args.only is not None:  # the remaining workloads are not selectable
-        return
-
-    sc = args.scale  # fraction of each workload's systems (1 = the configured sizes)
-    assert 0 < sc <= 1, "--scale in (0, 1]"
-
-    # long systems: 2048 x n=65,536 FP64 along axis 0
-    n, S = 65536, max(1, int(2048 * sc))
-    a, b, c, d = coeffs((S * n,), torch.float64)
-    ms = timed(lambda: tb.tridDmtsvStridedBatch(a, b, c, d, None, 2, 0, [n, S], [n, S]))
-    emit({"workload": f"FP64 {S} systems of n=65,536 (axis 0, blocked partition)",
-          "ms": round(ms, 4), "gbs": round(40 * n * S / (ms * 1e-3) / 1e9, 1),
-          "bytes_per_unknown": {"algorithmic": 40, "moved": "72 + block systems (a, b, c, d read "
-                                "twice: block reduction, then block finish)"}})
-    del a, b, c, d
-
-    # variable-length batch: 200,000 systems, lengths floor(exp(U(ln 8, ln 8192)))
-    rng = np.random.default_rng(7)
-    nvar = max(1, int(200000 * sc))
-    lens = np.floor(np.exp(rng.uniform(np.log(8), np.log(8192), nvar))).astype(np.int64)
-    off = torch.from_numpy(np.concatenate([[0], np.cumsum(lens)])).to(dev)
-    total = int(lens.sum())
-    a, b, c, d = coeffs((total,), torch.float64)
-    ms = timed(lambda: solve_varlen(a, b, c, d, off, total))
-    emit({"workload": f"FP64 variable-length batch, {nvar} systems, n ~ logU[8, 8192]",
-          "unknowns": total, "ms": round(ms, 4),
-          "gbs": round((40 * total + 8 * (len(lens) + 1)) / (ms * 1e-3) / 1e9, 1)})
-    del a, b, c, d, off
-
-    # systems split along the solve dimension: 256^3 FP64 along z cut into P
-    # slabs, every "rank" run in turn on this one GPU (reduce of every slab,
-    # the stacked numbers standing in for the all-gather, finish of every
-    # slab); per-rank time on P GPUs ~ total / P plus the exchange
-    import ctypes as _ct
-
-    from tridsolver_b200 import _lib as _tl
-
-    a, b, c, d = coeffs((UNKNOWNS,), torch.float64)
-    Ls = tb.lib()
-    plane = DIMS[0] * DIMS[1]
-    nsys_z = plane
-
-    def split_step(P):
-        m = DIMS[2] // P
-        loc, pads = _tl.int_array([DIMS[0], DIMS[1], m]), _tl.int_array(DIMS)
-        bn = torch.empty((P, 6, nsys_z), dtype=torch.float64, device=dev)
-        v = lambda t: _ct.c_void_p(t.data_ptr())
-        for r in range(P):
-            o = r * m * plane
-            st = Ls.tridDmtsvStridedBatchSplitReduce(v(a[o:]), v(b[o:]), v(c[o:]), v(d[o:]), 3, 2,
-                                                     loc, pads, v(bn[r]))
-            assert st == 0
-        for r in range(P):
-            o = r * m * plane
-            st = Ls.tridDmtsvStridedBatchSplitFinish(v(a[o:]), v(b[o:]), v(c[o:]), v(d[o:]), None,
-                                                     3, 2, loc, pads, v(bn), P, r, 0)
-            assert st == 0
-
-    tb.scalar._bind_stream(Ls)
-    ms1 = timed(lambda: tb.tridDmtsvStridedBatch(a, b, c, d, None, 3, 2, DIMS, DIMS))
-    for P in (2, 4):
-        ms = timed(lambda: split_step(P))
-        emit({"workload": f"FP64 256^3 along z split into {P} slabs (ranks emulated on one GPU)",
-              "ms_all_slabs": round(ms, 4), "ms_unsplit": round(ms1, 4),
-              "ms_per_rank_estimate": round(ms / P, 4),
-              "gbs_all_slabs": round(40 * UNKNOWNS / (ms * 1e-3) / 1e9, 1),
-              "bytes_per_unknown": "72 (slab reduce 32 + patched local solve 40), plus 48 B per "
-                                   "system and rank exchanged"})
-    del a, b, c, d
-
-    # block tridiagonal: M in {2, 4, 8}, N=256, P=32,768 (interleaved layout)
-    for M in (2, 4, 8):
-        N, P = 256, max(1, int(32768 * sc))
-        A = (torch.rand((N, P, M, M), dtype=torch.float64, device=dev, generator=gen) * 2 - 1) / M
-        C = (torch.rand((N, P, M, M), dtype=torch.float64, device=dev, generator=gen) * 2 - 1) / M
-        B = (torch.rand((N, P, M, M), dtype=torch.float64, device=dev, generator=gen) * 2 - 1) / M
-        B += (2 + torch.rand((N, P, 1, 1), dtype=torch.float64, device=dev, generator=gen)) * \
-            torch.eye(M, dtype=torch.float64, device=dev)
-        dv = torch.randn((N, P, M), dtype=torch.float64, device=dev, generator=gen)
-        x = torch.empty_like(dv)
-        ms = timed(lambda: btsv(A, B, C, dv, x))
-        rows = N * P
-        fwd_b = (3 * M * M + 2 * M) * 8 * rows
-        emit({"workload": f"FP64 block tridiagonal M={M}, N=256, P={P}: forward",
-              "ms": round(ms, 4), "gbs": round(fwd_b / (ms * 1e-3) / 1e9, 1),
-              "bytes_per_block_row": (3 * M * M + 2 * M) * 8})
-        w = torch.randn_like(dv)
-        msa = timed(lambda: btsv_adjoint(A, B, C, x, w))
-        adj_b = (6 * M * M + 3 * M) * 8 * rows
-        emit({"workload": f"FP64 block tridiagonal M={M}, N=256, P={P}: adjoint",
-              "ms": round(msa, 4), "gbs": round(adj_b / (msa * 1e-3) / 1e9, 1),
-              "bytes_per_block_row": (6 * M * M + 3 * M) * 8})
-        del A, B, C, dv, x, w
         torch.cuda.empty_cache()
 
-    # ADI heat diffusion: 128^3 x 100 steps, eager and CUDA graph; 64^3 x 10
-    for shape, steps in (((128, 128, 128), 100), ((64, 64, 64), 10)):
-        u = torch.rand(shape, dtype=torch.float64, device=dev, generator=gen)
-        adi = ADI(shape, 1.0)
-        ms_e = timed(lambda: adi.step(u, steps), reps=2)
-        adi.run(u, 2, graph=True)
-        ms_g = timed(lambda: adi.run(u, steps, graph=True), reps=2)
-        elems = int(np.prod(shape))
-        emit({"workload": f"FP64 ADI {shape[0]}^3 x {steps} steps (lambda=1)",
-              "ms_eager": round(ms_e, 3), "ms_graph": round(ms_g, 3),
-              "us_per_step_graph": round(1e3 * ms_g / steps, 2),
-              "gbs": round(56 * elems * steps / (ms_g * 1e-3) / 1e9, 1),
-              "bytes_per_element_step": "56: x solve with the stencil fused (read u, write "
-                                        "du1), y solve (du1 -> du2), z solve adding into u"})
-        del u, adi
+    # ---- long systems: 2048 x n=65,536 FP64 along axis 0
+    if want("long"):
+        n, S = 65536, max(1, int(2048 * sc))
+        a, b, c, d = coeffs((S * n,), torch.float64)
+        x = d.clone()
+        ms = timed(lambda: tb.tridDmtsvStridedBatch(a, b, c, x, None, 2, 0, [n, S], [n, S]))
+        x.copy_(d)
+        assert tb.tridDmtsvStridedBatch(a, b, c, x, None, 2, 0, [n, S], [n, S]) == 0
+        errs = []
+        for s_ in rng.choice(S, min(S, 3), replace=False):
+            sl = slice(int(s_) * n, int(s_ + 1) * n)
+            ref = oracle.mtsv(*(t[sl].cpu().numpy() for t in (a, b, c, d)), dims=[n], solvedim=0)
+            errs.append(_parity(x[sl].cpu().numpy(), ref, 1e-12, 1, "oracle Thomas"))
+        par = max(errs, key=lambda e: e["max_rel_err"])
+        par["checked"] = len(errs)
+        add({"workload": f"FP64 {S} systems of n=65,536 (axis 0, blocked partition)",
+             "ms": round(ms, 4), "gbs": round(40 * n * S / (ms * 1e-3) / 1e9, 1),
+             "bytes_per_unknown": 40, "parity": par})
+        del a, b, c, d, x
+        torch.cuda.empty_cache()
 
-    # checkpointed adjoint of ||u_200|| at 128^3 w.r.t. u0 and lambda
-    shape = (128, 128, 128)
-    u0 = torch.rand(shape, dtype=torch.float64, device=dev, generator=gen)
-    adi = ADI(shape, 1.0)
-    # warm-up at full size: the caching allocator then holds the run's
-    # temporaries (after the multi-GB block workloads its pool is otherwise
-    # shaped by them, and the timed run spends its time in cudaMalloc)
-    torch.cuda.empty_cache()
-    adi.grad_final_norm(u0, 200, 20)
-    torch.cuda.synchronize()
-    torch.cuda.reset_peak_memory_stats()
-    base = torch.cuda.memory_allocated()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    loss, du0, dlam = adi.grad_final_norm(u0, 200, 20)
-    e1.record()
-    torch.cuda.synchronize()
-    emit({"workload": "FP64 ADI 128^3 x 200 steps: d||u_200|| / d(u0, lambda), checkpoints "
-                      "every 20 steps", "ms": round(e0.elapsed_time(e1), 2),
-          "peak_extra_mib": round((torch.cuda.max_memory_allocated() - base) / 2**20, 1),
-          "loss": float(loss), "dloss_dlambda": float(dlam)})
+    # ---- variable-length batch: 200,000 systems, n ~ floor(exp(U(ln 8, ln 8192)))
+    if want("variable-length"):
+        vrng = np.random.default_rng(7)
+        nvar = max(1, int(200000 * sc))
+        lens = np.floor(np.exp(vrng.uniform(np.log(8), np.log(8192), nvar))).astype(np.int64)
+        off_h = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+        off = torch.from_numpy(off_h).to(dev)
+        total = int(off_h[-1])
+        a, b, c, d = coeffs((total,), torch.float64)
+        x = d.clone()
+        ms = timed(lambda: solve_varlen(a, b, c, x, off, total))
+        x.copy_(d)
+        solve_varlen(a, b, c, x, off, total)
+        pick = np.sort(vrng.choice(nvar, min(nvar, 64), replace=False))
+        segs = [(int(off_h[s_]), int(off_h[s_ + 1])) for s_ in pick]
+        cat = lambda t: np.concatenate([t[lo:hi].cpu().numpy() for lo, hi in segs])
+        soff = np.concatenate([[0], np.cumsum([hi - lo for lo, hi in segs])]).astype(np.int64)
+        ref = oracle.varlen(cat(a), cat(b), cat(c), cat(d), soff)
+        add({"workload": f"FP64 variable-length batch, {nvar} systems, n ~ logU[8, 8192]",
+             "unknowns": total, "ms": round(ms, 4),
+             "gbs": round((40 * total + 8 * (nvar + 1)) / (ms * 1e-3) / 1e9, 1),
+             "bytes": "40 per unknown + 8 per offset",
+             "parity": _parity(cat(x), ref, 1e-12, len(pick), "oracle Thomas per system")})
+        del a, b, c, d, x, off
+        torch.cuda.empty_cache()
+
+    # ---- systems split along the solve dimension (ranks emulated on one GPU)
+    if want("split"):
+        import ctypes as _ct
+
+        from tridsolver_b200 import _lib as _tl
+
+        a, b, c, d = coeffs((UNKNOWNS,), torch.float64)
+        Ls = tb.lib()
+        plane = DIMS[0] * DIMS[1]
+
+        def split_step(P, x):
+            m = DIMS[2] // P
+            loc, pads = _tl.int_array([DIMS[0], DIMS[1], m]), _tl.int_array(DIMS)
+            bn = torch.empty((P, 6, plane), dtype=torch.float64, device=dev)
+            v = lambda t: _ct.c_void_p(t.data_ptr())
+            for r in range(P):
+                o = r * m * plane
+                assert Ls.tridDmtsvStridedBatchSplitReduce(v(a[o:]), v(b[o:]), v(c[o:]), v(x[o:]),
+                                                           3, 2, loc, pads, v(bn[r])) == 0
+            for r in range(P):
+                o = r * m * plane
+                assert Ls.tridDmtsvStridedBatchSplitFinish(v(a[o:]), v(b[o:]), v(c[o:]), v(x[o:]),
+                                                           None, 3, 2, loc, pads, v(bn), P, r,
+                                                           0) == 0
+
+        tbs._bind_stream(Ls)
+        x = d.clone()
+        ms1 = timed(lambda: tb.tridDmtsvStridedBatch(a, b, c, x, None, 3, 2, DIMS, DIMS))
+        for P in (2, 4):
+            ms = timed(lambda: split_step(P, x))
+            x.copy_(d)
+            split_step(P, x)
+            add({"workload": f"FP64 256^3 along z split into {P} slabs (ranks emulated on one GPU)",
+                 "ms": round(ms, 4), "ms_unsplit": round(ms1, 4),
+                 "ms_per_rank_estimate": round(ms / P, 4),
+                 "gbs": round(40 * UNKNOWNS / (ms * 1e-3) / 1e9, 1),
+                 "bytes_per_unknown": "72 moved (slab reduce 32 + patched local solve 40), "
+                                      "40 algorithmic; 48 B per system and rank exchanged",
+                 "parity": cube_parity([a, b, c, d], x, 2, 1e-12, "oracle Thomas on whole systems")})
+        del a, b, c, d, x
+        torch.cuda.empty_cache()
+
+    # ---- block tridiagonal: M in {2, 4, 8}, N=256, P=32,768 (interleaved layout)
+    for M in (2, 4, 8):
+        if not want(f"block tridiagonal M={M}"):
+            continue
+        Nb, P = 256, max(1, int(32768 * sc))
+        kw = dict(dtype=torch.float64, device=dev, generator=gen)
+        A = (torch.rand((Nb, P, M, M), **kw) * 2 - 1) / M
+        C = (torch.rand((Nb, P, M, M), **kw) * 2 - 1) / M
+        B = (torch.rand((Nb, P, M, M), **kw) * 2 - 1) / M
+        B += (2 + torch.rand((Nb, P, 1, 1), **kw)) * torch.eye(M, dtype=torch.float64, device=dev)
+        dv = torch.randn((Nb, P, M), **kw)
+        x = torch.empty_like(dv)
+        ms = timed(lambda: btsv(A, B, C, dv, x))
+        w = torch.randn_like(dv)
+        grads = btsv_adjoint(A, B, C, x, w)
+        msa = timed(lambda: btsv_adjoint(A, B, C, x, w))
+        grads = btsv_adjoint(A, B, C, x, w)
+        torch.cuda.synchronize()
+        pick = torch.from_numpy(np.sort(rng.choice(P, min(P, 32), replace=False))).to(dev)
+        sA, sB, sC, sd_, sx, sw, gd = (t.index_select(1, pick).contiguous().cpu().numpy()
+                                       for t in (A, B, C, dv, x, w, grads[3]))
+        S = pick.numel()
+        u = oracle.btsv(sA, sB, sC, sd_, Nb, S, M, layout=0).reshape(Nb, S, M)
+        g = oracle.btsv(sA, sB, sC, sw, Nb, S, M, layout=0, transpose=True).reshape(Nb, S, M)
+        rows = Nb * P
+        add({"workload": f"FP64 block tridiagonal M={M}, N=256, P={P}: forward",
+             "ms": round(ms, 4), "gbs": round((3 * M * M + 2 * M) * 8 * rows / (ms * 1e-3) / 1e9, 1),
+             "bytes_per_block_row": (3 * M * M + 2 * M) * 8,
+             "parity": _parity(sx, u, 1e-12, S, "block Thomas oracle (corrected reference gold)")})
+        add({"workload": f"FP64 block tridiagonal M={M}, N=256, P={P}: adjoint",
+             "ms": round(msa, 4), "gbs": round((6 * M * M + 3 * M) * 8 * rows / (msa * 1e-3) / 1e9, 1),
+             "bytes_per_block_row": (6 * M * M + 3 * M) * 8,
+             "parity": _parity(gd, g, 1e-12, S, "block Thomas oracle on the transposed system")})
+        del A, B, C, dv, x, w, grads
+        torch.cuda.empty_cache()
+
+    # ---- ADI heat diffusion (baseline coefficients, lambda = 1)
+    if want("ADI"):
+        for shape, steps in (((64, 64, 64), 10), ((128, 128, 128), 100)):
+            u0 = torch.rand(shape, dtype=torch.float64, device=dev, generator=gen)
+            adi = ADI(shape, 1.0)
+            u = u0.clone()
+            ms_e = timed(lambda: adi.step(u, steps), reps=2)
+            ug = u0.clone()
+            adi.run(ug, 2, graph=True)
+            ms_g = timed(lambda: adi.run(ug, steps, graph=True), reps=2)
+            # parity: graph replay against eager steps from the same state,
+            # and (64^3) the eager steps against the oracle
+            ue, ug = u0.clone(), u0.clone()
+            adi.step(ue, steps)
+            adi._graph = None
+            adi.run(ug, steps, graph=True)
+            torch.cuda.synchronize()
+            par = {"graph_vs_eager_bitwise": bool(torch.equal(ue, ug))}
+            if shape[0] == 64:
+                ref = oracle.adi(u0.cpu().numpy(), 64, 64, 64, steps, 1.0, -1.0, 3.0, -1.0)
+                par.update(_parity(ue.cpu().numpy().ravel(), ref.ravel(), 1e-12, 1,
+                                   "oracle ADI steps (Thomas along x, y, z)"))
+                par["ok"] = par["ok"] and par["graph_vs_eager_bitwise"]
+            else:
+                par["ok"] = par["graph_vs_eager_bitwise"]
+            elems = int(np.prod(shape))
+            add({"workload": f"FP64 ADI {shape[0]}^3 x {steps} steps (lambda=1)",
+                 "ms_eager": round(ms_e, 3), "ms_graph": round(ms_g, 3),
+                 "us_per_step_graph": round(1e3 * ms_g / steps, 2),
+                 "gbs": round(56 * elems * steps / (ms_g * 1e-3) / 1e9, 1),
+                 "bytes_per_element_step": "56: x solve with the stencil fused (read u, write "
+                                           "du1), y solve (du1 -> du2), z solve adding into u; "
+                                           "the 128^3 working set stays in L2",
+                 "parity": par})
+            del u0, u, ug, ue, adi
+
+        # checkpointed adjoint of ||u_200|| at 128^3 w.r.t. u0 and lambda
+        shape = (128, 128, 128)
+        u0 = torch.rand(shape, dtype=torch.float64, device=dev, generator=gen)
+        adi = ADI(shape, 1.0)
+        torch.cuda.empty_cache()
+        adi.grad_final_norm(u0, 200, 20)  # warm-up at full size
+        torch.cuda.synchronize()
+        torch.cuda.reset_peak_memory_stats()
+        base = torch.cuda.memory_allocated()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        loss, du0, dlam = adi.grad_final_norm(u0, 200, 20)
+        e1.record()
+        torch.cuda.synchronize()
+        peak_mib = (torch.cuda.max_memory_allocated() - base) / 2**20
+
+        def final_norm(lam):
+            a2 = ADI(shape, lam)
+            u = u0.clone()
+            a2.step(u, 200)
+            return float(torch.linalg.vector_norm(u))
+
+        h = 1e-6
+        fd = (final_norm(1.0 + h) - final_norm(1.0 - h)) / (2 * h)
+        err = abs(fd - float(dlam)) / max(1.0, abs(fd))
+        add({"workload": "FP64 ADI 128^3 x 200 steps: d||u_200|| / d(u0, lambda), checkpoints "
+                         "every 20 steps", "ms": round(e0.elapsed_time(e1), 2),
+             "peak_extra_mib": round(peak_mib, 1), "loss": float(loss),
+             "dloss_dlambda": float(dlam),
+             "parity": {"checked": 1, "against": "central difference in lambda, h = 1e-6",
+                        "fd": fd, "rel_err": float(f"{err:.3e}"), "tol": 1e-6,
+                        "ok": bool(err <= 1e-6)}})
+        del u0, du0, adi
+        torch.cuda.empty_cache()
+    return out
+
+
+def measure_reference_gpu(torch, ta, tb_, tc, td0, ours_ms, K):
+    """The reference's own GPU library (scalar/src/cuda/trid_cuda.cu, built
+    unmodified for sm_100a into oracle/_ref) on the same 256^3 FP64 cube, per
+    axis and `opts` value (0 = its default: cuBLAS transposes around the y
+    solve on x, the strided Thomas kernel on y/z; 3 = its register-transpose
+    x kernel / its Thomas-PCR y/z kernels).  Its entry points synchronise the
+    device on every call (trid_cuda.cu:519-530), so each call is timed with
+    that included, as a caller sees it.  Compared with our solve of the same
+    cube (relative max-norm)."""
+    import ctypes
+
+    path = os.path.join(ROOT, "oracle", "_ref", "libtrid_cuda_ref.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/libtrid_cuda_ref.so not built"}
+    import tridsolver_b200 as tb
+
+    lib = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
+    f = lib.tridDmtsvStridedBatch
+    f.restype = ctypes.c_int
+    dims = (ctypes.c_int * 3)(*DIMS)
+    v = lambda t: ctypes.c_void_p(t.data_ptr())
+    out = {"library": "reference scalar/src/cuda/trid_cuda.cu (sm_100a, N_MAX=1024)",
+           "per_axis": []}
+    ours = td0.clone()
+    x = td0.clone()
+    for sd in range(3):
+        ours.copy_(td0)
+        assert tb.tridDmtsvStridedBatch(ta, tb_, tc, ours, None, 3, sd, DIMS, DIMS) == 0
+        for opt in (0, 3):
+            opts = (ctypes.c_int * 3)(*[opt if k == sd else 0 for k in range(3)])
+            call = lambda: f(v(ta), v(tb_), v(tc), v(x), None, 3, sd, dims, dims, opts, 1)
+            x.copy_(td0)
+            call()
+            torch.cuda.synchronize()
+            err = float((x - ours).abs().max() / ours.abs().max())
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(K):
+                call()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / K
+            out["per_axis"].append({
+                "solvedim": sd, "opt": opt, "ms": round(ms, 4),
+                "gbs": round(BYTES_PER_SOLVE / (ms * 1e-3) / 1e9, 1),
+                "ours_ms": round(ours_ms[sd], 4),
+                "speedup_ours": round(ms / ours_ms[sd], 2),
+                "rel_diff_vs_ours": float(f"{err:.3e}")})
+    del ours, x
+    return out
+
+
+def run_suite(args):
+    """--suite: one JSON line per workload (GPU, N=1)."""
+    import torch
+
+    import tridsolver_b200 as tb
+
+    peak, peak_kind = measured_peak()
+
+    def emit(d):
+        d["peak_gbs_" + peak_kind] = peak
+        print(json.dumps(d), flush=True)
+
+    measure_workloads(torch, tb, max(3, min(args.steps, 10)), args.scale, args.only, emit)
 
 
 def main():
@@ -685,11 +916,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="skip the workloads and reference_gpu keys (profiling runs)")
     ap.add_argument("--suite", action="store_true",
                     help="instead: one JSON line per other workload of the path (1 GPU)")
     ap.add_argument("--only", default=None,
-                    help="--suite: run only the cube workloads whose name contains this "
-                         "(e.g. 'complex128', 'FP32 storage')")
+                    help="--suite: run only the workloads whose name contains this "
+                         "(e.g. 'complex128', 'block tridiagonal M=8', 'ADI')")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="--suite: fraction of each workload's systems (profiling runs)")
     args = ap.parse_args()

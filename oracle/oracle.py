@@ -52,6 +52,9 @@ def ref_available():
 def ref_lib():
     global _REF
     if _REF is None:
+        # the reference keeps c2/d2[N_MAX] (N_MAX = 65536) of SIMD vectors on
+        # every OpenMP thread's stack; libgomp reads this when it loads
+        os.environ.setdefault("OMP_STACKSIZE", "64M")
         _REF = ctypes.CDLL(os.path.join(HERE, "_ref", "libtrid_cpu_ref.so"))
     return _REF
 
