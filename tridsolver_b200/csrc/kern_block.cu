@@ -912,6 +912,364 @@ __global__ void __launch_bounds__(128) blockm_adj_kernel(BlkArgs<T> a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// M = 8, FP64: four lanes per system, lane t owning columns 2t and 2t+1 of
+// the augmented block [X_n | C_n] and (replicated in all four) the right-hand
+// side column.
+//   * X_n = B_n - A_n C'_{n-1}: each lane needs all of A_n (read from shared
+//     memory, the same address for the system's four lanes) and only its own
+//     columns of C'_{n-1}, which it computed itself: no exchange.
+//   * Gauss-Jordan on [X | C | d]: at pivot q every lane needs column q of X
+//     (8 values, owned by lane q/2): one shuffle per value; the pivot row's
+//     entries in the lane's own columns are local.
+//   * Backward sweep x_n = d'_n - C'_n x_{n+1}: each lane forms the partial
+//     sums over its two columns for all eight rows, a two-round
+//     reduce-scatter over the four lanes leaves lane t rows 2t and 2t+1, which
+//     are exactly the unknowns its columns need one step later.
+// Per block row that is 8 value broadcasts per pivot and 6 in the backward
+// sweep, against the row-per-lane kernel's shared-memory round trip of every
+// pivot row and every row of C'.
+//
+// Staging: a CTA of kB8Warps warps owns 8*kB8Warps consecutive systems.  The
+// blocks of one block row n of those systems are contiguous in the
+// interleaved layout; they are copied 16 bytes at a time (cp.async, coalesced
+// global reads) into one shared-memory record per system, two records per
+// system (step n computed while step n+1 lands).  Inside a record the 16-byte
+// chunk (row r, half h) of a block sits at r*4 + (h ^ ((r >> 1) & 3)): the
+// lanes' own-column reads (forward: row r, chunk t) and the adjoint's
+// transposed reads (rows 2t, 2t+1, chunk h) then hit distinct banks, and the
+// record stride (200 doubles = 16 banks mod 32) separates the two systems of
+// a quarter-warp.
+// C'_n goes to the scratch array in a lane-major order (lane t's 16 values
+// contiguous), d'_n as the plain vector; the layout of the scratch is private
+// to this kernel.
+//
+// Adjoint: the transposed system (sub-diagonal C_{n-1}^T, diagonal B_n^T,
+// super-diagonal A_{n+1}^T, right-hand side w_n) through the same code with
+// transposed shared-memory reads; the backward sweep forms dA, dB, dC rows
+// 2t, 2t+1 and dd from g_n and the forward solution u.
+constexpr int kB8Warps = 7;
+constexpr int kB8Sys = 8 * kB8Warps;  // systems per CTA
+constexpr int kB8Rec = 200;           // doubles per system record: 3 blocks + rhs
+constexpr int kB8Smem = 2 * kB8Sys * kB8Rec * (int)sizeof(double);
+
+__device__ __forceinline__ int b8_chunk(int r, int h) { return r * 4 + (h ^ ((r >> 1) & 3)); }
+
+__device__ __forceinline__ void b8_cp16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+
+__device__ __forceinline__ double2 b8_lds(const double *p) {
+  return *reinterpret_cast<const double2 *>(p);
+}
+
+__device__ __forceinline__ double2 b8_ldg(const double *p) {
+  return __ldcs(reinterpret_cast<const double2 *>(p));
+}
+
+__device__ __forceinline__ void b8_stg(double *p, double x, double y) {
+  *reinterpret_cast<double2 *>(p) = make_double2(x, y);
+}
+
+// v[2t], v[2t+1] of a replicated 8-vector (t = lane's column pair) without
+// run-time register indexing
+__device__ __forceinline__ void b8_pick(const double (&v)[8], int t, double &v0, double &v1) {
+  v0 = t == 0 ? v[0] : (t == 1 ? v[2] : (t == 2 ? v[4] : v[6]));
+  v1 = t == 0 ? v[1] : (t == 1 ? v[3] : (t == 2 ? v[5] : v[7]));
+}
+
+// sum over the system's four lanes of part[0..7], lane t receiving the sums
+// of entries 2t and 2t+1 (two butterfly rounds, halves exchanged)
+__device__ __forceinline__ void b8_reduce_scatter(const double (&part)[8], int t, double &s0,
+                                                  double &s1) {
+  constexpr unsigned kFull = 0xffffffffu;
+  const bool hi2 = (t & 2) != 0, hi1 = (t & 1) != 0;
+  double keep[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const double send = hi2 ? part[j] : part[4 + j];
+    const double mine = hi2 ? part[4 + j] : part[j];
+    keep[j] = mine + __shfl_xor_sync(kFull, send, 2);
+  }
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const double send = hi1 ? keep[j] : keep[2 + j];
+    const double mine = hi1 ? keep[2 + j] : keep[j];
+    (j == 0 ? s0 : s1) = mine + __shfl_xor_sync(kFull, send, 1);
+  }
+}
+
+template <bool ADJ>
+__global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double> a) {
+  extern __shared__ __align__(16) unsigned char b8_dyn[];
+  double *sm = reinterpret_cast<double *>(b8_dyn);
+  constexpr unsigned kFull = 0xffffffffu;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int sw = lane >> 2, t = lane & 3;
+  const int sl = (tid >> 5) * 8 + sw;  // system within the CTA
+  const int64_t P = a.P;
+  const int N = a.N;
+  const int64_t p0 = (int64_t)blockIdx.x * kB8Sys;
+  const int nval = (int)(P - p0 < kB8Sys ? P - p0 : kB8Sys);
+  const bool valid = sl < nval;
+  const int64_t p = p0 + sl;
+  auto bx = [&](int n) { return ((int64_t)n * P + p) * 64; };
+  auto vx = [&](int n) { return ((int64_t)n * P + p) * 8; };
+
+  // copies of block row n into record set st: slot 0 sub-diagonal, 1
+  // diagonal, 2 super-diagonal (blocks), rhs at 192
+  auto issue = [&](int n, int st) {
+    double *base = sm + (size_t)st * kB8Sys * kB8Rec;
+    const double *blk[3];
+    int bn[3];
+    if (!ADJ) {
+      blk[0] = a.A; bn[0] = n;
+      blk[1] = a.B; bn[1] = n;
+      blk[2] = a.C; bn[2] = n;
+    } else {
+      blk[0] = a.C; bn[0] = n - 1;  // C_{n-1}^T
+      blk[1] = a.B; bn[1] = n;      // B_n^T
+      blk[2] = a.A; bn[2] = n + 1;  // A_{n+1}^T
+    }
+    const bool has[3] = {n > 0, true, n < N - 1};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (!has[k]) continue;
+      const double *src = blk[k] + ((int64_t)bn[k] * P + p0) * 64;
+      for (int j = tid; j < nval * 32; j += kB8Warps * 32) {
+        const int s = j >> 5, c = j & 31;
+        b8_cp16(base + s * kB8Rec + k * 64 + b8_chunk(c >> 2, c & 3) * 2, src + (int64_t)j * 2);
+      }
+    }
+    const double *rs = a.d + ((int64_t)n * P + p0) * 8;
+    for (int j = tid; j < nval * 4; j += kB8Warps * 32)
+      b8_cp16(base + (j >> 2) * kB8Rec + 192 + (j & 3) * 2, rs + (int64_t)j * 2);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+
+  double Cp[8][2], dp[8];  // own columns of C'_{n-1}; d'_{n-1} (replicated)
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    Cp[r][0] = Cp[r][1] = 0.0;
+    dp[r] = 0.0;
+  }
+  issue(0, 0);
+  for (int n = 0; n < N; ++n) {
+    const int st = n & 1;
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();  // block row n landed for every system; set st^1 is free
+    if (n + 1 < N) issue(n + 1, st ^ 1);
+    const double *rec = sm + (size_t)st * kB8Sys * kB8Rec + sl * kB8Rec;
+    double X[8][2], R[8][2], rd[8];
+    // diagonal and super-diagonal blocks, own columns (transposed: own rows)
+    if (!ADJ) {
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const double2 v = b8_lds(rec + 64 + b8_chunk(r, t) * 2);
+        X[r][0] = v.x;
+        X[r][1] = v.y;
+      }
+    } else {
+#pragma unroll
+      for (int h = 0; h < 4; ++h)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const double2 v = b8_lds(rec + 64 + b8_chunk(2 * t + c, h) * 2);
+          X[2 * h][c] = v.x;
+          X[2 * h + 1][c] = v.y;
+        }
+    }
+    if (n < N - 1) {
+      if (!ADJ) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const double2 v = b8_lds(rec + 128 + b8_chunk(r, t) * 2);
+          R[r][0] = v.x;
+          R[r][1] = v.y;
+        }
+      } else {
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            const double2 v = b8_lds(rec + 128 + b8_chunk(2 * t + c, h) * 2);
+            R[2 * h][c] = v.x;
+            R[2 * h + 1][c] = v.y;
+          }
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < 8; ++r) R[r][0] = R[r][1] = 0.0;
+    }
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const double2 v = b8_lds(rec + 192 + 2 * h);
+      rd[2 * h] = v.x;
+      rd[2 * h + 1] = v.y;
+    }
+    // X -= S C'_{n-1}, rd -= S d'_{n-1}, S the sub-diagonal block (A_n, or
+    // C_{n-1}^T for the adjoint)
+    if (n > 0) {
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const double2 v = b8_lds(rec + b8_chunk(r, h) * 2);
+          if (!ADJ) {  // A[r][2h], A[r][2h+1]
+#pragma unroll
+            for (int c = 0; c < 2; ++c) X[r][c] -= v.x * Cp[2 * h][c] + v.y * Cp[2 * h + 1][c];
+            rd[r] -= v.x * dp[2 * h] + v.y * dp[2 * h + 1];
+          } else {  // C[r][2h], C[r][2h+1] = C^T[2h][r], C^T[2h+1][r]
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              X[2 * h][c] -= v.x * Cp[r][c];
+              X[2 * h + 1][c] -= v.y * Cp[r][c];
+            }
+            rd[2 * h] -= v.x * dp[r];
+            rd[2 * h + 1] -= v.y * dp[r];
+          }
+        }
+    }
+    // Gauss-Jordan on [X | R | rd] (no pivoting: block diagonal dominance)
+    const int src0 = lane & ~3;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      double pc[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) pc[r] = __shfl_sync(kFull, X[r][q & 1], src0 + (q >> 1));
+      const double inv = rcp(pc[q]);
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        X[q][c] *= inv;
+        R[q][c] *= inv;
+      }
+      rd[q] *= inv;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        if (r == q) continue;
+        const double f = pc[r];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          X[r][c] -= f * X[q][c];
+          R[r][c] -= f * R[q][c];
+        }
+        rd[r] -= f * rd[q];
+      }
+    }
+    if (valid && n < N - 1) {
+#pragma unroll
+      for (int r = 0; r < 8; ++r) b8_stg(a.Cs + bx(n) + t * 16 + r * 2, R[r][0], R[r][1]);
+      double d0, d1;
+      b8_pick(rd, t, d0, d1);
+      b8_stg(a.ds + vx(n) + 2 * t, d0, d1);
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      Cp[r][0] = R[r][0];
+      Cp[r][1] = R[r][1];
+      dp[r] = rd[r];
+    }
+  }
+  // backward sweep; (x0, x1) = rows 2t, 2t+1 of x_n (g_n for the adjoint).
+  // Lanes of systems past the end stay in the loop (the reduce-scatter
+  // shuffles take the whole warp) with their memory accesses switched off.
+  double x0, x1;
+  b8_pick(dp, t, x0, x1);
+  double u_nx[8], u_cu[8], u_pv[8];  // adjoint: u_{n+1}, u_n, u_{n-1}
+  auto load_u = [&](int n, double (&u)[8]) {
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const double2 v =
+          (valid && n >= 0 && n < N) ? b8_ldg(a.u + vx(n) + 2 * h) : make_double2(0.0, 0.0);
+      u[2 * h] = v.x;
+      u[2 * h + 1] = v.y;
+    }
+  };
+  if (ADJ) {
+    load_u(N - 1, u_cu);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) u_nx[j] = 0.0;
+  }
+  auto emit = [&](int n) {
+    if (!valid) return;
+    if (!ADJ) {
+      b8_stg(a.x + vx(n) + 2 * t, x0, x1);
+      return;
+    }
+    if (a.dd) b8_stg(a.dd + vx(n) + 2 * t, x0, x1);
+    load_u(n - 1, u_pv);
+    const double *us[3] = {u_pv, u_cu, u_nx};
+    double *outs[3] = {a.dA, a.dB, a.dC};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (!outs[k]) continue;
+      double *o = outs[k] + bx(n) + t * 16;
+#pragma unroll
+      for (int j = 0; j < 8; j += 2) {
+        b8_stg(o + j, -x0 * us[k][j], -x0 * us[k][j + 1]);
+        b8_stg(o + 8 + j, -x1 * us[k][j], -x1 * us[k][j + 1]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      u_nx[j] = u_cu[j];
+      u_cu[j] = u_pv[j];
+    }
+  };
+  emit(N - 1);
+  // C'_n (own 16 values) and d'_n (own pair) one step ahead
+  double cn[8][2], dn0 = 0.0, dn1 = 0.0;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) cn[r][0] = cn[r][1] = 0.0;
+  auto load_c = [&](int n) {
+    if (n < 0 || !valid) return;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const double2 v = b8_ldg(a.Cs + bx(n) + t * 16 + r * 2);
+      cn[r][0] = v.x;
+      cn[r][1] = v.y;
+    }
+    const double2 v = b8_ldg(a.ds + vx(n) + 2 * t);
+    dn0 = v.x;
+    dn1 = v.y;
+  };
+  load_c(N - 2);
+  for (int n = N - 2; n >= 0; --n) {
+    double part[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) part[r] = cn[r][0] * x0 + cn[r][1] * x1;
+    const double e0 = dn0, e1 = dn1;
+    load_c(n - 1);
+    double s0, s1;
+    b8_reduce_scatter(part, t, s0, s1);
+    x0 = e0 - s0;
+    x1 = e1 - s1;
+    emit(n);
+  }
+}
+
+// Dynamic shared memory of the M = 8 kernels, set once per device.
+static cudaError_t block8_prepare() {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  static bool done[64] = {};
+  if (!done[dev]) {
+    e = cudaFuncSetAttribute(block8_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kB8Smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(block8_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kB8Smem);
+    if (e != cudaSuccess) return e;
+    done[dev] = true;
+  }
+  return cudaSuccess;
+}
+
 template <typename T, bool ADJ>
 cudaError_t launch_block(const BlkArgs<T> &a, int M, cudaStream_t st) {
   auto go = [&](auto kern, int m) {
@@ -950,6 +1308,22 @@ cudaError_t launch_block(const BlkArgs<T> &a, int M, cudaStream_t st) {
         if (M == 3) blockm_kernel<T, 3><<<g, b, 0, st>>>(a);
         else blockm_kernel<T, 4><<<g, b, 0, st>>>(a);
       }
+      return cudaGetLastError();
+    }
+  }
+  if constexpr (sizeof(T) == 8) {
+    // M = 8 FP64: four lanes per system (16-byte copies and accesses: every
+    // array 16-byte aligned, a null gradient output counts as aligned)
+    const uintptr_t bits = (uintptr_t)a.A | (uintptr_t)a.B | (uintptr_t)a.C | (uintptr_t)a.d |
+                           (uintptr_t)a.u | (uintptr_t)a.x | (uintptr_t)a.dA | (uintptr_t)a.dB |
+                           (uintptr_t)a.dC | (uintptr_t)a.dd | (uintptr_t)a.Cs | (uintptr_t)a.ds;
+    if (M == 8 && (bits & 15) == 0) {
+      const int64_t blocks = (a.P + kB8Sys - 1) / kB8Sys;
+      if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
+      cudaError_t e = block8_prepare();
+      if (e != cudaSuccess) return e;
+      block8_kernel<ADJ><<<dim3((unsigned)blocks), dim3(kB8Warps * 32), kB8Smem, st>>>(
+          reinterpret_cast<const BlkArgs<double> &>(a));
       return cudaGetLastError();
     }
   }
