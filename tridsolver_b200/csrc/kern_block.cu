@@ -951,7 +951,15 @@ __global__ void __launch_bounds__(128) blockm_adj_kernel(BlkArgs<T> a) {
 constexpr int kB8Warps = 7;
 constexpr int kB8Sys = 8 * kB8Warps;  // systems per CTA
 constexpr int kB8Rec = 200;           // doubles per system record: 3 blocks + rhs
-constexpr int kB8Smem = 2 * kB8Sys * kB8Rec * (int)sizeof(double);
+constexpr int kB8WarpDoubles = 2 * 8 * kB8Rec;  // a warp's region: two record sets
+constexpr int kB8Smem = kB8Warps * kB8WarpDoubles * (int)sizeof(double);
+// backward ring: per slot 8 records of C'_n (64) + d'_n (8), then u_{n-1} of
+// the 8 systems (adjoint); the record stride (72 doubles = 16 banks mod 32)
+// keeps a quarter-warp's two systems on separate banks
+constexpr int kB8BackRec = 72;
+constexpr int kB8BackSlot = 8 * kB8BackRec + 64;
+constexpr int kB8Ring = kB8WarpDoubles / kB8BackSlot;  // 5 slots
+static_assert(kB8Ring >= 2, "backward ring");
 
 __device__ __forceinline__ int b8_chunk(int r, int h) { return r * 4 + (h ^ ((r >> 1) & 3)); }
 
@@ -1005,24 +1013,27 @@ __device__ __forceinline__ void b8_reduce_scatter(const double (&part)[8], int t
 template <bool ADJ>
 __global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double> a) {
   extern __shared__ __align__(16) unsigned char b8_dyn[];
-  double *sm = reinterpret_cast<double *>(b8_dyn);
   constexpr unsigned kFull = 0xffffffffu;
-  const int tid = threadIdx.x, lane = tid & 31;
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
   const int sw = lane >> 2, t = lane & 3;
-  const int sl = (tid >> 5) * 8 + sw;  // system within the CTA
   const int64_t P = a.P;
   const int N = a.N;
-  const int64_t p0 = (int64_t)blockIdx.x * kB8Sys;
-  const int nval = (int)(P - p0 < kB8Sys ? P - p0 : kB8Sys);
-  const bool valid = sl < nval;
-  const int64_t p = p0 + sl;
+  // this warp's 8 systems and its private shared-memory region
+  const int64_t pw = (int64_t)blockIdx.x * kB8Sys + wi * 8;
+  if (pw >= P) return;  // warp-uniform: no system of this warp exists
+  const int nvw = (int)(P - pw < 8 ? P - pw : 8);
+  const bool valid = sw < nvw;
+  const int64_t p = pw + sw;
+  double *wreg = reinterpret_cast<double *>(b8_dyn) + (size_t)wi * kB8WarpDoubles;
   auto bx = [&](int n) { return ((int64_t)n * P + p) * 64; };
   auto vx = [&](int n) { return ((int64_t)n * P + p) * 8; };
 
-  // copies of block row n into record set st: slot 0 sub-diagonal, 1
-  // diagonal, 2 super-diagonal (blocks), rhs at 192
+  // ---- forward sweep: block row n of the warp's systems staged into
+  // record set n & 1 (slot 0 sub-diagonal, 1 diagonal, 2 super-diagonal,
+  // rhs at 192); lane l copies chunk l of every block
+  const int cpos = b8_chunk(lane >> 2, lane & 3) * 2;
   auto issue = [&](int n, int st) {
-    double *base = sm + (size_t)st * kB8Sys * kB8Rec;
+    double *base = wreg + st * 8 * kB8Rec;
     const double *blk[3];
     int bn[3];
     if (!ADJ) {
@@ -1038,15 +1049,12 @@ __global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       if (!has[k]) continue;
-      const double *src = blk[k] + ((int64_t)bn[k] * P + p0) * 64;
-      for (int j = tid; j < nval * 32; j += kB8Warps * 32) {
-        const int s = j >> 5, c = j & 31;
-        b8_cp16(base + s * kB8Rec + k * 64 + b8_chunk(c >> 2, c & 3) * 2, src + (int64_t)j * 2);
-      }
+      const double *src = blk[k] + ((int64_t)bn[k] * P + pw) * 64 + lane * 2;
+#pragma unroll
+      for (int s = 0; s < 8; ++s)
+        if (s < nvw) b8_cp16(base + s * kB8Rec + k * 64 + cpos, src + s * 64);
     }
-    const double *rs = a.d + ((int64_t)n * P + p0) * 8;
-    for (int j = tid; j < nval * 4; j += kB8Warps * 32)
-      b8_cp16(base + (j >> 2) * kB8Rec + 192 + (j & 3) * 2, rs + (int64_t)j * 2);
+    if (valid) b8_cp16(base + sw * kB8Rec + 192 + t * 2, a.d + ((int64_t)n * P + pw) * 8 + lane * 2);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
 
@@ -1060,11 +1068,11 @@ __global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double
   for (int n = 0; n < N; ++n) {
     const int st = n & 1;
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    __syncthreads();  // block row n landed for every system; set st^1 is free
+    __syncwarp();  // row n landed for the warp; set st^1 is no longer read
     if (n + 1 < N) issue(n + 1, st ^ 1);
-    const double *rec = sm + (size_t)st * kB8Sys * kB8Rec + sl * kB8Rec;
+    const double *rec = wreg + st * 8 * kB8Rec + sw * kB8Rec;
     double X[8][2], R[8][2], rd[8];
-    // diagonal and super-diagonal blocks, own columns (transposed: own rows)
+    // diagonal block, own columns (transposed: own rows)
     if (!ADJ) {
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
@@ -1081,28 +1089,6 @@ __global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double
           X[2 * h][c] = v.x;
           X[2 * h + 1][c] = v.y;
         }
-    }
-    if (n < N - 1) {
-      if (!ADJ) {
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          const double2 v = b8_lds(rec + 128 + b8_chunk(r, t) * 2);
-          R[r][0] = v.x;
-          R[r][1] = v.y;
-        }
-      } else {
-#pragma unroll
-        for (int h = 0; h < 4; ++h)
-#pragma unroll
-          for (int c = 0; c < 2; ++c) {
-            const double2 v = b8_lds(rec + 128 + b8_chunk(2 * t + c, h) * 2);
-            R[2 * h][c] = v.x;
-            R[2 * h + 1][c] = v.y;
-          }
-      }
-    } else {
-#pragma unroll
-      for (int r = 0; r < 8; ++r) R[r][0] = R[r][1] = 0.0;
     }
 #pragma unroll
     for (int h = 0; h < 4; ++h) {
@@ -1132,6 +1118,29 @@ __global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double
             rd[2 * h + 1] -= v.y * dp[r];
           }
         }
+    }
+    // super-diagonal block, own columns (C'_{n-1} is dead from here on)
+    if (n < N - 1) {
+      if (!ADJ) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const double2 v = b8_lds(rec + 128 + b8_chunk(r, t) * 2);
+          R[r][0] = v.x;
+          R[r][1] = v.y;
+        }
+      } else {
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            const double2 v = b8_lds(rec + 128 + b8_chunk(2 * t + c, h) * 2);
+            R[2 * h][c] = v.x;
+            R[2 * h + 1][c] = v.y;
+          }
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < 8; ++r) R[r][0] = R[r][1] = 0.0;
     }
     // Gauss-Jordan on [X | R | rd] (no pivoting: block diagonal dominance)
     const int src0 = lane & ~3;
@@ -1173,13 +1182,36 @@ __global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double
       dp[r] = rd[r];
     }
   }
-  // backward sweep; (x0, x1) = rows 2t, 2t+1 of x_n (g_n for the adjoint).
+
+  // ---- backward sweep; (x0, x1) = rows 2t, 2t+1 of x_n (g_n for the
+  // adjoint).  C'_n, d'_n (and u_{n-1} for the adjoint) of the warp's
+  // systems stream through a ring of kB8Ring slots in the same region, kB8Ring
+  // - 1 steps ahead; lane (sw, t) reads its 16 values of C'_n as chunk
+  // t*8 + (r ^ t) of its system's record (conflict-free), d'_n at +64.
   // Lanes of systems past the end stay in the loop (the reduce-scatter
   // shuffles take the whole warp) with their memory accesses switched off.
+  __syncwarp();  // every lane is done with the forward records
+  const int bpos = (lane >> 3) * 8 + ((lane & 7) ^ (lane >> 3));  // chunk of lane's C' copy
+  auto issue_back = [&](int n, int slot) {
+    if (n >= 0) {
+      double *base = wreg + slot * kB8BackSlot;
+      const double *cs = a.Cs + ((int64_t)n * P + pw) * 64 + lane * 2;
+#pragma unroll
+      for (int s = 0; s < 8; ++s)
+        if (s < nvw) b8_cp16(base + s * kB8BackRec + bpos * 2, cs + s * 64);
+      if (valid) {
+        b8_cp16(base + sw * kB8BackRec + 64 + t * 2, a.ds + ((int64_t)n * P + pw) * 8 + lane * 2);
+        if (ADJ && n > 0)
+          b8_cp16(base + 8 * kB8BackRec + sw * 8 + t * 2,
+                  a.u + ((int64_t)(n - 1) * P + pw) * 8 + lane * 2);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
   double x0, x1;
   b8_pick(dp, t, x0, x1);
   double u_nx[8], u_cu[8], u_pv[8];  // adjoint: u_{n+1}, u_n, u_{n-1}
-  auto load_u = [&](int n, double (&u)[8]) {
+  auto ldg_u = [&](int n, double (&u)[8]) {
 #pragma unroll
     for (int h = 0; h < 4; ++h) {
       const double2 v =
@@ -1188,11 +1220,6 @@ __global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double
       u[2 * h + 1] = v.y;
     }
   };
-  if (ADJ) {
-    load_u(N - 1, u_cu);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) u_nx[j] = 0.0;
-  }
   auto emit = [&](int n) {
     if (!valid) return;
     if (!ADJ) {
@@ -1200,7 +1227,6 @@ __global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double
       return;
     }
     if (a.dd) b8_stg(a.dd + vx(n) + 2 * t, x0, x1);
-    load_u(n - 1, u_pv);
     const double *us[3] = {u_pv, u_cu, u_nx};
     double *outs[3] = {a.dA, a.dB, a.dC};
 #pragma unroll
@@ -1219,36 +1245,46 @@ __global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double
       u_cu[j] = u_pv[j];
     }
   };
+  // the ring: step N-2-k in slot k % kB8Ring
+#pragma unroll
+  for (int k = 0; k < kB8Ring - 1; ++k) issue_back(N - 2 - k, k);
+  if (ADJ) {
+    ldg_u(N - 1, u_cu);
+    ldg_u(N - 2, u_pv);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) u_nx[j] = 0.0;
+  }
   emit(N - 1);
-  // C'_n (own 16 values) and d'_n (own pair) one step ahead
-  double cn[8][2], dn0 = 0.0, dn1 = 0.0;
-#pragma unroll
-  for (int r = 0; r < 8; ++r) cn[r][0] = cn[r][1] = 0.0;
-  auto load_c = [&](int n) {
-    if (n < 0 || !valid) return;
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const double2 v = b8_ldg(a.Cs + bx(n) + t * 16 + r * 2);
-      cn[r][0] = v.x;
-      cn[r][1] = v.y;
-    }
-    const double2 v = b8_ldg(a.ds + vx(n) + 2 * t);
-    dn0 = v.x;
-    dn1 = v.y;
-  };
-  load_c(N - 2);
-  for (int n = N - 2; n >= 0; --n) {
+  for (int n = N - 2, k = 0; n >= 0; --n, ++k) {
+    const int slot = k % kB8Ring;
+    issue_back(n - (kB8Ring - 1), (k + kB8Ring - 1) % kB8Ring);
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kB8Ring - 1) : "memory");
+    __syncwarp();
+    const double *rb = wreg + slot * kB8BackSlot + sw * kB8BackRec;
     double part[8];
 #pragma unroll
-    for (int r = 0; r < 8; ++r) part[r] = cn[r][0] * x0 + cn[r][1] * x1;
-    const double e0 = dn0, e1 = dn1;
-    load_c(n - 1);
+    for (int r = 0; r < 8; ++r) {
+      const double2 v = b8_lds(rb + (t * 8 + (r ^ t)) * 2);
+      part[r] = v.x * x0 + v.y * x1;
+    }
+    const double2 dv = b8_lds(rb + 64 + 2 * t);
+    if (ADJ) {
+      const double *ub = wreg + slot * kB8BackSlot + 8 * kB8BackRec + sw * 8;
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const double2 v = n > 0 ? b8_lds(ub + 2 * h) : make_double2(0.0, 0.0);
+        u_pv[2 * h] = v.x;
+        u_pv[2 * h + 1] = v.y;
+      }
+    }
+    __syncwarp();  // the slot is read: the next issue may overwrite it
     double s0, s1;
     b8_reduce_scatter(part, t, s0, s1);
-    x0 = e0 - s0;
-    x1 = e1 - s1;
+    x0 = dv.x - s0;
+    x1 = dv.y - s1;
     emit(n);
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // Dynamic shared memory of the M = 8 kernels, set once per device.
