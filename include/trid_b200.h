@@ -287,7 +287,16 @@ TRID_EXTERN_C tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const do
  *   and solves for the step RHS; transpose=1 solves with T^T (adjoint);
  *   inc=1 (axes 1, 2) adds the solution into out.
  * tridDadiLaplacianT: out += lambda * L^T g (L the interior-masked
- *   7-point Laplacian): the stencil's adjoint. */
+ *   7-point Laplacian): the stencil's adjoint.
+ * tridDadiStepVjp: the rest of one step's adjoint in one pass.  Given the
+ *   step's input u, its parts du1 = X^{-1} lambda L u, du2 = Y^{-1} du1,
+ *   du3 = Z^{-1} du2 and the transposed solves g3 = Z^{-T} ubar,
+ *   g2 = Y^{-T} g3, g1 = X^{-T} g2: ubar += lambda L^T g1 (the cotangent of
+ *   u) and *lbar += <g1, L u> - <g1, X' du1> - <g2, Y' du2> - <g3, Z' du3>,
+ *   X' = dX/dlambda (interior rows (da, db, dc): (-1/2, 1, -1/2) for the
+ *   reference coefficients, (-1, 2, -1) for the baseline ones).  lbar is
+ *   one device double, accumulated in place; the sum is formed in a fixed
+ *   order (same result on every run). */
 TRID_EXTERN_C tridStatus_t tridDadiSteps(double *u, double *work, int nx, int ny, int nz,
                                          int nsteps, double lambda, double a, double b, double c);
 TRID_EXTERN_C tridStatus_t tridSadiSteps(float *u, float *work, int nx, int ny, int nz, int nsteps,
@@ -300,6 +309,11 @@ TRID_EXTERN_C tridStatus_t tridSadiSolve(const float *rhs, float *out, int nx, i
                                          float lambda, float a, float b, float c);
 TRID_EXTERN_C tridStatus_t tridDadiLaplacianT(const double *g, double *out, int nx, int ny, int nz,
                                               double lambda);
+TRID_EXTERN_C tridStatus_t tridDadiStepVjp(const double *u, const double *du1, const double *du2,
+                                           const double *du3, const double *g1, const double *g2,
+                                           const double *g3, double *ubar, int nx, int ny, int nz,
+                                           double lambda, double da, double db, double dc,
+                                           double *lbar);
 
 /* ---- replaces trid_cuda.h:44 (a no-op in the reference, trid_cuda.cu:612) ---- */
 TRID_EXTERN_C void initTridMultiDimBatchSolve(int ndim, int *dims, int *pads);
@@ -352,7 +366,10 @@ TRID_EXTERN_C tridStatus_t tridGetDeviceErrors(unsigned *flags);
 
 /* Load an autotuning table written by tridsolver_b200.autotune (text lines
  * "<dtype> <axis class> <nmax> <method> <chunk> <sys_per_cta>", dtype f32 or
- * f64, axis class as in tridQueryMethod); NULL clears it.  Process-wide.
+ * f64, axis class as in tridQueryMethod; class 4 lines "<dtype> 4 <nmax> 2
+ * <chunk> 0" set the variable-length batch's length buckets: systems of up
+ * to nmax rows take `chunk` rows per lane, 2 up to at most 64 rows, 4 up to
+ * at most 128, else 8); NULL clears it.  Process-wide.
  * The first solve of a process also loads the file named by the environment
  * variable TRID_B200_TUNING, when set. */
 TRID_EXTERN_C tridStatus_t tridLoadTuningTable(const char *path);
@@ -360,7 +377,8 @@ TRID_EXTERN_C tridStatus_t tridLoadTuningTable(const char *path);
 /* The method/chunk/sys_per_cta the dispatcher would use for a problem:
  * dtype_bytes 4 or 8; axis class 0 = solve along axis 0 (unit stride),
  * 1 = strided solve with a row stride of at most 64 KiB, 2 = at most 1 MiB,
- * 3 = larger stride. */
+ * 3 = larger stride, 4 = a system of n rows in a variable-length batch
+ * (method 2, chunk = its rows per lane). */
 TRID_EXTERN_C tridStatus_t tridQueryMethod(int dtype_bytes, int axis, int n, int *method,
                                            int *chunk, int *sys_per_cta);
 

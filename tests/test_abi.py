@@ -211,8 +211,13 @@ def test_method_override_and_query():
         assert L.tridQueryMethod(4, cls, 256, ctypes.byref(m), ctypes.byref(ch),
                                  ctypes.byref(spc)) == 0
         assert (m.value, ch.value, spc.value) == (2, 8, 32)
-    assert L.tridQueryMethod(8, 4, 256, ctypes.byref(m), ctypes.byref(ch),
+    assert L.tridQueryMethod(8, 5, 256, ctypes.byref(m), ctypes.byref(ch),
                              ctypes.byref(spc)) == INVALID
+    # class 4: the variable-length batch's length buckets (2 / 4 / 8 rows per lane)
+    for n, want in ((8, 2), (64, 2), (65, 4), (128, 4), (129, 8), (256, 8), (5000, 8)):
+        assert L.tridQueryMethod(8, 4, n, ctypes.byref(m), ctypes.byref(ch),
+                                 ctypes.byref(spc)) == 0
+        assert (m.value, ch.value) == (2, want), n
     tb.set_method(1)
     assert L.tridQueryMethod(8, 0, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
     assert m.value == 1

@@ -61,3 +61,31 @@ def test_written_table_loads_and_steers(tmp_path):
         assert (m.value, spc.value) == (2, 16)
     finally:
         assert L.tridLoadTuningTable(None) == 0
+
+
+def test_varlen_bucket_entries_move_the_cutoffs(tmp_path):
+    """Axis-class-4 lines of a tuning table set the variable-length batch's
+    length buckets; rows per lane never exceed what 32 lanes hold."""
+    path = tmp_path / "vl.txt"
+    autotune.write_table([("f64", 4, 32, (2, 2, 0)), ("f64", 4, 200, (2, 4, 0))], str(path))
+    L = tb.lib()
+    assert L.tridLoadTuningTable(str(path).encode()) == 0
+    try:
+        m, ch, spc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        got = {}
+        for n in (8, 32, 33, 128, 129, 300):
+            assert L.tridQueryMethod(8, 4, n, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+            got[n] = ch.value
+        # 2 up to 32, 4 up to 128 (the 200 of the table is capped), then 8
+        assert got == {8: 2, 32: 2, 33: 4, 128: 4, 129: 8, 300: 8}
+        # FP32 keeps the built-in cut-offs (the table names f64 only)
+        assert L.tridQueryMethod(4, 4, 33, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+        assert ch.value == 2
+    finally:
+        assert L.tridLoadTuningTable(None) == 0
+
+
+def test_varlen_bucket_entries_validated(tmp_path):
+    path = tmp_path / "bad.txt"
+    path.write_text("f64 4 64 3 2 0\n")  # class 4 takes method 2 only
+    assert tb.lib().tridLoadTuningTable(str(path).encode()) == 3

@@ -31,6 +31,8 @@ register({
     "tridSadiSolve": (c_int, [vp, vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_flt, c_flt,
                               c_flt, c_flt]),
     "tridDadiLaplacianT": (c_int, [vp, vp, c_int, c_int, c_int, c_dbl]),
+    "tridDadiStepVjp": (c_int, [vp, vp, vp, vp, vp, vp, vp, vp, c_int, c_int, c_int, c_dbl, c_dbl,
+                                c_dbl, c_dbl, vp]),
 })
 
 COEFFS = {
@@ -109,40 +111,29 @@ class ADI:
         return du1, du2, du3
 
     # ------------------------------------------------------------ adjoint --
-    @staticmethod
-    def _lap(u):
-        out = torch.zeros_like(u)
-        out[1:-1, 1:-1, 1:-1] = (u[2:, 1:-1, 1:-1] + u[:-2, 1:-1, 1:-1] + u[1:-1, 2:, 1:-1] +
-                                 u[1:-1, :-2, 1:-1] + u[1:-1, 1:-1, 2:] + u[1:-1, 1:-1, :-2] -
-                                 6.0 * u[1:-1, 1:-1, 1:-1])
-        return out
-
-    def _dop(self, v, axis):
-        """(dT/dlambda) v along a torch axis (2 = x, 1 = y, 0 = z), interior rows."""
-        out = torch.zeros_like(v)
-        ii = (slice(1, -1),) * 3
-        lo = list(ii)
-        hi = list(ii)
-        lo[axis] = slice(0, -2)
-        hi[axis] = slice(2, None)
-        out[ii] = self.da * v[tuple(lo)] + self.db * v[ii] + self.dc * v[tuple(hi)]
-        return out
-
-    def step_vjp(self, u, ubar):
-        """Cotangents of (u, lambda) for one step u' = u + du3, given ubar = dL/du'."""
+    def _step_vjp_into(self, u, ubar, lbar):
+        """One step's adjoint: ubar (the cotangent of the step's output) is
+        replaced by the cotangent of its input u and the lambda cotangent is
+        added into the device scalar lbar.  Six solves (the step's three
+        parts, then the three transposed solves) and one fused pass
+        (tridDadiStepVjp)."""
+        if self.dtype != torch.float64:
+            raise TypeError("the ADI adjoint runs in float64")
         du1, du2, du3 = self.parts(u)
         g3 = self._solve(ubar, torch.empty_like(u), 2, transpose=1)
         g2 = self._solve(g3, torch.empty_like(u), 1, transpose=1)
         g1 = self._solve(g2, torch.empty_like(u), 0, transpose=1)
-        uprev = ubar.clone()
         L = lib()
         _bind_stream(L)
-        _check(L.tridDadiLaplacianT(_ptr(g1), _ptr(uprev), self.nx, self.ny, self.nz, self.lam),
-               "tridDadiLaplacianT")
-        lbar = (torch.dot(g1.reshape(-1), self._lap(u).reshape(-1))
-                - torch.dot(g1.reshape(-1), self._dop(du1, 2).reshape(-1))
-                - torch.dot(g2.reshape(-1), self._dop(du2, 1).reshape(-1))
-                - torch.dot(g3.reshape(-1), self._dop(du3, 0).reshape(-1)))
+        _check(L.tridDadiStepVjp(_ptr(u), _ptr(du1), _ptr(du2), _ptr(du3), _ptr(g1), _ptr(g2),
+                                 _ptr(g3), _ptr(ubar), self.nx, self.ny, self.nz, self.lam,
+                                 self.da, self.db, self.dc, _ptr(lbar)), "tridDadiStepVjp")
+        return ubar
+
+    def step_vjp(self, u, ubar):
+        """Cotangents of (u, lambda) for one step u' = u + du3, given ubar = dL/du'."""
+        lbar = torch.zeros((), dtype=u.dtype, device=u.device)
+        uprev = self._step_vjp_into(u, ubar.clone(), lbar)
         return uprev, lbar
 
     def grad_final_norm(self, u0, nsteps, every=20):
@@ -167,6 +158,5 @@ class ADI:
                 self.step(nxt)
                 states.append(nxt)
             for t in reversed(range(t1 - t0)):
-                ubar, lb = self.step_vjp(states[t], ubar)
-                lbar = lbar + lb
+                self._step_vjp_into(states[t], ubar, lbar)
         return loss, ubar, lbar

@@ -19,7 +19,12 @@ Candidates (see tridSetMethod in include/trid_b200.h):
     method 6, chunk     axis 0, longer systems: one CTA per system, 4/8/16
                         rows per thread (up to 4096 rows)
     (method 2 above 512 rows on axis 0 also means the blocked partition:
-    block reduction, recursive block solve, block finish)
+    block reduction, recursive block solve, block finish; its chunk 8 or 16
+    is the block size, 256 or 512 rows, swept for lengths past 4096)
+
+Axis class 4 is the variable-length batch: its length buckets (2 rows per
+lane up to m2max rows, 4 up to m4max, else 8) are swept on a batch of short
+systems (lengths log-uniform on [8, 256]) and written as class-4 lines.
 
 --stride-sweep instead times the default algorithm on FP64 problems of
 64 M unknowns whose solve axis has plane strides from 8 KiB to 2 MiB, against
@@ -74,8 +79,86 @@ def candidates(axis, n):
             for ch in (4, 8, 16):
                 out.append((6, ch, 0))
         if not ch0:
-            out.append((2, 8, 0))  # blocked partition, 256-row blocks
+            out.append((2, 8, 0))   # blocked partition, 256-row blocks
+            out.append((2, 16, 0))  # 512-row blocks
+    if axis > 0 and not ch0:
+        # strided systems past 512 rows: the blocked partition, 256- or
+        # 512-row blocks, 8 or 16 systems per CTA
+        for ch in (8, 16):
+            for spc in (8, 16):
+                out.append((2, ch, spc))
     return out
+
+
+# (m2max, m4max) settings of the variable-length buckets
+VARLEN_BUCKETS = ((64, 128), (32, 128), (0, 128), (64, 64), (32, 64), (0, 0))
+
+
+def varlen_entries(dt, m2max, m4max):
+    """Class-4 table lines for the bucket cut-offs (m2max, m4max)."""
+    out = []
+    if m2max:
+        out.append((dt, 4, m2max, (2, 2, 0)))
+    if m4max > m2max:
+        out.append((dt, 4, m4max, (2, 4, 0)))
+    out.append((dt, 4, 256, (2, 8, 0)))
+    return out
+
+
+def tune_varlen(dt, nsys=400_000, reps=10, verbose=True, seed=3):
+    """Time every bucket setting on one batch of short systems; returns the
+    winning table lines and the timings."""
+    import os
+    import tempfile
+
+    import torch
+
+    from .varlen import solve_varlen
+
+    tdtype = torch.float64 if dt == "f64" else torch.float32
+    rng = np.random.default_rng(seed)
+    lens = np.floor(np.exp(rng.uniform(np.log(8), np.log(256), nsys))).astype(np.int64)
+    off = torch.from_numpy(np.concatenate([[0], np.cumsum(lens)])).cuda()
+    total = int(lens.sum())
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    a = torch.rand(total, device="cuda", dtype=tdtype, generator=g) * 2 - 1
+    c = torch.rand(total, device="cuda", dtype=tdtype, generator=g) * 2 - 1
+    b = a.abs() + c.abs() + 1 + torch.rand(total, device="cuda", dtype=tdtype, generator=g)
+    d = torch.randn(total, device="cuda", dtype=tdtype, generator=g)
+    L = lib()
+    report, best = [], None
+    fd, path = tempfile.mkstemp(suffix=".txt")
+    os.close(fd)
+    try:
+        for m2, m4 in VARLEN_BUCKETS:
+            entries = varlen_entries(dt, m2, m4)
+            write_table(entries, path)
+            if L.tridLoadTuningTable(path.encode()) != 0:
+                raise TridError(3, "tridLoadTuningTable")
+            x = d.clone()
+            for _ in range(3):
+                solve_varlen(a, b, c, x, off, total)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                solve_varlen(a, b, c, x, off, total)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            gbs = (5 * tdtype.itemsize * total + 8 * (nsys + 1)) / (ms * 1e-3) / 1e9
+            report.append({"dtype": dt, "axis": 4, "m2max": m2, "m4max": m4, "ms": ms,
+                           "GBs": round(gbs, 1)})
+            if verbose:
+                print(f"{dt} varlen m2max={m2:3d} m4max={m4:3d}: {ms:.4f} ms {gbs:8.1f} GB/s",
+                      file=sys.stderr)
+            if best is None or ms < best[0]:
+                best = (ms, entries)
+    finally:
+        L.tridLoadTuningTable(None)
+        os.unlink(path)
+    return best[1], report
 
 
 def problem_dims(axis, n, elems):
@@ -131,6 +214,11 @@ def tune(dtypes=("f64", "f32"), lengths=(32, 64, 128, 256, 512), elems=1 << 24, 
     for dt in dtypes:
         tdtype = torch.float64 if dt == "f64" else torch.float32
         for axis in classes:
+            if axis == 4:
+                entries, rep = tune_varlen(dt, verbose=verbose)
+                table.extend((e[0], e[1], e[2], e[3]) for e in entries)
+                report.extend(rep)
+                continue
             for n in lengths:
                 dims, sd = problem_dims(axis, n, elems)
                 best = None
@@ -182,9 +270,10 @@ def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--out", default="tuning_b200.txt")
     ap.add_argument("--dtypes", default="f64,f32")
-    ap.add_argument("--lengths", default="32,64,128,256,512")
+    ap.add_argument("--lengths", default="32,64,128,256,512,1024,4096,65536")
     ap.add_argument("--elems", type=int, default=1 << 24)
-    ap.add_argument("--classes", default="0,1,2", help="axis classes to sweep (0-3)")
+    ap.add_argument("--classes", default="0,1,2,4",
+                    help="axis classes to sweep (0-3 strided-batch strides, 4 variable-length)")
     ap.add_argument("--report", default=None, help="also write every timing as JSON")
     ap.add_argument("--stride-sweep", action="store_true",
                     help="only time strided solves against the plane stride")

@@ -102,8 +102,11 @@ static tridStatus_t parse_tuning_table(const char *path, std::vector<TuneEntry> 
     e.dtype_bytes = (strcmp(dt, "f64") == 0) ? 8 : (strcmp(dt, "f32") == 0 ? 4 : 0);
     const bool chunk_ok = e.chunk == 0 || e.chunk == 2 || e.chunk == 4 || e.chunk == 8 || e.chunk == 16;
     const bool spc_ok = e.spc == 0 || e.spc == 4 || e.spc == 8 || e.spc == 16 || e.spc == 32;
+    // axis class 4: the variable-length batch's length buckets (method 2,
+    // chunk 2/4/8 for the lengths up to nmax)
+    const bool vl_ok = e.axis != 4 || (e.method == 2 && e.chunk >= 2 && e.chunk <= 8);
     if (e.dtype_bytes == 0 || e.method < 1 || e.method > 6 || e.method == 4 || e.method == 5 ||
-        e.axis < 0 || e.axis > 3 ||
+        e.axis < 0 || e.axis > 4 || !vl_ok ||
         !chunk_ok || !spc_ok) {
       fclose(f);
       return TRID_STATUS_INVALID_VALUE;
@@ -135,6 +138,32 @@ static int chunk_for(int n, int dtype_bytes) {
   if (n <= 256) return 8;
   if (n <= 512) return 16;
   return 0;  // too long for a register-resident partition
+}
+
+// Length buckets of the variable-length batch: systems of at most m2max rows
+// take 2 rows per lane, at most m4max 4, longer ones 8 (64 / 128 built in).
+// A tuning table's axis-class-4 entries (lengths up to nmax use `chunk`)
+// move the cut-offs: the leading run of chunk-2 entries sets m2max (at most
+// 64 rows fit), the chunk-4 entries after it m4max (at most 128).
+void varlen_buckets(int dtype_bytes, int &m2max, int &m4max) {
+  std::call_once(g_env_tune_once, load_env_tuning);
+  m2max = 64;
+  m4max = 128;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  bool any = false;
+  int a2 = 0, a4 = 0, stage = 2;
+  for (const TuneEntry &e : g_tune) {  // sorted by nmax
+    if (e.dtype_bytes != dtype_bytes || e.axis != 4) continue;
+    any = true;
+    if (e.chunk < stage) continue;  // not monotone: ignored
+    stage = e.chunk;
+    if (e.chunk == 2) a2 = std::min(e.nmax, 64);
+    if (e.chunk == 4) a4 = std::min(e.nmax, 128);
+  }
+  if (any) {
+    m2max = a2;
+    m4max = std::max(a2, a4);
+  }
 }
 
 MethodChoice choose_method(int dtype_bytes, int axis, int n, int opt_hint) {
@@ -705,9 +734,17 @@ extern "C" tridStatus_t tridLoadTuningTable(const char *path) {
 
 extern "C" tridStatus_t tridQueryMethod(int dtype_bytes, int axis, int n, int *method, int *chunk,
                                         int *sys_per_cta) {
-  if ((dtype_bytes != 4 && dtype_bytes != 8) || axis < 0 || axis > 3 || n < 0 || !method ||
+  if ((dtype_bytes != 4 && dtype_bytes != 8) || axis < 0 || axis > 4 || n < 0 || !method ||
       !chunk || !sys_per_cta)
     return TRID_STATUS_INVALID_VALUE;
+  if (axis == 4) {  // the variable-length batch's bucket for a system of n rows
+    int m2 = 0, m4 = 0;
+    varlen_buckets(dtype_bytes, m2, m4);
+    *method = 2;
+    *chunk = n <= m2 ? 2 : (n <= m4 ? 4 : 8);
+    *sys_per_cta = 0;
+    return TRID_STATUS_SUCCESS;
+  }
   const MethodChoice m = choose_method(dtype_bytes, axis, n, 0);
   *method = m.method;
   *chunk = m.chunk;

@@ -190,6 +190,81 @@ __global__ void adi_lt_kernel(AdiArgs<T> g, const T *__restrict__ gin) {
   }
 }
 
+// Cotangent of one step's lambda and the u-cotangent's Laplacian term, in one
+// pass.  With du1 = X^{-1} r, du2 = Y^{-1} du1, du3 = Z^{-1} du2 (r = lam L u)
+// and g3 = Z^{-T} ubar, g2 = Y^{-T} g3, g1 = X^{-T} g2:
+//     ubar_prev = ubar + lam L^T g1
+//     dL/dlam  += <g1, L u> - <g1, X' du1> - <g2, Y' du2> - <g3, Z' du3>
+// with X' = dX/dlam the interior rows (da, db, dc) along x (Y', Z' along y,
+// z; face rows are identity and do not depend on lam).  Each CTA writes its
+// partial sum of the lam term; adi_vjp_sum_kernel adds the partials in a
+// fixed order (the result does not depend on scheduling).
+template <typename T>
+struct AdiVjpArgs {
+  int nx, ny, nz;
+  T lam, da, db, dc;
+  const T *u, *du1, *du2, *du3, *g1, *g2, *g3;
+  T *ubar;      // in: cotangent of the step's output; out: of its input
+  T *partial;   // one per CTA
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) adi_vjp_kernel(AdiVjpArgs<T> v) {
+  __shared__ T red[8];
+  const int64_t total = (int64_t)v.nx * v.ny * v.nz;
+  const int64_t sx = 1, sy = v.nx, sz = (int64_t)v.nx * v.ny;
+  AdiArgs<T> g = {v.nx, v.ny, v.nz, v.lam, T(0), T(1), T(0), nullptr, nullptr};
+  T acc = T(0);
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < total;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(p % v.nx), j = (int)((p / v.nx) % v.ny), k = (int)(p / sz);
+    const bool in = adi_inside(g, i, j, k);
+    const T g1 = v.g1[p];
+    // (L^T g1)_p
+    T lt = in ? T(-6) * g1 : T(0);
+    if (i > 0 && adi_inside(g, i - 1, j, k)) lt += v.g1[p - sx];
+    if (i < v.nx - 1 && adi_inside(g, i + 1, j, k)) lt += v.g1[p + sx];
+    if (j > 0 && adi_inside(g, i, j - 1, k)) lt += v.g1[p - sy];
+    if (j < v.ny - 1 && adi_inside(g, i, j + 1, k)) lt += v.g1[p + sy];
+    if (k > 0 && adi_inside(g, i, j, k - 1)) lt += v.g1[p - sz];
+    if (k < v.nz - 1 && adi_inside(g, i, j, k + 1)) lt += v.g1[p + sz];
+    v.ubar[p] += v.lam * lt;
+    if (in) {
+      const T lu = v.u[p - sx] + v.u[p + sx] + v.u[p - sy] + v.u[p + sy] + v.u[p - sz] +
+                   v.u[p + sz] - T(6) * v.u[p];
+      const T xd = v.da * v.du1[p - sx] + v.db * v.du1[p] + v.dc * v.du1[p + sx];
+      const T yd = v.da * v.du2[p - sy] + v.db * v.du2[p] + v.dc * v.du2[p + sy];
+      const T zd = v.da * v.du3[p - sz] + v.db * v.du3[p] + v.dc * v.du3[p + sz];
+      acc += g1 * (lu - xd) - v.g2[p] * yd - v.g3[p] * zd;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    T s = T(0);
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    v.partial[blockIdx.x] = s;
+  }
+}
+
+// *lbar += sum of the n partials, in a fixed order
+template <typename T>
+__global__ void __launch_bounds__(256) adi_vjp_sum_kernel(const T *__restrict__ partial, int n,
+                                                          T *lbar) {
+  __shared__ T red[256];
+  T s = T(0);
+  for (int q = threadIdx.x; q < n; q += 256) s += partial[q];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *lbar += red[0];
+}
+
 // ------------------------------------------------------------- launchers --
 template <typename T, int M>
 static cudaError_t adi_x_m(const AdiArgs<T> &g, bool stencil, bool trans, bool inc,
@@ -261,6 +336,18 @@ cudaError_t adi_lt(const AdiArgs<T> &g, const T *gin, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t adi_vjp(AdiVjpArgs<T> v, T *lbar, cudaStream_t st) {
+  const int64_t total = (int64_t)v.nx * v.ny * v.nz;
+  int64_t blocks = (total + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  v.partial = (T *)scratch((size_t)blocks * sizeof(T), 0);
+  if (!v.partial) return cudaErrorMemoryAllocation;
+  adi_vjp_kernel<T><<<dim3((unsigned)blocks), dim3(256), 0, st>>>(v);
+  adi_vjp_sum_kernel<T><<<1, 256, 0, st>>>(v.partial, (int)blocks, lbar);
+  return cudaGetLastError();
+}
+
 }  // namespace tridb200
 
 using namespace tridb200;
@@ -328,4 +415,19 @@ extern "C" tridStatus_t tridDadiLaplacianT(const double *g, double *out, int nx,
   AdiArgs<double> a = {nx, ny, nz, lambda, 0.0, 1.0, 0.0, nullptr, out};
   return adi_lt<double>(a, g, current_stream()) == cudaSuccess ? TRID_STATUS_SUCCESS
                                                                : TRID_STATUS_EXECUTION_FAILED;
+}
+
+extern "C" tridStatus_t tridDadiStepVjp(const double *u, const double *du1, const double *du2,
+                                        const double *du3, const double *g1, const double *g2,
+                                        const double *g3, double *ubar, int nx, int ny, int nz,
+                                        double lambda, double da, double db, double dc,
+                                        double *lbar) {
+  if (!adi_dims_ok(nx, ny, nz) || !u || !du1 || !du2 || !du3 || !g1 || !g2 || !g3 || !ubar ||
+      !lbar)
+    return TRID_STATUS_INVALID_VALUE;
+  AdiVjpArgs<double> v = {nx, ny, nz, lambda, da, db, dc, u, du1, du2, du3, g1, g2, g3, ubar,
+                          nullptr};
+  const cudaError_t e = adi_vjp<double>(v, lbar, current_stream());
+  if (e == cudaErrorMemoryAllocation) return TRID_STATUS_ALLOC_FAILED;
+  return e == cudaSuccess ? TRID_STATUS_SUCCESS : TRID_STATUS_EXECUTION_FAILED;
 }

@@ -227,6 +227,7 @@ struct VLArgs {
   int64_t nsys;
   int64_t total;
   int64_t cap;               // entries of item_sys / fitem_sys / block rows
+  int m2max, m4max;          // length buckets: 2 rows per lane up to m2max, 4 up to m4max
   unsigned *sys_count;
   unsigned long long *queue;  // [0] reduce queue, [1] finish queue
   T *rows;       // per reduce item: the block's 8 row values; later its 2 unknowns
@@ -399,9 +400,9 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
     }
     if (len == 0) continue;
     if (len <= kVLShort) {
-      if (len <= 64)
+      if (len <= A.m2max)
         vl_short<T, 2>(A, reg, lo, len, lane, between);
-      else if (len <= 128)
+      else if (len <= A.m4max)
         vl_short<T, 4>(A, reg, lo, len, lane, between);
       else
         vl_short<T, 8>(A, reg, lo, len, lane, between);
@@ -546,6 +547,7 @@ cudaError_t launch_varlen(const T *a, const T *b, const T *c, T *d, const int64_
   A.nsys = nsys;
   A.total = total;
   A.cap = max_items;
+  varlen_buckets((int)sizeof(T), A.m2max, A.m4max);
   A.item_off = (int64_t *)w;
   A.fitem_off = (int64_t *)(w + al(b_off));
   A.sys_count = (unsigned *)(w + 2 * al(b_off));
@@ -697,6 +699,7 @@ extern "C" tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const doubl
   A.nsys = nsys;
   A.total = total;
   A.cap = varlen_cap(nsys, total);
+  varlen_buckets((int)sizeof(double), A.m2max, A.m4max);
   A.err = (unsigned *)(w + off[0]);
   A.item_off = (int64_t *)(w + off[1]);
   A.fitem_off = (int64_t *)(w + off[1] + (off[2] - off[1]) / 2);

@@ -124,6 +124,9 @@ unsigned *device_error_flags();
 // The same word when it exists already on the current device (nullptr if no
 // kernel has needed it yet); never allocates.
 unsigned *device_error_flags_if_present();
+// Length-bucket cut-offs of the variable-length batch (api_scalar.cu): rows
+// per lane 2 up to m2max, 4 up to m4max, else 8; from the tuning table.
+void varlen_buckets(int dtype_bytes, int &m2max, int &m4max);
 // The allocation-free varlen solve's own error word on the current device
 // (kern_varlen.cu), nullptr until that entry point has run there.
 unsigned *noalloc_error_word();
