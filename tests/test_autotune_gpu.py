@@ -32,7 +32,8 @@ def test_sweep_writes_a_table_that_steers_dispatch(tmp_path):
     table, report = autotune.tune(dtypes=("f64",), lengths=(64, 128), elems=1 << 21,
                                   verbose=False, classes=(1,))
     assert [(t[0], t[1], t[2]) for t in table] == [("f64", 1, 64), ("f64", 1, 128)]
-    assert len(report) == sum(len(autotune.candidates(1, n)) for n in (64, 128))
+    # every candidate plus the built-in choice of each bucket
+    assert len(report) == sum(len(autotune.candidates(1, n)) + 1 for n in (64, 128))
     path = tmp_path / "tuning.txt"
     autotune.write_table(table, str(path))
     assert L.tridLoadTuningTable(str(path).encode()) == 0

@@ -222,6 +222,11 @@ def tune(dtypes=("f64", "f32"), lengths=(32, 64, 128, 256, 512), elems=1 << 24, 
             for n in lengths:
                 dims, sd = problem_dims(axis, n, elems)
                 best = None
+                # the built-in choice, for comparison (not a table candidate)
+                ms = time_candidate(torch, tdtype, dims, sd, (0, 0, 0))
+                report.append({"dtype": dt, "axis": axis, "n": n, "method": "built-in", "ms": ms,
+                               "GBs": round(5 * tdtype.itemsize * int(np.prod(dims)) /
+                                            (ms * 1e-3) / 1e9, 1)})
                 for m in candidates(axis, n):
                     ms = time_candidate(torch, tdtype, dims, sd, m)
                     gbs = 5 * tdtype.itemsize * int(np.prod(dims)) / (ms * 1e-3) / 1e9

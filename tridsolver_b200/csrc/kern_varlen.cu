@@ -282,32 +282,13 @@ __device__ __forceinline__ void vl_read(const T *reg, int64_t rb, int64_t len, i
   }
 }
 
-// L2 bulk prefetch of rows [first, first+count) of a, b, c, d, widened to
-// 16-byte units that stay inside the arrays (whose bases must then be 16-byte
-// aligned; otherwise nothing is prefetched: it is only a hint)
-template <typename T>
-__device__ __forceinline__ void vl_prefetch_rows(const VLArgs<T> &A, int64_t first, int64_t count) {
-  const T *base[4] = {A.a, A.b, A.c, A.d};
-  const int64_t end = (A.total * (int64_t)sizeof(T)) & ~(int64_t)15;
-  int64_t b0 = (first * (int64_t)sizeof(T)) & ~(int64_t)15;
-  int64_t b1 = ((first + count) * (int64_t)sizeof(T) + 15) & ~(int64_t)15;
-  if (b1 > end) b1 = end;
-  if (b1 <= b0) return;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (((uintptr_t)base[k] & 15) != 0) continue;
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
-                     reinterpret_cast<const char *>(base[k]) + b0),
-                 "r"((uint32_t)(b1 - b0))
-                 : "memory");
-  }
-}
-
-// this lane's solution rows through the d region, coalesced to d
+// this lane's solution rows through the warp's store region (the fifth),
+// coalesced to d; the four staging regions may already hold the next item's
+// copies in flight
 template <typename T, int M>
 __device__ __forceinline__ void vl_store(const VLArgs<T> &A, T *reg, int64_t lo, int64_t rb,
                                          int64_t len, int lane, const T (&x)[M]) {
-  T *rd = reg + 3 * kVLRegion;
+  T *rd = reg + 4 * kVLRegion;
   const int ts = lane * (M + 1);
 #pragma unroll
   for (int j = 0; j < M; ++j) rd[ts + j] = x[j];  // d slots read only by this lane
@@ -317,37 +298,7 @@ __device__ __forceinline__ void vl_store(const VLArgs<T> &A, T *reg, int64_t lo,
     const int q = j * kWarp + lane;
     if (rb + q < len) A.d[lo + rb + q] = rd[q + q / M];
   }
-  __syncwarp();  // the regions are reused by the warp's next item
-}
-
-// `between` runs while the item's rows are in flight (it warms the next item)
-template <typename T, int M, typename Fn>
-__device__ __forceinline__ void vl_short(const VLArgs<T> &A, T *reg, int64_t lo, int64_t len,
-                                         int lane, Fn &&between) {
-  T al[M], be[M], ga[M], de[M];
-  vl_issue<T, M>(A, reg, lo, 0, len, lane);
-  between();
-  vl_read<T, M>(reg, 0, len, lane, al, be, ga, de);
-  Row<T> F, L;
-  chunk_reduce<T, M>(al, be, ga, de, F, L);
-  T xF, xL;
-  warp_interface_solve(F, L, xF, xL, lane);
-  chunk_backsub<T, M>(al, ga, de, xF, xL);
-  vl_store<T, M>(A, reg, lo, 0, len, lane, de);
-}
-
-// one block of a long system: chunk reduction + block basis
-template <typename T, typename Fn>
-__device__ __forceinline__ void vl_block(const VLArgs<T> &A, T *reg, int64_t lo, int64_t len,
-                                         int blk, int lane, T (&al)[8], T (&ga)[8], T (&de)[8],
-                                         Row<T> &F, Row<T> &L, T (&bF)[3], T (&bL)[3],
-                                         Fn &&between) {
-  T be[8];
-  vl_issue<T, 8>(A, reg, lo, (int64_t)blk * kVLBlock, len, lane);
-  between();
-  vl_read<T, 8>(reg, (int64_t)blk * kVLBlock, len, lane, al, be, ga, de);
-  chunk_reduce<T, 8>(al, be, ga, de, F, L);
-  warp_block_basis(F, L, lane, bF, bL);
+  __syncwarp();  // the store region is reused by the warp's next item
 }
 
 __device__ __forceinline__ unsigned vl_load_acquire(const unsigned *p) {
@@ -356,142 +307,222 @@ __device__ __forceinline__ unsigned vl_load_acquire(const unsigned *p) {
   return v;
 }
 
+// One work item as a warp sees it: the rows of system s to stage (a whole
+// short system, or block `blk` of a long one) and the rows per lane m.
+struct VLItem {
+  int64_t s;    // system, -1: nothing to do
+  int64_t lo;   // first row of the system
+  int64_t len;  // rows of the system
+  int blk;      // block of a long system, -1: the whole (short) system
+  int m;        // rows per lane of the staging: 2, 4 or 8
+};
+
+template <typename T>
+__device__ __forceinline__ void vl_issue_item(const VLArgs<T> &A, T *reg, const VLItem &d,
+                                              int lane) {
+  if (d.s < 0) return;
+  const int64_t rb = d.blk < 0 ? 0 : (int64_t)d.blk * kVLBlock;
+  if (d.m == 2)
+    vl_issue<T, 2>(A, reg, d.lo, rb, d.len, lane);
+  else if (d.m == 4)
+    vl_issue<T, 4>(A, reg, d.lo, rb, d.len, lane);
+  else
+    vl_issue<T, 8>(A, reg, d.lo, rb, d.len, lane);
+}
+
+// reduce-queue item `it` (every lane computes the same descriptor); records
+// malformed offsets and over-long systems once
+template <typename T>
+__device__ __forceinline__ VLItem vl_reduce_item(const VLArgs<T> &A, int64_t it, int64_t nitems,
+                                                 int lane) {
+  VLItem d = {-1, 0, 0, -1, 8};
+  if (it >= nitems) return d;
+  const int64_t s = A.item_sys[it];
+  if (s < 0) return d;  // skipped by the preparation (past cap)
+  const int64_t lo = A.offsets[s], hi = A.offsets[s + 1];
+  if (vl_bad(lo, hi, A.total)) {
+    if (lane == 0) atomicOr(A.err, kErrBadOffsets);
+    return d;
+  }
+  const int64_t len = hi - lo;
+  if (len == 0) return d;
+  if (len <= kVLShort) {
+    d.m = len <= A.m2max ? 2 : (len <= A.m4max ? 4 : 8);
+  } else {
+    const int64_t nblk = (len + kVLBlock - 1) / kVLBlock;
+    if (nblk > kVLMaxBlocks) {
+      if (lane == 0 && it == A.item_off[s]) atomicOr(A.err, kErrTooLong);
+      return d;
+    }
+    d.blk = (int)(it - A.item_off[s]);
+  }
+  d.s = s;
+  d.lo = lo;
+  d.len = len;
+  return d;
+}
+
+template <typename T>
+__device__ __forceinline__ VLItem vl_finish_item(const VLArgs<T> &A, int64_t fi, int64_t nf) {
+  VLItem d = {-1, 0, 0, -1, 8};
+  if (fi >= nf) return d;
+  const int64_t s = A.fitem_sys[fi];
+  if (s < 0) return d;
+  d.s = s;
+  d.lo = A.offsets[s];
+  d.len = A.offsets[s + 1] - d.lo;
+  d.blk = (int)(fi - A.fitem_off[s]);
+  return d;
+}
+
+// a whole short system: rows already staged; the next item's copies go out
+// as soon as the rows are in registers
+template <typename T, int M>
+__device__ __forceinline__ void vl_short_solve(const VLArgs<T> &A, T *reg, const VLItem &cur,
+                                               const VLItem &nxt, int lane) {
+  T al[M], be[M], ga[M], de[M];
+  vl_read<T, M>(reg, 0, cur.len, lane, al, be, ga, de);
+  vl_issue_item(A, reg, nxt, lane);
+  Row<T> F, L;
+  chunk_reduce<T, M>(al, be, ga, de, F, L);
+  T xF, xL;
+  warp_interface_solve(F, L, xF, xL, lane);
+  chunk_backsub<T, M>(al, ga, de, xF, xL);
+  vl_store<T, M>(A, reg, cur.lo, 0, cur.len, lane, de);
+}
+
+// Both queues are software-pipelined per warp: lane 0 claims the next item
+// while the current one is staged; once the current item's rows are in
+// registers the next item's copies are issued into the same staging
+// regions, so they are in flight while the current item is solved and
+// stored (stores go through a fifth region).
 template <typename T>
 __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
   extern __shared__ __align__(16) unsigned char vl_dyn[];
   const int lane = threadIdx.x & (kWarp - 1);
-  T *reg = reinterpret_cast<T *>(vl_dyn) + (size_t)(threadIdx.x / kWarp) * 4 * kVLRegion;
+  T *reg = reinterpret_cast<T *>(vl_dyn) + (size_t)(threadIdx.x / kWarp) * 5 * kVLRegion;
   // the prefixes can pass cap only for non-monotone offsets; the systems past
   // it were skipped by the preparation
   const int64_t nitems = A.item_off[A.nsys] < A.cap ? A.item_off[A.nsys] : A.cap;
   const int64_t nf = A.fitem_off[A.nsys] < A.cap ? A.fitem_off[A.nsys] : A.cap;
-  // Both queues are software-pipelined: lane 0 claims the next item one
-  // iteration ahead and, while the current item's rows are in flight, looks
-  // up the next item's rows and warms L2 with them.
-  auto warm = [&](unsigned long long nx, int64_t nlimit, const int *tsys,
-                  const int64_t *toff, bool long_only) {
-    if (lane != 0 || (int64_t)nx >= nlimit) return;
-    const int64_t s2 = tsys[nx];
-    if (s2 < 0) return;
-    const int64_t lo2 = A.offsets[s2], hi2 = A.offsets[s2 + 1];
-    if (vl_bad(lo2, hi2, A.total) || hi2 == lo2) return;
-    int64_t first = lo2, cnt = hi2 - lo2;
-    if (long_only || cnt > kVLShort) {
-      first = lo2 + ((int64_t)nx - toff[s2]) * kVLBlock;
-      cnt = hi2 - first < kVLBlock ? hi2 - first : kVLBlock;
-    }
-    if (cnt > 0) vl_prefetch_rows(A, first, cnt);
-  };
   // ---- reduce queue ----
-  unsigned long long nit = 0;  // lane 0: the next claimed reduce item
-  if (lane == 0) nit = atomicAdd(&A.queue[0], 1ull);
-  for (;;) {
-    const unsigned long long it = __shfl_sync(0xffffffffu, nit, 0);
-    if ((int64_t)it >= nitems) break;
-    if (lane == 0) nit = atomicAdd(&A.queue[0], 1ull);
-    auto between = [&]() { warm(nit, nitems, A.item_sys, A.item_off, false); };
-    const int64_t s = A.item_sys[it];
-    if (s < 0) continue;  // skipped by the preparation (past cap)
-    const int64_t lo = A.offsets[s], hi = A.offsets[s + 1];
-    const int64_t len = hi - lo;
-    if (vl_bad(lo, hi, A.total)) {
-      if (lane == 0) atomicOr(A.err, kErrBadOffsets);
-      continue;
-    }
-    if (len == 0) continue;
-    if (len <= kVLShort) {
-      if (len <= A.m2max)
-        vl_short<T, 2>(A, reg, lo, len, lane, between);
-      else if (len <= A.m4max)
-        vl_short<T, 4>(A, reg, lo, len, lane, between);
+  unsigned long long claim = 0;
+  if (lane == 0) claim = atomicAdd(&A.queue[0], 1ull);
+  int64_t it = (int64_t)__shfl_sync(0xffffffffu, claim, 0);
+  VLItem cur = vl_reduce_item(A, it, nitems, lane);
+  vl_issue_item(A, reg, cur, lane);
+  while (it < nitems) {
+    if (lane == 0) claim = atomicAdd(&A.queue[0], 1ull);
+    const int64_t nit = (int64_t)__shfl_sync(0xffffffffu, claim, 0);
+    const VLItem nxt = vl_reduce_item(A, nit, nitems, lane);
+    if (cur.s < 0) {
+      vl_issue_item(A, reg, nxt, lane);
+    } else if (cur.blk < 0) {
+      if (cur.m == 2)
+        vl_short_solve<T, 2>(A, reg, cur, nxt, lane);
+      else if (cur.m == 4)
+        vl_short_solve<T, 4>(A, reg, cur, nxt, lane);
       else
-        vl_short<T, 8>(A, reg, lo, len, lane, between);
-      continue;
-    }
-    const int nblk = (int)((len + kVLBlock - 1) / kVLBlock);
-    if (nblk > kVLMaxBlocks) {
-      if (lane == 0 && it == (unsigned long long)A.item_off[s]) atomicOr(A.err, kErrTooLong);
-      continue;
-    }
-    const int blk = (int)((int64_t)it - A.item_off[s]);
-    T al[8], ga[8], de[8], bF[3], bL[3];
-    Row<T> F, L, FB, LB;
-    vl_block<T>(A, reg, lo, len, blk, lane, al, ga, de, F, L, bF, bL, between);
-    block_rows(F, L, bF, bL, lane, FB, LB);
-    T *rw = A.rows + ((int64_t)A.item_off[s] + blk) * 8;
-    if (lane == 0) {
-      rw[0] = FB.a; rw[1] = FB.b; rw[2] = FB.c; rw[3] = FB.d;
-      rw[4] = LB.a; rw[5] = LB.b; rw[6] = LB.c; rw[7] = LB.d;
-    }
-    __threadfence();  // publish the block rows before counting the block done
-    unsigned done = 0;
-    if (lane == 0) done = atomicAdd(&A.sys_count[s], 1u);
-    done = __shfl_sync(0xffffffffu, done, 0);
-    if (done != (unsigned)(nblk - 1)) continue;
-    __threadfence();  // every block's rows are visible to this warp now
-    // the block system of s: lane t holds block t's two rows
-    T *rs = A.rows + (int64_t)A.item_off[s] * 8;
-    Row<T> RF{T(0), T(1), T(0), T(0)}, RL{T(0), T(1), T(0), T(0)};
-    if (lane < nblk) {
-      const T *q = rs + (int64_t)lane * 8;
-      RF = {__ldcg(q + 0), __ldcg(q + 1), __ldcg(q + 2), __ldcg(q + 3)};
-      RL = {__ldcg(q + 4), __ldcg(q + 5), __ldcg(q + 6), __ldcg(q + 7)};
-    }
-    T fB, lB;
-    int span = 1;
-    while (span < nblk) span <<= 1;
-    warp_interface_solve(RF, RL, fB, lB, lane, span);
-    __syncwarp();  // all block rows read before they are overwritten
-    if (lane < nblk) {
-      rs[(int64_t)lane * 8 + 0] = fB;  // block t's boundary unknowns
-      rs[(int64_t)lane * 8 + 1] = lB;
-    }
-    __threadfence();
-    __syncwarp();
-    if (lane == 0) atomicOr(&A.sys_count[s], kVLSolved);
-  }
-  // ---- finish queue ----
-  unsigned long long nfi = 0;  // lane 0: the next claimed finish item
-  if (lane == 0) nfi = atomicAdd(&A.queue[1], 1ull);
-  for (;;) {
-    const unsigned long long fi = __shfl_sync(0xffffffffu, nfi, 0);
-    if ((int64_t)fi >= nf) break;
-    if (lane == 0) nfi = atomicAdd(&A.queue[1], 1ull);
-    const int64_t s = A.fitem_sys[fi];
-    if (s < 0) continue;  // skipped by the preparation (past cap)
-    // the system's reduce items were all taken by running warps: its mark
-    // comes; poll a bounded number of times
-    int ok = 0;
-    if (lane == 0) {
-      for (uint32_t k = 0; k < kVLMaxIdle; ++k) {
-        if (vl_load_acquire(&A.sys_count[s]) & kVLSolved) {
-          ok = 1;
-          break;
-        }
-        __nanosleep(128);
+        vl_short_solve<T, 8>(A, reg, cur, nxt, lane);
+    } else {
+      // one block of a long system: chunk reduction + block basis, its two
+      // block rows published, the block counted done
+      const int64_t s = cur.s;
+      const int nblk = (int)((cur.len + kVLBlock - 1) / kVLBlock);
+      T al[8], be[8], ga[8], de[8], bF[3], bL[3];
+      vl_read<T, 8>(reg, (int64_t)cur.blk * kVLBlock, cur.len, lane, al, be, ga, de);
+      vl_issue_item(A, reg, nxt, lane);
+      Row<T> F, L, FB, LB;
+      chunk_reduce<T, 8>(al, be, ga, de, F, L);
+      warp_block_basis(F, L, lane, bF, bL);
+      block_rows(F, L, bF, bL, lane, FB, LB);
+      T *rw = A.rows + ((int64_t)A.item_off[s] + cur.blk) * 8;
+      if (lane == 0) {
+        rw[0] = FB.a; rw[1] = FB.b; rw[2] = FB.c; rw[3] = FB.d;
+        rw[4] = LB.a; rw[5] = LB.b; rw[6] = LB.c; rw[7] = LB.d;
       }
-      if (!ok) atomicOr(A.err, kErrWaitTimeout);
+      __threadfence();  // publish the block rows before counting the block done
+      unsigned done = 0;
+      if (lane == 0) done = atomicAdd(&A.sys_count[s], 1u);
+      done = __shfl_sync(0xffffffffu, done, 0);
+      if (done == (unsigned)(nblk - 1)) {
+        __threadfence();  // every block's rows are visible to this warp now
+        // the block system of s: lane t holds block t's two rows
+        T *rs = A.rows + (int64_t)A.item_off[s] * 8;
+        Row<T> RF{T(0), T(1), T(0), T(0)}, RL{T(0), T(1), T(0), T(0)};
+        if (lane < nblk) {
+          const T *q = rs + (int64_t)lane * 8;
+          RF = {__ldcg(q + 0), __ldcg(q + 1), __ldcg(q + 2), __ldcg(q + 3)};
+          RL = {__ldcg(q + 4), __ldcg(q + 5), __ldcg(q + 6), __ldcg(q + 7)};
+        }
+        T fB, lB;
+        int span = 1;
+        while (span < nblk) span <<= 1;
+        warp_interface_solve(RF, RL, fB, lB, lane, span);
+        __syncwarp();  // all block rows read before they are overwritten
+        if (lane < nblk) {
+          rs[(int64_t)lane * 8 + 0] = fB;  // block t's boundary unknowns
+          rs[(int64_t)lane * 8 + 1] = lB;
+        }
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) atomicOr(&A.sys_count[s], kVLSolved);
+      }
     }
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    if (!ok) continue;
-    const int blk = (int)((int64_t)fi - A.fitem_off[s]);
-    const int64_t lo = A.offsets[s], len = A.offsets[s + 1] - lo;
-    T al[8], ga[8], de[8], bF[3], bL[3];
-    Row<T> F, L;
-    vl_block<T>(A, reg, lo, len, blk, lane, al, ga, de, F, L, bF, bL,
-                [&]() { warm(nfi, nf, A.fitem_sys, A.fitem_off, true); });
-    const T *bs = A.rows + ((int64_t)A.item_off[s] + blk) * 8;
-    const T f = __ldcg(bs), l = __ldcg(bs + 1);
-    const T xF = bF[0] + f * bF[1] + l * bF[2];
-    const T xL = bL[0] + f * bL[1] + l * bL[2];
-    chunk_backsub<T, 8>(al, ga, de, xF, xL);
-    vl_store<T, 8>(A, reg, lo, (int64_t)blk * kVLBlock, len, lane, de);
+    it = nit;
+    cur = nxt;
+  }
+  // ---- finish queue: every block of a long system again, back-substituted
+  // from its boundary unknowns once the system's mark is set ----
+  if (lane == 0) claim = atomicAdd(&A.queue[1], 1ull);
+  int64_t fi = (int64_t)__shfl_sync(0xffffffffu, claim, 0);
+  cur = vl_finish_item(A, fi, nf);
+  vl_issue_item(A, reg, cur, lane);
+  while (fi < nf) {
+    if (lane == 0) claim = atomicAdd(&A.queue[1], 1ull);
+    const int64_t nfi = (int64_t)__shfl_sync(0xffffffffu, claim, 0);
+    const VLItem nxt = vl_finish_item(A, nfi, nf);
+    if (cur.s < 0) {
+      vl_issue_item(A, reg, nxt, lane);
+    } else {
+      const int64_t s = cur.s;
+      T al[8], be[8], ga[8], de[8], bF[3], bL[3];
+      vl_read<T, 8>(reg, (int64_t)cur.blk * kVLBlock, cur.len, lane, al, be, ga, de);
+      vl_issue_item(A, reg, nxt, lane);
+      Row<T> F, L;
+      chunk_reduce<T, 8>(al, be, ga, de, F, L);
+      warp_block_basis(F, L, lane, bF, bL);
+      // the system's reduce items were all taken by running warps before the
+      // finish queue opened: its mark comes; poll a bounded number of times
+      int ok = 0;
+      if (lane == 0) {
+        for (uint32_t k = 0; k < kVLMaxIdle; ++k) {
+          if (vl_load_acquire(&A.sys_count[s]) & kVLSolved) {
+            ok = 1;
+            break;
+          }
+          __nanosleep(128);
+        }
+        if (!ok) atomicOr(A.err, kErrWaitTimeout);
+      }
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (ok) {
+        const T *bs = A.rows + ((int64_t)A.item_off[s] + cur.blk) * 8;
+        const T f = __ldcg(bs), l = __ldcg(bs + 1);
+        const T xF = bF[0] + f * bF[1] + l * bF[2];
+        const T xL = bL[0] + f * bL[1] + l * bL[2];
+        chunk_backsub<T, 8>(al, ga, de, xF, xL);
+        vl_store<T, 8>(A, reg, cur.lo, (int64_t)cur.blk * kVLBlock, cur.len, lane, de);
+      }
+    }
+    fi = nfi;
+    cur = nxt;
   }
 }
 
 template <typename T>
 static int varlen_smem_bytes() {
-  return kVLWarps * 4 * kVLRegion * (int)sizeof(T);
+  return kVLWarps * 5 * kVLRegion * (int)sizeof(T);
 }
 
 // Residency of the persistent kernel on the current device (sets the
