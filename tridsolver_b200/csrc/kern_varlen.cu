@@ -56,6 +56,9 @@ constexpr uint32_t kVLMaxIdle = 1u << 22;    // bounded polls of a finish item f
 // 256 rows an item): a chunk's finish items are taken right after the next
 // chunk's reduce items, while the chunk's rows are still in L2.
 constexpr int64_t kVLChunk = 4096;
+// chunk bounds kept in shared memory by every CTA (the merged order is looked
+// up on each claim); larger problems read them from global memory
+constexpr int kVLBoundsSmem = 1024;
 
 __device__ __forceinline__ bool vl_bad(int64_t lo, int64_t hi, int64_t total) {
   return hi < lo || lo < 0 || hi > total;
@@ -266,6 +269,7 @@ struct VLArgs {
   int64_t cap;               // entries of item_sys / fitem_sys / block rows
   int m2max, m4max;          // length buckets: 2 rows per lane up to m2max, 4 up to m4max
   const int64_t *fbound;     // chunk bounds of the finish items (varlen_prep_bounds)
+  int64_t kmax;              // fbound has kmax + 1 entries
   unsigned *sys_count;
   unsigned long long *queue;  // [0] reduce queue, [1] finish queue
   T *rows;       // per reduce item: the block's 8 row values; later its 2 unknowns
@@ -481,6 +485,7 @@ struct VLOrder {
 template <typename T>
 __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
   extern __shared__ __align__(16) unsigned char vl_dyn[];
+  __shared__ int64_t sbound[kVLBoundsSmem];
   const int lane = threadIdx.x & (kWarp - 1);
   T *reg = reinterpret_cast<T *>(vl_dyn) + (size_t)(threadIdx.x / kWarp) * 5 * kVLRegion;
   // the prefixes can pass cap only for non-monotone offsets; the systems past
@@ -490,6 +495,11 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
   ord.nf = A.fitem_off[A.nsys] < A.cap ? A.fitem_off[A.nsys] : A.cap;
   ord.K = (ord.ni + kVLChunk - 1) / kVLChunk;
   ord.fbound = A.fbound;
+  if (A.kmax < kVLBoundsSmem) {  // uniform over the CTA
+    for (int k = threadIdx.x; k <= (int)A.kmax; k += blockDim.x) sbound[k] = A.fbound[k];
+    __syncthreads();
+    ord.fbound = sbound;
+  }
   auto claim = [&](bool &fin, VLItem &d) {
     unsigned long long q = 0;
     int64_t idx = 0;
@@ -680,6 +690,7 @@ cudaError_t launch_varlen(const T *a, const T *b, const T *c, T *d, const int64_
   A.item_sys = (const int *)(w + 2 * al(b_off) + al(b_cnt) + al(b_q) + al(b_rows));
   A.fitem_sys = A.item_sys + al(b_map) / sizeof(int);
   A.fbound = fbound;
+  A.kmax = varlen_kmax(max_items);
   A.err = err;
   int grid = 0;
   cudaError_t e = varlen_grid<T>(grid);
@@ -844,6 +855,7 @@ extern "C" tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const doubl
                          al(sizeof(int64_t) * 2 * (size_t)((nsys + kPrepThreads - 1) / kPrepThreads)));
   }
   A.fbound = fbound;
+  A.kmax = varlen_kmax(A.cap);
   // the preparation rewrites the prefix sums and clears the queues and counters,
   // so whatever the previous call left in the array does not matter
   int grid = 0;
