@@ -122,93 +122,3 @@ def test_random_malformed_offsets_stay_in_bounds(seed):
     for s in np.unique(item_sys[: min(ri[-1], cap)]):
         if s >= 0:
             assert ri[s + 1] <= cap
-
-
-# ---------------------------------------------------------------------------
-# The merged work order (VLOrder and varlen_prep_bounds in kern_varlen.cu):
-# reduce items in chunks of CHUNK; the finish items of the systems whose last
-# reduce item is in chunk k come right after the reduce items of chunk k + 1.
-CHUNK = 4096
-
-
-def fbounds(item_off, fitem_off, cap):
-    nsys = item_off.size - 1
-    ni = min(int(item_off[-1]), cap)
-    nf = min(int(fitem_off[-1]), cap)
-    K = -(-ni // CHUNK)
-    kmax = cap // CHUNK + 2
-    out = np.empty(kmax + 1, dtype=np.int64)
-    for k in range(kmax + 1):
-        if k >= K:
-            out[k] = nf
-            continue
-        # first s with item_off[s+1] > k * CHUNK (binary search as in the kernel)
-        lo, hi = 0, nsys
-        while lo < hi:
-            mid = (lo + hi) >> 1
-            if item_off[mid + 1] > k * CHUNK:
-                hi = mid
-            else:
-                lo = mid + 1
-        out[k] = min(int(fitem_off[lo]), nf)
-    return out, ni, nf, K
-
-
-def order_map(q, fb, ni, nf, K):
-    """merged index -> ('R' | 'F', table index), None past the end."""
-    if q >= ni + nf:
-        return None
-    rlo = lambda k: min(k * CHUNK, ni)
-    start = lambda k: rlo(k) + (fb[k - 1] if k >= 1 else 0)
-    lo, hi = 0, K
-    while lo < hi:
-        mid = (lo + hi + 1) >> 1
-        if start(mid) <= q:
-            lo = mid
-        else:
-            hi = mid - 1
-    off = q - start(lo)
-    rsize = rlo(lo + 1) - rlo(lo)
-    if off >= rsize:
-        return "F", int(fb[lo - 1] + off - rsize)
-    return "R", int(rlo(lo) + off)
-
-
-@pytest.mark.parametrize("seed,nsys", [(0, 3000), (1, 20000), (2, 1)])
-def test_merged_order_is_a_valid_schedule(seed, nsys):
-    rng = np.random.default_rng(seed)
-    lens = np.floor(np.exp(rng.uniform(np.log(8), np.log(8192), nsys))).astype(np.int64)
-    off = np.concatenate([[0], np.cumsum(lens)])
-    total = int(off[-1])
-    cap = cap_of(nsys, total)
-    ni_s, nf_s, _ = counts(off, total, cap)
-    item_off = np.concatenate([[0], np.cumsum(ni_s)])
-    fitem_off = np.concatenate([[0], np.cumsum(nf_s)])
-    item_sys = np.repeat(np.arange(nsys), ni_s)
-    fitem_sys = np.repeat(np.arange(nsys), nf_s)
-    fb, ni, nf, K = fbounds(item_off, fitem_off, cap)
-    seq = [order_map(q, fb, ni, nf, K) for q in range(ni + nf)]
-    assert order_map(ni + nf, fb, ni, nf, K) is None
-    # every reduce item and every finish item exactly once
-    assert sorted(i for k, i in seq if k == "R") == list(range(ni))
-    assert sorted(i for k, i in seq if k == "F") == list(range(nf))
-    # reduce items in their own order, finish items in theirs
-    assert [i for k, i in seq if k == "R"] == list(range(ni))
-    assert [i for k, i in seq if k == "F"] == list(range(nf))
-    # a finish item comes after every reduce item of its system (the waits
-    # can never be circular) ...
-    last_r = {}
-    for q, (k, i) in enumerate(seq):
-        if k == "R":
-            last_r[item_sys[i]] = q
-    first_f = {}
-    for q, (k, i) in enumerate(seq):
-        if k == "F":
-            s = fitem_sys[i]
-            assert last_r[s] < q
-            first_f.setdefault(s, q)
-    # ... and no more than about two chunks of reduce items later (the rows
-    # are still in L2)
-    for s, qf in first_f.items():
-        between = sum(1 for kk, _ in seq[last_r[s] + 1:qf] if kk == "R")
-        assert between <= 2 * CHUNK, (s, between)

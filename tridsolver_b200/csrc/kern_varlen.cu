@@ -1,9 +1,10 @@
 // Variable-length packed batch: one persistent launch (sm_100a).
 //
 // System s occupies rows [offsets[s], offsets[s+1]) of every array (unit
-// stride, int64 offsets).  Two kinds of work items, in system order:
-//   * reduce items: a system of at most 256 rows is one item, solved whole
-//     by one warp with the partitioned Thomas of partition.cuh, the
+// stride, int64 offsets).  Two work queues in system order, served by the
+// same persistent warps one after the other:
+//   * the reduce queue: a system of at most 256 rows is one item, solved
+//     whole by one warp with the partitioned Thomas of partition.cuh, the
 //     rows-per-lane chunk M picked from the length (2/4/8: the length
 //     buckets); a longer system (up to 32 blocks of 256 rows = 8192 rows)
 //     gives one item per block: the warp reduces its block to the block's two
@@ -11,23 +12,24 @@
 //     the block done on the system's counter; the warp that completes the
 //     count solves the system's block system (2 rows per block, one warp
 //     interface solve), publishes the block boundary unknowns and marks the
-//     system solved.  Reduce items never wait.
-//   * finish items: one per block of a long system; the warp reduces the
-//     block again and back-substitutes from the block's boundary unknowns
-//     once the system's mark is set (polled a bounded number of times; a
-//     timeout is recorded in the device error word and the block skipped).
-// Both kinds are served from one merged order (VLOrder): reduce items in
-// chunks of 4096, each chunk's finish items right after the next chunk's
-// reduce items, so that the second read of a long system's rows finds them
-// in L2 (about 32 MB of rows in between) instead of DRAM.
+//     system solved.  Nothing waits in this phase.
+//   * the finish queue (taken once the reduce queue is empty): one item per
+//     block of a long system; the warp reduces the block again and
+//     back-substitutes from the block's boundary unknowns.  Its system was
+//     marked solved long ago except for the last few systems, whose reduce
+//     items are held by running warps; for those the warp polls the mark a
+//     bounded number of times (a timeout is recorded in the device error
+//     word and the block skipped).
 // Items map to their system through per-item tables built beforehand.
 // Rows reach each warp's shared-memory regions by coalesced cp.async (row q
 // of the 32*M at q + q/M, conflict-free for the lane-per-chunk reads) and
-// leave by coalesced stores.
+// leave by coalesced stores.  Long systems move their rows twice (reduce,
+// finish): 72 bytes per FP64 unknown, like the blocked partition of
+// kern_general.cu.
 //
-// Four preparation launches (launch_varlen_prep) turn offsets into the
-// prefix sums and item tables of both kinds, the chunk bounds of the finish
-// items, and clear the queue and the per-system counters.
+// Three preparation launches (launch_varlen_prep) turn offsets into the
+// prefix sums and item tables of both queues and clear the queues and the
+// per-system counters.
 // Malformed offsets (decreasing or past `total`) and systems longer than
 // 8192 rows are skipped and recorded in the device error word (bits 4 and 8).
 // The item tables hold `cap` = nsys + total/256 + 1 entries, which bounds the
@@ -51,14 +53,7 @@ constexpr int kVLRegion = 32 * (8 + 1);  // elements per staged array and warp
 constexpr unsigned kErrBadOffsets = 4u;
 constexpr unsigned kErrTooLong = 8u;
 constexpr unsigned kVLSolved = 0x80000000u;  // sys_count flag: block solution published
-constexpr uint32_t kVLMaxIdle = 1u << 22;    // bounded polls of a finish item for its system's mark
-// Reduce items per chunk of the merged work order (about 32 MB of rows at
-// 256 rows an item): a chunk's finish items are taken right after the next
-// chunk's reduce items, while the chunk's rows are still in L2.
-constexpr int64_t kVLChunk = 4096;
-// chunk bounds kept in shared memory by every CTA (the merged order is looked
-// up on each claim); larger problems read them from global memory
-constexpr int kVLBoundsSmem = 1024;
+constexpr uint32_t kVLMaxIdle = 1u << 22;    // finish-queue polls after the reduce queue ran dry
 
 __device__ __forceinline__ bool vl_bad(int64_t lo, int64_t hi, int64_t total) {
   return hi < lo || lo < 0 || hi > total;
@@ -197,50 +192,18 @@ __global__ void __launch_bounds__(kPrepThreads) varlen_prep_fill(
   for (int64_t k = rf; k < rf + nf && k < cap; ++k) fitem_sys[k] = tag;
 }
 
-// Chunk bounds of the finish items: fbound[k] = the first finish item of a
-// system whose last reduce item lies in chunk k or later (systems in order,
-// so each chunk's finish items are one range); fbound[K] = every finish item,
-// K = ceil(reduce items / kVLChunk).  One thread per entry, binary search over
-// the reduce prefix (strictly increasing: every system has a reduce item).
-__global__ void __launch_bounds__(kPrepThreads) varlen_prep_bounds(
-    const int64_t *__restrict__ item_off, const int64_t *__restrict__ fitem_off, int64_t nsys,
-    int64_t cap, int64_t kmax, int64_t *__restrict__ fbound) {
-  const int64_t k = (int64_t)blockIdx.x * kPrepThreads + threadIdx.x;
-  if (k > kmax) return;
-  const int64_t ni = item_off[nsys] < cap ? item_off[nsys] : cap;
-  const int64_t nf = fitem_off[nsys] < cap ? fitem_off[nsys] : cap;
-  const int64_t K = (ni + kVLChunk - 1) / kVLChunk;
-  if (k >= K) {
-    fbound[k] = nf;
-    return;
-  }
-  // first s with item_off[s+1] > k * kVLChunk
-  int64_t lo = 0, hi = nsys;
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (item_off[mid + 1] > k * kVLChunk) hi = mid; else lo = mid + 1;
-  }
-  const int64_t f = fitem_off[lo];
-  fbound[k] = f < nf ? f : nf;
-}
-
-// entries of fbound (plus one) for a problem whose item tables hold cap entries
-static inline int64_t varlen_kmax(int64_t cap) { return cap / kVLChunk + 2; }
-
 // Capacity of the item tables: enough for any monotone offsets
 // (sum over systems of max(1, ceil(len/256)) <= nsys + total/256).
 static inline int64_t varlen_cap(int64_t nsys, int64_t total) {
   return nsys + total / kVLBlock + 1;
 }
 
-// the four preparation launches; bsum holds 2*ceil(nsys/256) int64, the
-// item tables cap = varlen_cap(nsys, total) entries each, fbound
-// varlen_kmax(cap) + 1
+// the three preparation launches; bsum holds 2*ceil(nsys/256) int64, the
+// item tables cap = varlen_cap(nsys, total) entries each
 static cudaError_t launch_varlen_prep(const int64_t *offsets, int64_t nsys, int64_t total,
                                       int64_t *bsum, int64_t *item_off, int64_t *fitem_off,
                                       int *item_sys, int *fitem_sys, unsigned *sys_count,
-                                      unsigned long long *queue, unsigned *err, int64_t *fbound,
-                                      cudaStream_t st) {
+                                      unsigned long long *queue, unsigned *err, cudaStream_t st) {
   const int64_t nb = (nsys + kPrepThreads - 1) / kPrepThreads;
   if (nb > 0x7fffffff) return cudaErrorInvalidValue;
   const int64_t cap = varlen_cap(nsys, total);
@@ -249,9 +212,6 @@ static cudaError_t launch_varlen_prep(const int64_t *offsets, int64_t nsys, int6
   varlen_prep_fill<<<(unsigned)nb, kPrepThreads, 0, st>>>(offsets, nsys, total, cap, bsum,
                                                           item_off, fitem_off, item_sys,
                                                           fitem_sys, sys_count, err);
-  const int64_t kmax = varlen_kmax(cap);
-  varlen_prep_bounds<<<(unsigned)((kmax + kPrepThreads) / kPrepThreads), kPrepThreads, 0, st>>>(
-      item_off, fitem_off, nsys, cap, kmax, fbound);
   return cudaGetLastError();
 }
 
@@ -268,8 +228,6 @@ struct VLArgs {
   int64_t total;
   int64_t cap;               // entries of item_sys / fitem_sys / block rows
   int m2max, m4max;          // length buckets: 2 rows per lane up to m2max, 4 up to m4max
-  const int64_t *fbound;     // chunk bounds of the finish items (varlen_prep_bounds)
-  int64_t kmax;              // fbound has kmax + 1 entries
   unsigned *sys_count;
   unsigned long long *queue;  // [0] reduce queue, [1] finish queue
   T *rows;       // per reduce item: the block's 8 row values; later its 2 unknowns
@@ -444,104 +402,42 @@ __device__ __forceinline__ void vl_or_release(unsigned *p, unsigned v) {
   asm volatile("red.release.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// The merged work order: reduce items in chunks of kVLChunk, R(0), R(1),
-// F(0), R(2), F(1), ..., R(K-1), F(K-2), F(K-1), where F(k) holds the finish
-// items of the systems whose last reduce item is in R(k).  A finish item so
-// comes about one chunk of rows after its system's reduce items (its rows
-// still in L2), and always after every one of them: each item a warp waits
-// for was claimed before the waiting item, by a warp that completes it
-// (reduce items never wait), so no wait can be circular.
-struct VLOrder {
-  int64_t ni, nf, K;
-  const int64_t *fbound;
-  __device__ __forceinline__ int64_t rlo(int64_t k) const {
-    const int64_t v = k * kVLChunk;
-    return v < ni ? v : ni;
-  }
-  __device__ __forceinline__ int64_t start(int64_t k) const {  // first merged index of R(k)
-    return rlo(k) + (k >= 1 ? fbound[k - 1] : 0);
-  }
-  // merged index q -> (finish?, index into its table); false past the end
-  __device__ __forceinline__ bool map(int64_t q, bool &fin, int64_t &idx) const {
-    if (q >= ni + nf) return false;
-    int64_t lo = 0, hi = K;  // largest k in [0, K] with start(k) <= q
-    while (lo < hi) {
-      const int64_t mid = (lo + hi + 1) >> 1;
-      if (start(mid) <= q) lo = mid; else hi = mid - 1;
-    }
-    const int64_t off = q - start(lo);
-    const int64_t rsize = rlo(lo + 1) - rlo(lo);
-    fin = off >= rsize;
-    idx = fin ? fbound[lo - 1] + (off - rsize) : rlo(lo) + off;
-    return true;
-  }
-};
-
-// Every item of the merged order goes through one software pipeline per
-// warp: lane 0 claims the next item while the current one is staged; once
-// the current item's rows are in registers the next item's copies are
-// issued into the same staging regions, so they are in flight while the
-// current item is solved and stored (stores go through a fifth region).
+// Both queues are software-pipelined per warp: lane 0 claims the next item
+// while the current one is staged; once the current item's rows are in
+// registers the next item's copies are issued into the same staging
+// regions, so they are in flight while the current item is solved and
+// stored (stores go through a fifth region).
 template <typename T>
 __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
   extern __shared__ __align__(16) unsigned char vl_dyn[];
-  __shared__ int64_t sbound[kVLBoundsSmem];
   const int lane = threadIdx.x & (kWarp - 1);
   T *reg = reinterpret_cast<T *>(vl_dyn) + (size_t)(threadIdx.x / kWarp) * 5 * kVLRegion;
   // the prefixes can pass cap only for non-monotone offsets; the systems past
   // it were skipped by the preparation
-  VLOrder ord;
-  ord.ni = A.item_off[A.nsys] < A.cap ? A.item_off[A.nsys] : A.cap;
-  ord.nf = A.fitem_off[A.nsys] < A.cap ? A.fitem_off[A.nsys] : A.cap;
-  ord.K = (ord.ni + kVLChunk - 1) / kVLChunk;
-  ord.fbound = A.fbound;
-  if (A.kmax < kVLBoundsSmem) {  // uniform over the CTA
-    for (int k = threadIdx.x; k <= (int)A.kmax; k += blockDim.x) sbound[k] = A.fbound[k];
-    __syncthreads();
-    ord.fbound = sbound;
-  }
-  auto claim = [&](bool &fin, VLItem &d) {
-    unsigned long long q = 0;
-    int64_t idx = 0;
-    int f = 0, more = 0;
-    if (lane == 0) {
-      q = atomicAdd(&A.queue[0], 1ull);
-      bool fb = false;
-      more = ord.map((int64_t)q, fb, idx) ? 1 : 0;
-      f = fb ? 1 : 0;
-    }
-    more = __shfl_sync(0xffffffffu, more, 0);
-    f = __shfl_sync(0xffffffffu, f, 0);
-    idx = __shfl_sync(0xffffffffu, idx, 0);
-    fin = f != 0;
-    if (!more) {
-      d = {-1, 0, 0, -1, 8};
-      return false;
-    }
-    d = fin ? vl_finish_item(A, idx, ord.nf) : vl_reduce_item(A, idx, ord.ni, lane);
-    return true;
-  };
-  bool cfin = false;
-  VLItem cur;
-  bool live = claim(cfin, cur);
+  const int64_t nitems = A.item_off[A.nsys] < A.cap ? A.item_off[A.nsys] : A.cap;
+  const int64_t nf = A.fitem_off[A.nsys] < A.cap ? A.fitem_off[A.nsys] : A.cap;
+  // ---- reduce queue ----
+  unsigned long long claim = 0;
+  if (lane == 0) claim = atomicAdd(&A.queue[0], 1ull);
+  int64_t it = (int64_t)__shfl_sync(0xffffffffu, claim, 0);
+  VLItem cur = vl_reduce_item(A, it, nitems, lane);
   vl_issue_item(A, reg, cur, lane);
-  while (live) {
-    bool nfin = false;
-    VLItem nxt;
-    const bool nlive = claim(nfin, nxt);
+  while (it < nitems) {
+    if (lane == 0) claim = atomicAdd(&A.queue[0], 1ull);
+    const int64_t nit = (int64_t)__shfl_sync(0xffffffffu, claim, 0);
+    const VLItem nxt = vl_reduce_item(A, nit, nitems, lane);
     if (cur.s < 0) {
       vl_issue_item(A, reg, nxt, lane);
-    } else if (!cfin && cur.blk < 0) {
+    } else if (cur.blk < 0) {
       if (cur.m == 2)
         vl_short_solve<T, 2>(A, reg, cur, nxt, lane);
       else if (cur.m == 4)
         vl_short_solve<T, 4>(A, reg, cur, nxt, lane);
       else
         vl_short_solve<T, 8>(A, reg, cur, nxt, lane);
-    } else if (!cfin) {
+    } else {
       // one block of a long system: chunk reduction + block basis, its two
-      // block rows published, the block counted done (release: the rows
-      // before the count; acquire for the warp that completes the count)
+      // block rows published, the block counted done
       const int64_t s = cur.s;
       const int nblk = (int)((cur.len + kVLBlock - 1) / kVLBlock);
       T al[8], be[8], ga[8], de[8], bF[3], bL[3];
@@ -551,6 +447,8 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
       chunk_reduce<T, 8>(al, be, ga, de, F, L);
       warp_block_basis(F, L, lane, bF, bL);
       block_rows(F, L, bF, bL, lane, FB, LB);
+      // the block rows published by lane 0 before it counts the block done
+      // (release); the warp that completes the count acquires every block's
       T *rw = A.rows + ((int64_t)A.item_off[s] + cur.blk) * 8;
       unsigned done = 0;
       if (lane == 0) {
@@ -581,10 +479,23 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
         __syncwarp();
         if (lane == 0) vl_or_release(&A.sys_count[s], kVLSolved);  // cumulative release
       }
+    }
+    it = nit;
+    cur = nxt;
+  }
+  // ---- finish queue: every block of a long system again, back-substituted
+  // from its boundary unknowns once the system's mark is set ----
+  if (lane == 0) claim = atomicAdd(&A.queue[1], 1ull);
+  int64_t fi = (int64_t)__shfl_sync(0xffffffffu, claim, 0);
+  cur = vl_finish_item(A, fi, nf);
+  vl_issue_item(A, reg, cur, lane);
+  while (fi < nf) {
+    if (lane == 0) claim = atomicAdd(&A.queue[1], 1ull);
+    const int64_t nfi = (int64_t)__shfl_sync(0xffffffffu, claim, 0);
+    const VLItem nxt = vl_finish_item(A, nfi, nf);
+    if (cur.s < 0) {
+      vl_issue_item(A, reg, nxt, lane);
     } else {
-      // a finish item: the block again, back-substituted from its boundary
-      // unknowns once the system's mark is set (polled a bounded number of
-      // times; normally set long before)
       const int64_t s = cur.s;
       T al[8], be[8], ga[8], de[8], bF[3], bL[3];
       vl_read<T, 8>(reg, (int64_t)cur.blk * kVLBlock, cur.len, lane, al, be, ga, de);
@@ -592,6 +503,8 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
       Row<T> F, L;
       chunk_reduce<T, 8>(al, be, ga, de, F, L);
       warp_block_basis(F, L, lane, bF, bL);
+      // the system's reduce items were all taken by running warps before the
+      // finish queue opened: its mark comes; poll a bounded number of times
       int ok = 0;
       if (lane == 0) {
         for (uint32_t k = 0; k < kVLMaxIdle; ++k) {
@@ -614,8 +527,7 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
         vl_store<T, 8>(A, reg, cur.lo, (int64_t)cur.blk * kVLBlock, cur.len, lane, de);
       }
     }
-    live = nlive;
-    cfin = nfin;
+    fi = nfi;
     cur = nxt;
   }
 }
@@ -656,8 +568,7 @@ template <typename T>
 cudaError_t launch_varlen(const T *a, const T *b, const T *c, T *d, const int64_t *offsets,
                           int64_t nsys, int64_t total, unsigned *err, cudaStream_t st) {
   // scratch: item_off and fitem_off (nsys+1 each), sys_count, queues, block
-  // rows (8 per item), item_sys and fitem_sys (one int per item each), the
-  // preparation's per-CTA sums, the chunk bounds of the finish items
+  // rows (8 per item), item_sys and fitem_sys (one int per item each)
   const int64_t max_items = varlen_cap(nsys, total);
   const size_t b_off = sizeof(int64_t) * (size_t)(nsys + 1);
   const size_t b_cnt = sizeof(unsigned) * (size_t)(nsys + 1);
@@ -665,13 +576,11 @@ cudaError_t launch_varlen(const T *a, const T *b, const T *c, T *d, const int64_
   const size_t b_rows = sizeof(T) * 8 * (size_t)max_items;
   const size_t b_map = sizeof(int) * (size_t)max_items;
   const size_t b_bsum = sizeof(int64_t) * 2 * (size_t)((nsys + kPrepThreads - 1) / kPrepThreads);
-  const size_t b_fb = sizeof(int64_t) * (size_t)(varlen_kmax(max_items) + 1);
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   unsigned char *w = (unsigned char *)scratch(
-      2 * al(b_off) + al(b_cnt) + al(b_q) + al(b_rows) + 2 * al(b_map) + al(b_bsum) + al(b_fb), 0);
+      2 * al(b_off) + al(b_cnt) + al(b_q) + al(b_rows) + 2 * al(b_map) + al(b_bsum), 0);
   if (!w) return cudaErrorMemoryAllocation;
   int64_t *bsum = (int64_t *)(w + 2 * al(b_off) + al(b_cnt) + al(b_q) + al(b_rows) + 2 * al(b_map));
-  int64_t *fbound = (int64_t *)((unsigned char *)bsum + al(b_bsum));
   VLArgs<T> A;
   A.a = a;
   A.b = b;
@@ -689,15 +598,13 @@ cudaError_t launch_varlen(const T *a, const T *b, const T *c, T *d, const int64_
   A.rows = (T *)(w + 2 * al(b_off) + al(b_cnt) + al(b_q));
   A.item_sys = (const int *)(w + 2 * al(b_off) + al(b_cnt) + al(b_q) + al(b_rows));
   A.fitem_sys = A.item_sys + al(b_map) / sizeof(int);
-  A.fbound = fbound;
-  A.kmax = varlen_kmax(max_items);
   A.err = err;
   int grid = 0;
   cudaError_t e = varlen_grid<T>(grid);
   if (e != cudaSuccess) return e;
   e = launch_varlen_prep(offsets, nsys, total, bsum, (int64_t *)A.item_off,
                          (int64_t *)A.fitem_off, (int *)A.item_sys, (int *)A.fitem_sys,
-                         A.sys_count, A.queue, err, fbound, st);
+                         A.sys_count, A.queue, err, st);
   if (e != cudaSuccess) return e;
   varlen_kernel<T><<<dim3((unsigned)grid), dim3(kVLWarps * 32), varlen_smem_bytes<T>(), st>>>(A);
   return cudaGetLastError();
@@ -804,10 +711,9 @@ static size_t noalloc_layout(int64_t nsys, int64_t total, size_t off[5]) {
   off[3] = at;  // queue
   at += 256;
   off[4] = at;  // block rows, 8 per item; then item_sys and fitem_sys; then
-                // the preparation's per-CTA sums; then the finish chunk bounds
+                // the preparation's per-CTA sums
   at += al(sizeof(double) * 8 * (size_t)max_items) + 2 * al(sizeof(int) * (size_t)max_items);
   at += al(sizeof(int64_t) * 2 * (size_t)((nsys + kPrepThreads - 1) / kPrepThreads));
-  at += al(sizeof(int64_t) * (size_t)(varlen_kmax(max_items) + 1));
   return at <= kNoAllocScratchBytes ? at : 0;
 }
 
@@ -843,7 +749,7 @@ extern "C" tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const doubl
   A.sys_count = (unsigned *)(w + off[2]);
   A.queue = (unsigned long long *)(w + off[3]);
   A.rows = (double *)(w + off[4]);
-  int64_t *bsum = nullptr, *fbound = nullptr;
+  int64_t *bsum = nullptr;
   {
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const int64_t max_items = A.cap;
@@ -851,18 +757,14 @@ extern "C" tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const doubl
     A.fitem_sys = A.item_sys + al(sizeof(int) * (size_t)max_items) / sizeof(int);
     bsum = (int64_t *)(w + off[4] + al(sizeof(double) * 8 * (size_t)max_items) +
                        2 * al(sizeof(int) * (size_t)max_items));
-    fbound = (int64_t *)((unsigned char *)bsum +
-                         al(sizeof(int64_t) * 2 * (size_t)((nsys + kPrepThreads - 1) / kPrepThreads)));
   }
-  A.fbound = fbound;
-  A.kmax = varlen_kmax(A.cap);
   // the preparation rewrites the prefix sums and clears the queues and counters,
   // so whatever the previous call left in the array does not matter
   int grid = 0;
   if (varlen_grid<double>(grid) != cudaSuccess) return TRID_STATUS_EXECUTION_FAILED;
   if (launch_varlen_prep(A.offsets, nsys, total, bsum, (int64_t *)A.item_off,
                          (int64_t *)A.fitem_off, (int *)A.item_sys, (int *)A.fitem_sys,
-                         A.sys_count, A.queue, A.err, fbound, st) != cudaSuccess)
+                         A.sys_count, A.queue, A.err, st) != cudaSuccess)
     return TRID_STATUS_EXECUTION_FAILED;
   varlen_kernel<double><<<dim3((unsigned)grid), dim3(kVLWarps * 32), varlen_smem_bytes<double>(),
                           st>>>(A);
