@@ -197,6 +197,10 @@ def test_method_override_and_query():
     m, ch, spc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     assert L.tridQueryMethod(8, 0, 256, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
     assert (m.value, ch.value) == (2, 8)
+    # axis 0 up to 64 rows: plain loads (the sweep's winner over TMA staging)
+    for n in (2, 32, 64):
+        assert L.tridQueryMethod(8, 0, n, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+        assert m.value == 3, n
     # long systems: blocked partition with 256-row blocks
     assert L.tridQueryMethod(8, 1, 5000, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
     assert (m.value, ch.value) == (2, 8)

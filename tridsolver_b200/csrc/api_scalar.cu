@@ -196,7 +196,9 @@ MethodChoice choose_method(int dtype_bytes, int axis, int n, int opt_hint) {
     // take one CTA each, longer ones the blocked partition (blocks of
     // 32*chunk rows).
     if (axis == 0) {
-      m.method = 2;
+      // systems of at most 64 rows: plain coalesced loads beat the TMA
+      // staging (sweep: 1.28-1.45x at n = 32 and 64, FP64 and FP32)
+      m.method = n <= 64 ? 3 : 2;
     } else {
       m.method = 2;
       m.spc = 128 / dtype_bytes;
@@ -206,6 +208,13 @@ MethodChoice choose_method(int dtype_bytes, int axis, int n, int opt_hint) {
       } else {
         m.fb_method = (axis == 1) ? 3 : 2;
         m.fb_spc = 8;
+      }
+      // 257..512 rows (past the streamed tiles): the narrow plain-load tiles
+      // that won the sweep (FP64 class 1: 4 systems per CTA, 1.14x; class 2:
+      // 16, 1.11x; FP32 class 1: 8, 1.19x)
+      if (n > 256 && n <= 512 && axis <= 2) {
+        m.fb_method = 3;
+        m.fb_spc = dtype_bytes == 8 ? (axis == 1 ? 4 : 16) : (axis == 1 ? 8 : 16);
       }
     }
   }
