@@ -204,9 +204,8 @@ def test_method_override_and_query():
     # long systems: blocked partition with 256-row blocks
     assert L.tridQueryMethod(8, 1, 5000, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
     assert (m.value, ch.value) == (2, 8)
-    # axis 0 past 4096 rows: one thread-block cluster per system (method 6)
     assert L.tridQueryMethod(8, 0, 65536, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
-    assert (m.value, ch.value) == (6, 16)
+    assert (m.value, ch.value) == (2, 8)
     # strided axes, every stride class: streamed tiles of one 128-byte line of
     # systems (16 FP64, 32 FP32)
     for cls in (1, 2, 3):

@@ -81,8 +81,6 @@ def candidates(axis, n):
         if not ch0:
             out.append((2, 8, 0))   # blocked partition, 256-row blocks
             out.append((2, 16, 0))  # 512-row blocks
-        if 4096 < n <= 65536:
-            out.append((6, 16, 0))  # one thread-block cluster per system
     if axis > 0 and not ch0:
         # strided systems past 512 rows: the blocked partition, 256- or
         # 512-row blocks, 8 or 16 systems per CTA

@@ -28,8 +28,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
 
 # sources shared by both libraries
 COMMON = ["kern_scalar.cu", "kern_xtma.cu", "kern_sptma.cu", "kern_general.cu", "kern_block.cu",
-          "kern_varlen.cu", "kern_adi.cu", "kern_xcta.cu", "kern_xclu.cu", "kern_split.cu",
-          "tma_host.cu"]
+          "kern_varlen.cu", "kern_adi.cu", "kern_xcta.cu", "kern_split.cu", "tma_host.cu"]
 MAIN = ["api_scalar.cu", "kern_ext.cu"]
 COMPAT = [("api_scalar.cu", ["-DTRID_CUDACOMPAT"]), ("api_compat.cu", [])]
 

@@ -199,11 +199,6 @@ MethodChoice choose_method(int dtype_bytes, int axis, int n, int opt_hint) {
       // systems of at most 64 rows: plain coalesced loads beat the TMA
       // staging (sweep: 1.28-1.45x at n = 32 and 64, FP64 and FP32)
       m.method = n <= 64 ? 3 : 2;
-      // past 4096 rows: one thread-block cluster per system (rows read once)
-      if (n > 4096) {
-        m.method = 6;
-        m.chunk = 16;
-      }
     } else {
       m.method = 2;
       m.spc = 128 / dtype_bytes;
@@ -329,17 +324,12 @@ static int axis_class(const Geom &g, int solvedim, int elem_bytes) {
   return bytes <= 65536 ? 1 : (bytes <= (1 << 20) ? 2 : 3);
 }
 
-// Axis-0 systems solved whole on chip: one CTA each up to 4096 rows (method
-// 6, and the default), one thread-block cluster each for the forward modes
-// up to 65,536 rows (method 6, the default past 4096 rows).
-// cudaErrorNotSupported when neither applies.
+// Axis-0 systems solved whole by one CTA each (method 6, and the default up
+// to 4096 rows).  cudaErrorNotSupported when it does not apply.
 template <typename T, int MODE>
 static cudaError_t launch_x_whole(const Geom &g, const XArgs<T> &A, const MethodChoice &m,
                                   cudaStream_t st) {
   if (g.n <= 4096) return launch_xcta<T, MODE>(g, A, m.method == 6 ? m.chunk : 0, st);
-  if constexpr (MODE == kXcFwd || MODE == kXcFwdInc) {
-    if (m.method == 6) return launch_xclu<T, MODE == kXcFwdInc ? 1 : 0>(g, A, st);
-  }
   return cudaErrorNotSupported;
 }
 

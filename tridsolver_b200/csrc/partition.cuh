@@ -403,11 +403,9 @@ __device__ __forceinline__ void warp_interface_solve_n(const RowN<T, NR> &F, con
 //   x = P + F^B * UF + L^B * UL
 // by one 3-RHS solve in which lane 0's F row and lane 31's L row are replaced
 // by identity rows.  Returns, per lane, (P, UF, UL) for its F and L unknown.
-// `last` < 31 makes lane last's L the block's last unknown; the lanes past it
-// must hold identity rows (they then decouple).
 template <typename T>
 __device__ __forceinline__ void warp_block_basis(const Row<T> &F, const Row<T> &L, int lane,
-                                                 T (&bF)[3], T (&bL)[3], int last = kWarp - 1) {
+                                                 T (&bF)[3], T (&bL)[3]) {
   RowN<T, 3> F3, L3;
   F3.a = F.a;
   F3.b = F.b;
@@ -428,7 +426,7 @@ __device__ __forceinline__ void warp_block_basis(const Row<T> &F, const Row<T> &
     F3.d[0] = T(0);
     F3.d[1] = T(1);
   }
-  if (lane == last) {  // L_last = L^B
+  if (lane == kWarp - 1) {  // L_31 = L^B
     L3.a = T(0);
     L3.b = T(1);
     L3.c = T(0);
@@ -442,22 +440,20 @@ __device__ __forceinline__ void warp_block_basis(const Row<T> &F, const Row<T> &
 // rows of lanes 0 and 31 and the basis of warp_block_basis:
 //   FB row: fa*L^B_{k-1} + (fb + fc*UF(L_0))*F^B + fc*UL(L_0)*L^B = fd - fc*P(L_0)
 //   LB row: la*UF(F_31)*F^B + (lb + la*UL(F_31))*L^B + lc*F^B_{k+1} = ld - la*P(F_31)
-// (lane 0 fills FB, lane 31 fills LB; every lane gets both).  `last` as in
-// warp_block_basis.
+// (lane 0 fills FB, lane 31 fills LB).
 template <typename T>
 __device__ __forceinline__ void block_rows(const Row<T> &F, const Row<T> &L, const T (&bF)[3],
-                                           const T (&bL)[3], int lane, Row<T> &FB, Row<T> &LB,
-                                           int last = kWarp - 1) {
+                                           const T (&bL)[3], int lane, Row<T> &FB, Row<T> &LB) {
   const T l0P = __shfl_sync(0xffffffffu, bL[0], 0);
   const T l0F = __shfl_sync(0xffffffffu, bL[1], 0);
   const T l0L = __shfl_sync(0xffffffffu, bL[2], 0);
-  const T f31P = __shfl_sync(0xffffffffu, bF[0], last);
-  const T f31F = __shfl_sync(0xffffffffu, bF[1], last);
-  const T f31L = __shfl_sync(0xffffffffu, bF[2], last);
+  const T f31P = __shfl_sync(0xffffffffu, bF[0], kWarp - 1);
+  const T f31F = __shfl_sync(0xffffffffu, bF[1], kWarp - 1);
+  const T f31L = __shfl_sync(0xffffffffu, bF[2], kWarp - 1);
   const T fa = __shfl_sync(0xffffffffu, F.a, 0), fb = __shfl_sync(0xffffffffu, F.b, 0);
   const T fc = __shfl_sync(0xffffffffu, F.c, 0), fd = __shfl_sync(0xffffffffu, F.d, 0);
-  const T la = __shfl_sync(0xffffffffu, L.a, last), lb = __shfl_sync(0xffffffffu, L.b, last);
-  const T lc = __shfl_sync(0xffffffffu, L.c, last), ld = __shfl_sync(0xffffffffu, L.d, last);
+  const T la = __shfl_sync(0xffffffffu, L.a, kWarp - 1), lb = __shfl_sync(0xffffffffu, L.b, kWarp - 1);
+  const T lc = __shfl_sync(0xffffffffu, L.c, kWarp - 1), ld = __shfl_sync(0xffffffffu, L.d, kWarp - 1);
   (void)lane;
   FB = {fa, fb + fc * l0F, fc * l0L, fd - fc * l0P};
   LB = {la * f31F, lb + la * f31L, lc, ld - la * f31P};

@@ -177,10 +177,6 @@ struct XArgs {
 };
 template <typename T, int MODE>
 cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, int chunk, cudaStream_t st);
-// axis-0 systems of 4097..65,536 rows, one thread-block cluster each, forward
-// modes (kern_xclu.cu); cudaErrorNotSupported where it does not apply
-template <typename T, int INC>
-cudaError_t launch_xclu(const Geom &g, const XArgs<T> &A, cudaStream_t st);
 template <typename T, int INC>
 cudaError_t launch_generic(const Geom &g, const T *a, const T *b, const T *c, T *d, T *u,
                            T *work, int64_t work_systems, cudaStream_t st);
