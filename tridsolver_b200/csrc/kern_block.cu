@@ -913,127 +913,154 @@ __global__ void __launch_bounds__(128) blockm_adj_kernel(BlkArgs<T> a) {
 }
 
 // ---------------------------------------------------------------------------
-// M = 8, FP64: four lanes per system, lane t owning columns 2t and 2t+1 of
-// the augmented block [X_n | C_n] and (replicated in all four) the right-hand
-// side column.
+// M = 4 and 8, FP64: four lanes per system, lane t owning CPL = M/4 columns
+// (t*CPL .. t*CPL+CPL-1) of the augmented block [X_n | C_n] and (replicated
+// in all four) the right-hand side column.
 //   * X_n = B_n - A_n C'_{n-1}: each lane needs all of A_n (read from shared
 //     memory, the same address for the system's four lanes) and only its own
 //     columns of C'_{n-1}, which it computed itself: no exchange.
 //   * Gauss-Jordan on [X | C | d]: at pivot q every lane needs column q of X
-//     (8 values, owned by lane q/2): one shuffle per value; the pivot row's
+//     (M values, owned by lane q/CPL): one shuffle per value; the pivot row's
 //     entries in the lane's own columns are local.
 //   * Backward sweep x_n = d'_n - C'_n x_{n+1}: each lane forms the partial
-//     sums over its two columns for all eight rows, a two-round
-//     reduce-scatter over the four lanes leaves lane t rows 2t and 2t+1, which
-//     are exactly the unknowns its columns need one step later.
-// Per block row that is 8 value broadcasts per pivot and 6 in the backward
-// sweep, against the row-per-lane kernel's shared-memory round trip of every
-// pivot row and every row of C'.
+//     sums over its own columns for all M rows, a two-round reduce-scatter
+//     over the four lanes leaves lane t rows t*CPL .. t*CPL+CPL-1, exactly
+//     the unknowns its columns need one step later.
+// Per block row that is M value broadcasts per pivot and M/2 + M/4 in the
+// backward sweep, against the row-per-lane kernel's shared-memory round trip
+// of every pivot row and every row of C'.
 //
-// Staging: a CTA of kB8Warps warps owns 8*kB8Warps consecutive systems.  The
-// blocks of one block row n of those systems are contiguous in the
-// interleaved layout; they are copied 16 bytes at a time (cp.async, coalesced
-// global reads) into one shared-memory record per system, two records per
-// system (step n computed while step n+1 lands).  Inside a record the 16-byte
-// chunk (row r, half h) of a block sits at r*4 + (h ^ ((r >> 1) & 3)): the
-// lanes' own-column reads (forward: row r, chunk t) and the adjoint's
-// transposed reads (rows 2t, 2t+1, chunk h) then hit distinct banks, and the
-// record stride (200 doubles = 16 banks mod 32) separates the two systems of
-// a quarter-warp.
-// C'_n goes to the scratch array in a lane-major order (lane t's 16 values
-// contiguous), d'_n as the plain vector; the layout of the scratch is private
-// to this kernel.
+// Staging: each warp owns 8 consecutive systems and its own shared-memory
+// region (no CTA barrier: warps run their own pipelines).  The blocks of one
+// block row n of those systems are contiguous in the interleaved layout;
+// they are copied 16 bytes at a time (cp.async, coalesced global reads)
+// into one record per system, two record sets (step n computed while step
+// n+1 lands).  Record strides and chunk placement (BQ<M>) keep the lanes'
+// own-column reads (forward: row r; adjoint, transposed: rows of the lane's
+// columns) and the broadcast reads on distinct banks within a quarter-warp.
+// C'_n goes to the scratch array in a lane-major order (lane t's M*CPL
+// values contiguous), d'_n as the plain vector; the layout of the scratch is
+// private to this kernel.  The backward sweep streams C'_n, d'_n (and u_{n-1}
+// for the adjoint) through a ring of cp.async slots in the same region.
 //
 // Adjoint: the transposed system (sub-diagonal C_{n-1}^T, diagonal B_n^T,
 // super-diagonal A_{n+1}^T, right-hand side w_n) through the same code with
-// transposed shared-memory reads; the backward sweep forms dA, dB, dC rows
-// 2t, 2t+1 and dd from g_n and the forward solution u.
-constexpr int kB8Warps = 7;
-constexpr int kB8Sys = 8 * kB8Warps;  // systems per CTA
-constexpr int kB8Rec = 200;           // doubles per system record: 3 blocks + rhs
-constexpr int kB8WarpDoubles = 2 * 8 * kB8Rec;  // a warp's region: two record sets
-constexpr int kB8Smem = kB8Warps * kB8WarpDoubles * (int)sizeof(double);
-// backward ring: per slot 8 records of C'_n (64) + d'_n (8), then u_{n-1} of
-// the 8 systems (adjoint); the record stride (72 doubles = 16 banks mod 32)
-// keeps a quarter-warp's two systems on separate banks
-constexpr int kB8BackRec = 72;
-constexpr int kB8BackSlot = 8 * kB8BackRec + 64;
-constexpr int kB8Ring = kB8WarpDoubles / kB8BackSlot;  // 5 slots
-static_assert(kB8Ring >= 2, "backward ring");
+// transposed shared-memory reads; the backward sweep forms the rows of dA,
+// dB, dC of the lane's columns and dd from g_n and the forward solution u.
+template <int M>
+struct BQ;
+template <>
+struct BQ<8> {
+  static constexpr int kWarps = 7;      // one CTA per SM (registers); 585 CTAs at P = 32,768
+  static constexpr int kMinBlocks = 1;
+  static constexpr int kRec = 200;      // doubles per record: 3 blocks + rhs (16 banks mod 32)
+  static constexpr int kBackRec = 72;   // C'_n (64) + d'_n (8): 16 banks mod 32
+  // 16-byte chunk (row r, half h) of a block: rows of 4 chunks, XOR-swizzled
+  __device__ static int chunk(int r, int h) { return r * 4 + (h ^ ((r >> 1) & 3)); }
+  // chunk q of lane t's lane-major C' values in the backward ring
+  __device__ static int bchunk(int t, int q) { return t * 8 + (q ^ t); }
+};
+template <>
+struct BQ<4> {
+  static constexpr int kWarps = 14;     // two CTAs per SM; 293 CTAs at P = 32,768
+  static constexpr int kMinBlocks = 2;
+  static constexpr int kRec = 54;       // 3 blocks + rhs + 2 pad: 108 words, 12 banks mod 32
+  static constexpr int kBackRec = 22;   // C'_n (16) + d'_n (4) + 2 pad: 12 banks mod 32
+  __device__ static int chunk(int r, int h) { return r * 2 + h; }
+  __device__ static int bchunk(int t, int q) { return t * 2 + q; }
+};
 
-__device__ __forceinline__ int b8_chunk(int r, int h) { return r * 4 + (h ^ ((r >> 1) & 3)); }
+template <int M>
+struct BQL {  // derived layout constants
+  static constexpr int kCPL = M / 4;               // columns per lane
+  static constexpr int kHPR = M / 2;               // 16-byte chunks per block row
+  static constexpr int kBlk = M * M;
+  static constexpr int kCPB = M * M / 2;           // chunks per block
+  static constexpr int kWarpDoubles = 2 * 8 * BQ<M>::kRec;
+  static constexpr int kSmem = BQ<M>::kWarps * kWarpDoubles * (int)sizeof(double);
+  static constexpr int kSys = 8 * BQ<M>::kWarps;  // systems per CTA
+  static constexpr int kBackSlot = 8 * BQ<M>::kBackRec + 8 * M;
+  static constexpr int kRing = kWarpDoubles / kBackSlot;
+  static_assert(kRing >= 2, "backward ring");
+};
 
-__device__ __forceinline__ void b8_cp16(void *dst, const void *src) {
+__device__ __forceinline__ void bq_cp16(void *dst, const void *src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
                    (unsigned)__cvta_generic_to_shared(dst)),
                "l"(src)
                : "memory");
 }
 
-__device__ __forceinline__ double2 b8_lds(const double *p) {
+__device__ __forceinline__ double2 bq_lds(const double *p) {
   return *reinterpret_cast<const double2 *>(p);
 }
 
-__device__ __forceinline__ double2 b8_ldg(const double *p) {
+__device__ __forceinline__ double2 bq_ldg(const double *p) {
   return __ldcs(reinterpret_cast<const double2 *>(p));
 }
 
-__device__ __forceinline__ void b8_stg(double *p, double x, double y) {
+__device__ __forceinline__ void bq_stg(double *p, double x, double y) {
   *reinterpret_cast<double2 *>(p) = make_double2(x, y);
 }
 
-// v[2t], v[2t+1] of a replicated 8-vector (t = lane's column pair) without
-// run-time register indexing
-__device__ __forceinline__ void b8_pick(const double (&v)[8], int t, double &v0, double &v1) {
-  v0 = t == 0 ? v[0] : (t == 1 ? v[2] : (t == 2 ? v[4] : v[6]));
-  v1 = t == 0 ? v[1] : (t == 1 ? v[3] : (t == 2 ? v[5] : v[7]));
+// v[t*CPL + c] of a replicated M-vector without run-time register indexing
+template <int M>
+__device__ __forceinline__ double bq_pick(const double (&v)[M], int t, int c) {
+  constexpr int CPL = M / 4;
+  return t == 0 ? v[c] : (t == 1 ? v[CPL + c] : (t == 2 ? v[2 * CPL + c] : v[3 * CPL + c]));
 }
 
-// sum over the system's four lanes of part[0..7], lane t receiving the sums
-// of entries 2t and 2t+1 (two butterfly rounds, halves exchanged)
-__device__ __forceinline__ void b8_reduce_scatter(const double (&part)[8], int t, double &s0,
-                                                  double &s1) {
+// sum over the system's four lanes of part[0..M-1], lane t receiving the sums
+// of entries t*CPL .. t*CPL+CPL-1 (two butterfly rounds, halves exchanged)
+template <int M>
+__device__ __forceinline__ void bq_reduce_scatter(const double (&part)[M], int t,
+                                                  double (&out)[M / 4]) {
   constexpr unsigned kFull = 0xffffffffu;
+  constexpr int H = M / 2, Q = M / 4;
   const bool hi2 = (t & 2) != 0, hi1 = (t & 1) != 0;
-  double keep[4];
+  double keep[H];
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const double send = hi2 ? part[j] : part[4 + j];
-    const double mine = hi2 ? part[4 + j] : part[j];
+  for (int j = 0; j < H; ++j) {
+    const double send = hi2 ? part[j] : part[H + j];
+    const double mine = hi2 ? part[H + j] : part[j];
     keep[j] = mine + __shfl_xor_sync(kFull, send, 2);
   }
 #pragma unroll
-  for (int j = 0; j < 2; ++j) {
-    const double send = hi1 ? keep[j] : keep[2 + j];
-    const double mine = hi1 ? keep[2 + j] : keep[j];
-    (j == 0 ? s0 : s1) = mine + __shfl_xor_sync(kFull, send, 1);
+  for (int j = 0; j < Q; ++j) {
+    const double send = hi1 ? keep[j] : keep[Q + j];
+    const double mine = hi1 ? keep[Q + j] : keep[j];
+    out[j] = mine + __shfl_xor_sync(kFull, send, 1);
   }
 }
 
-template <bool ADJ>
-__global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double> a) {
-  extern __shared__ __align__(16) unsigned char b8_dyn[];
+template <int M, bool ADJ>
+__global__ void __launch_bounds__(BQ<M>::kWarps * 32, BQ<M>::kMinBlocks)
+    blockq_kernel(BlkArgs<double> a) {
+  using L = BQL<M>;
+  constexpr int CPL = L::kCPL, HPR = L::kHPR, BLK = L::kBlk, CPB = L::kCPB;
+  constexpr int REC = BQ<M>::kRec, BREC = BQ<M>::kBackRec;
   constexpr unsigned kFull = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char bq_dyn[];
   const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
   const int sw = lane >> 2, t = lane & 3;
   const int64_t P = a.P;
   const int N = a.N;
   // this warp's 8 systems and its private shared-memory region
-  const int64_t pw = (int64_t)blockIdx.x * kB8Sys + wi * 8;
+  const int64_t pw = (int64_t)blockIdx.x * L::kSys + wi * 8;
   if (pw >= P) return;  // warp-uniform: no system of this warp exists
   const int nvw = (int)(P - pw < 8 ? P - pw : 8);
   const bool valid = sw < nvw;
   const int64_t p = pw + sw;
-  double *wreg = reinterpret_cast<double *>(b8_dyn) + (size_t)wi * kB8WarpDoubles;
-  auto bx = [&](int n) { return ((int64_t)n * P + p) * 64; };
-  auto vx = [&](int n) { return ((int64_t)n * P + p) * 8; };
+  double *wreg = reinterpret_cast<double *>(bq_dyn) + (size_t)wi * L::kWarpDoubles;
+  auto bx = [&](int n) { return ((int64_t)n * P + p) * BLK; };
+  auto vx = [&](int n) { return ((int64_t)n * P + p) * M; };
 
   // ---- forward sweep: block row n of the warp's systems staged into
-  // record set n & 1 (slot 0 sub-diagonal, 1 diagonal, 2 super-diagonal,
-  // rhs at 192); lane l copies chunk l of every block
-  const int cpos = b8_chunk(lane >> 2, lane & 3) * 2;
+  // record set n & 1 (blocks at 0: sub-diagonal, BLK: diagonal, 2*BLK:
+  // super-diagonal; rhs at 3*BLK); the warp's lanes copy the 8*CPB chunks of
+  // every block in turn
   auto issue = [&](int n, int st) {
-    double *base = wreg + st * 8 * kB8Rec;
+    double *base = wreg + st * 8 * REC;
     const double *blk[3];
     int bn[3];
     if (!ADJ) {
@@ -1049,19 +1076,25 @@ __global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       if (!has[k]) continue;
-      const double *src = blk[k] + ((int64_t)bn[k] * P + pw) * 64 + lane * 2;
+      const double *src = blk[k] + ((int64_t)bn[k] * P + pw) * BLK;
 #pragma unroll
-      for (int s = 0; s < 8; ++s)
-        if (s < nvw) b8_cp16(base + s * kB8Rec + k * 64 + cpos, src + s * 64);
+      for (int j0 = 0; j0 < 8 * CPB; j0 += 32) {
+        const int j = j0 + lane, s = j / CPB, c = j % CPB;
+        if (s < nvw)
+          bq_cp16(base + s * REC + k * BLK + BQ<M>::chunk(c / HPR, c % HPR) * 2, src + j * 2);
+      }
     }
-    if (valid) b8_cp16(base + sw * kB8Rec + 192 + t * 2, a.d + ((int64_t)n * P + pw) * 8 + lane * 2);
+    const double *rs = a.d + ((int64_t)n * P + pw) * M;
+    if (lane < 8 * HPR && lane / HPR < nvw)  // 8 systems x HPR chunks
+      bq_cp16(base + (lane / HPR) * REC + 3 * BLK + (lane % HPR) * 2, rs + lane * 2);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
 
-  double Cp[8][2], dp[8];  // own columns of C'_{n-1}; d'_{n-1} (replicated)
+  double Cp[M][CPL], dp[M];  // own columns of C'_{n-1}; d'_{n-1} (replicated)
 #pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    Cp[r][0] = Cp[r][1] = 0.0;
+  for (int r = 0; r < M; ++r) {
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) Cp[r][c] = 0.0;
     dp[r] = 0.0;
   }
   issue(0, 0);
@@ -1070,98 +1103,91 @@ __global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncwarp();  // row n landed for the warp; set st^1 is no longer read
     if (n + 1 < N) issue(n + 1, st ^ 1);
-    const double *rec = wreg + st * 8 * kB8Rec + sw * kB8Rec;
-    double X[8][2], R[8][2], rd[8];
-    // diagonal block, own columns (transposed: own rows)
-    if (!ADJ) {
+    const double *rec = wreg + st * 8 * REC + sw * REC;
+    double X[M][CPL], R[M][CPL], rd[M];
+    // a block's own columns (forward) or own rows (transposed) into v
+    auto own = [&](const double *blkp, double (&v)[M][CPL]) {
+      if (!ADJ) {
 #pragma unroll
-      for (int r = 0; r < 8; ++r) {
-        const double2 v = b8_lds(rec + 64 + b8_chunk(r, t) * 2);
-        X[r][0] = v.x;
-        X[r][1] = v.y;
-      }
-    } else {
-#pragma unroll
-      for (int h = 0; h < 4; ++h)
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const double2 v = b8_lds(rec + 64 + b8_chunk(2 * t + c, h) * 2);
-          X[2 * h][c] = v.x;
-          X[2 * h + 1][c] = v.y;
+        for (int r = 0; r < M; ++r) {
+          const double2 u = bq_lds(blkp + BQ<M>::chunk(r, (t * CPL) / 2) * 2);
+          if (CPL == 2) {
+            v[r][0] = u.x;
+            v[r][CPL - 1] = u.y;
+          } else {
+            v[r][0] = (t & 1) ? u.y : u.x;
+          }
         }
-    }
+      } else {
 #pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const double2 v = b8_lds(rec + 192 + 2 * h);
-      rd[2 * h] = v.x;
-      rd[2 * h + 1] = v.y;
+        for (int h = 0; h < HPR; ++h)
+#pragma unroll
+          for (int c = 0; c < CPL; ++c) {
+            const double2 u = bq_lds(blkp + BQ<M>::chunk(CPL * t + c, h) * 2);
+            v[2 * h][c] = u.x;
+            v[2 * h + 1][c] = u.y;
+          }
+      }
+    };
+    own(rec + BLK, X);
+#pragma unroll
+    for (int h = 0; h < HPR; ++h) {
+      const double2 u = bq_lds(rec + 3 * BLK + 2 * h);
+      rd[2 * h] = u.x;
+      rd[2 * h + 1] = u.y;
     }
     // X -= S C'_{n-1}, rd -= S d'_{n-1}, S the sub-diagonal block (A_n, or
     // C_{n-1}^T for the adjoint)
     if (n > 0) {
 #pragma unroll
-      for (int r = 0; r < 8; ++r)
+      for (int r = 0; r < M; ++r)
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          const double2 v = b8_lds(rec + b8_chunk(r, h) * 2);
+        for (int h = 0; h < HPR; ++h) {
+          const double2 u = bq_lds(rec + BQ<M>::chunk(r, h) * 2);
           if (!ADJ) {  // A[r][2h], A[r][2h+1]
 #pragma unroll
-            for (int c = 0; c < 2; ++c) X[r][c] -= v.x * Cp[2 * h][c] + v.y * Cp[2 * h + 1][c];
-            rd[r] -= v.x * dp[2 * h] + v.y * dp[2 * h + 1];
+            for (int c = 0; c < CPL; ++c) X[r][c] -= u.x * Cp[2 * h][c] + u.y * Cp[2 * h + 1][c];
+            rd[r] -= u.x * dp[2 * h] + u.y * dp[2 * h + 1];
           } else {  // C[r][2h], C[r][2h+1] = C^T[2h][r], C^T[2h+1][r]
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
-              X[2 * h][c] -= v.x * Cp[r][c];
-              X[2 * h + 1][c] -= v.y * Cp[r][c];
+            for (int c = 0; c < CPL; ++c) {
+              X[2 * h][c] -= u.x * Cp[r][c];
+              X[2 * h + 1][c] -= u.y * Cp[r][c];
             }
-            rd[2 * h] -= v.x * dp[r];
-            rd[2 * h + 1] -= v.y * dp[r];
+            rd[2 * h] -= u.x * dp[r];
+            rd[2 * h + 1] -= u.y * dp[r];
           }
         }
     }
     // super-diagonal block, own columns (C'_{n-1} is dead from here on)
     if (n < N - 1) {
-      if (!ADJ) {
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          const double2 v = b8_lds(rec + 128 + b8_chunk(r, t) * 2);
-          R[r][0] = v.x;
-          R[r][1] = v.y;
-        }
-      } else {
-#pragma unroll
-        for (int h = 0; h < 4; ++h)
-#pragma unroll
-          for (int c = 0; c < 2; ++c) {
-            const double2 v = b8_lds(rec + 128 + b8_chunk(2 * t + c, h) * 2);
-            R[2 * h][c] = v.x;
-            R[2 * h + 1][c] = v.y;
-          }
-      }
+      own(rec + 2 * BLK, R);
     } else {
 #pragma unroll
-      for (int r = 0; r < 8; ++r) R[r][0] = R[r][1] = 0.0;
+      for (int r = 0; r < M; ++r)
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) R[r][c] = 0.0;
     }
     // Gauss-Jordan on [X | R | rd] (no pivoting: block diagonal dominance)
     const int src0 = lane & ~3;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      double pc[8];
+    for (int q = 0; q < M; ++q) {
+      double pc[M];
 #pragma unroll
-      for (int r = 0; r < 8; ++r) pc[r] = __shfl_sync(kFull, X[r][q & 1], src0 + (q >> 1));
+      for (int r = 0; r < M; ++r) pc[r] = __shfl_sync(kFull, X[r][q % CPL], src0 + q / CPL);
       const double inv = rcp(pc[q]);
 #pragma unroll
-      for (int c = 0; c < 2; ++c) {
+      for (int c = 0; c < CPL; ++c) {
         X[q][c] *= inv;
         R[q][c] *= inv;
       }
       rd[q] *= inv;
 #pragma unroll
-      for (int r = 0; r < 8; ++r) {
+      for (int r = 0; r < M; ++r) {
         if (r == q) continue;
         const double f = pc[r];
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
+        for (int c = 0; c < CPL; ++c) {
           X[r][c] -= f * X[q][c];
           R[r][c] -= f * R[q][c];
         }
@@ -1169,53 +1195,61 @@ __global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double
       }
     }
     if (valid && n < N - 1) {
+      // lane t's M*CPL values of C'_n, flat index r*CPL + c
+      double *cs = a.Cs + bx(n) + t * (M * CPL);
 #pragma unroll
-      for (int r = 0; r < 8; ++r) b8_stg(a.Cs + bx(n) + t * 16 + r * 2, R[r][0], R[r][1]);
-      double d0, d1;
-      b8_pick(rd, t, d0, d1);
-      b8_stg(a.ds + vx(n) + 2 * t, d0, d1);
+      for (int i = 0; i < M * CPL; i += 2)
+        bq_stg(cs + i, R[i / CPL][i % CPL], R[(i + 1) / CPL][(i + 1) % CPL]);
+      if (CPL == 2) {
+        bq_stg(a.ds + vx(n) + 2 * t, bq_pick<M>(rd, t, 0), bq_pick<M>(rd, t, CPL - 1));
+      } else {
+        a.ds[vx(n) + t] = bq_pick<M>(rd, t, 0);
+      }
     }
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      Cp[r][0] = R[r][0];
-      Cp[r][1] = R[r][1];
+    for (int r = 0; r < M; ++r) {
+#pragma unroll
+      for (int c = 0; c < CPL; ++c) Cp[r][c] = R[r][c];
       dp[r] = rd[r];
     }
   }
 
-  // ---- backward sweep; (x0, x1) = rows 2t, 2t+1 of x_n (g_n for the
+  // ---- backward sweep; xo[c] = row t*CPL + c of x_n (g_n for the
   // adjoint).  C'_n, d'_n (and u_{n-1} for the adjoint) of the warp's
-  // systems stream through a ring of kB8Ring slots in the same region, kB8Ring
-  // - 1 steps ahead; lane (sw, t) reads its 16 values of C'_n as chunk
-  // t*8 + (r ^ t) of its system's record (conflict-free), d'_n at +64.
-  // Lanes of systems past the end stay in the loop (the reduce-scatter
-  // shuffles take the whole warp) with their memory accesses switched off.
+  // systems stream through a ring of kRing slots in the same region, kRing -
+  // 1 steps ahead.  Lanes of systems past the end stay in the loop (the
+  // reduce-scatter shuffles take the whole warp) with their memory accesses
+  // switched off.
+  constexpr int RING = L::kRing, SLOT = L::kBackSlot;
   __syncwarp();  // every lane is done with the forward records
-  const int bpos = (lane >> 3) * 8 + ((lane & 7) ^ (lane >> 3));  // chunk of lane's C' copy
   auto issue_back = [&](int n, int slot) {
     if (n >= 0) {
-      double *base = wreg + slot * kB8BackSlot;
-      const double *cs = a.Cs + ((int64_t)n * P + pw) * 64 + lane * 2;
+      double *base = wreg + slot * SLOT;
+      const double *cs = a.Cs + ((int64_t)n * P + pw) * BLK;
+      constexpr int LQ = CPB / 4;  // chunks of one lane's C' values
 #pragma unroll
-      for (int s = 0; s < 8; ++s)
-        if (s < nvw) b8_cp16(base + s * kB8BackRec + bpos * 2, cs + s * 64);
-      if (valid) {
-        b8_cp16(base + sw * kB8BackRec + 64 + t * 2, a.ds + ((int64_t)n * P + pw) * 8 + lane * 2);
+      for (int j0 = 0; j0 < 8 * CPB; j0 += 32) {
+        const int j = j0 + lane, s = j / CPB, q = j % CPB;
+        if (s < nvw) bq_cp16(base + s * BREC + BQ<M>::bchunk(q / LQ, q % LQ) * 2, cs + j * 2);
+      }
+      if (lane < 4 * M && lane / HPR < nvw) {
+        const int s = lane / HPR, c = lane % HPR;
+        bq_cp16(base + s * BREC + BLK + 2 * c, a.ds + ((int64_t)n * P + pw) * M + lane * 2);
         if (ADJ && n > 0)
-          b8_cp16(base + 8 * kB8BackRec + sw * 8 + t * 2,
-                  a.u + ((int64_t)(n - 1) * P + pw) * 8 + lane * 2);
+          bq_cp16(base + 8 * BREC + s * M + 2 * c, a.u + ((int64_t)(n - 1) * P + pw) * M + lane * 2);
       }
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
-  double x0, x1;
-  b8_pick(dp, t, x0, x1);
-  double u_nx[8], u_cu[8], u_pv[8];  // adjoint: u_{n+1}, u_n, u_{n-1}
-  auto ldg_u = [&](int n, double (&u)[8]) {
+  double xo[CPL];
 #pragma unroll
-    for (int h = 0; h < 4; ++h) {
+  for (int c = 0; c < CPL; ++c) xo[c] = bq_pick<M>(dp, t, c);
+  double u_nx[M], u_cu[M], u_pv[M];  // adjoint: u_{n+1}, u_n, u_{n-1}
+  auto ldg_u = [&](int n, double (&u)[M]) {
+#pragma unroll
+    for (int h = 0; h < HPR; ++h) {
       const double2 v =
-          (valid && n >= 0 && n < N) ? b8_ldg(a.u + vx(n) + 2 * h) : make_double2(0.0, 0.0);
+          (valid && n >= 0 && n < N) ? bq_ldg(a.u + vx(n) + 2 * h) : make_double2(0.0, 0.0);
       u[2 * h] = v.x;
       u[2 * h + 1] = v.y;
     }
@@ -1223,87 +1257,118 @@ __global__ void __launch_bounds__(kB8Warps * 32, 1) block8_kernel(BlkArgs<double
   auto emit = [&](int n) {
     if (!valid) return;
     if (!ADJ) {
-      b8_stg(a.x + vx(n) + 2 * t, x0, x1);
+      if (CPL == 2)
+        bq_stg(a.x + vx(n) + 2 * t, xo[0], xo[CPL - 1]);
+      else
+        a.x[vx(n) + t] = xo[0];
       return;
     }
-    if (a.dd) b8_stg(a.dd + vx(n) + 2 * t, x0, x1);
+    if (a.dd) {
+      if (CPL == 2)
+        bq_stg(a.dd + vx(n) + 2 * t, xo[0], xo[CPL - 1]);
+      else
+        a.dd[vx(n) + t] = xo[0];
+    }
     const double *us[3] = {u_pv, u_cu, u_nx};
     double *outs[3] = {a.dA, a.dB, a.dC};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       if (!outs[k]) continue;
-      double *o = outs[k] + bx(n) + t * 16;
+      double *o = outs[k] + bx(n) + t * CPL * M;  // rows t*CPL .. t*CPL+CPL-1
 #pragma unroll
-      for (int j = 0; j < 8; j += 2) {
-        b8_stg(o + j, -x0 * us[k][j], -x0 * us[k][j + 1]);
-        b8_stg(o + 8 + j, -x1 * us[k][j], -x1 * us[k][j + 1]);
-      }
+      for (int c = 0; c < CPL; ++c)
+#pragma unroll
+        for (int j = 0; j < M; j += 2)
+          bq_stg(o + c * M + j, -xo[c] * us[k][j], -xo[c] * us[k][j + 1]);
     }
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < M; ++j) {
       u_nx[j] = u_cu[j];
       u_cu[j] = u_pv[j];
     }
   };
-  // the ring: step N-2-k in slot k % kB8Ring
+  // the ring: step N-2-k in slot k % RING
 #pragma unroll
-  for (int k = 0; k < kB8Ring - 1; ++k) issue_back(N - 2 - k, k);
+  for (int k = 0; k < RING - 1; ++k) issue_back(N - 2 - k, k);
   if (ADJ) {
     ldg_u(N - 1, u_cu);
     ldg_u(N - 2, u_pv);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) u_nx[j] = 0.0;
+    for (int j = 0; j < M; ++j) u_nx[j] = 0.0;
   }
   emit(N - 1);
   for (int n = N - 2, k = 0; n >= 0; --n, ++k) {
-    const int slot = k % kB8Ring;
-    issue_back(n - (kB8Ring - 1), (k + kB8Ring - 1) % kB8Ring);
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(kB8Ring - 1) : "memory");
+    const int slot = k % RING;
+    issue_back(n - (RING - 1), (k + RING - 1) % RING);
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(RING - 1) : "memory");
     __syncwarp();
-    const double *rb = wreg + slot * kB8BackSlot + sw * kB8BackRec;
-    double part[8];
+    const double *rb = wreg + slot * SLOT + sw * BREC;
+    double part[M];
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const double2 v = b8_lds(rb + (t * 8 + (r ^ t)) * 2);
-      part[r] = v.x * x0 + v.y * x1;
+    for (int r = 0; r < M; ++r) part[r] = 0.0;
+    // lane t's C'_n values, flat index r*CPL + c, two per chunk
+#pragma unroll
+    for (int q = 0; q < M * CPL / 2; ++q) {
+      const double2 v = bq_lds(rb + BQ<M>::bchunk(t, q) * 2);
+      const int i0 = 2 * q, i1 = 2 * q + 1;
+      part[i0 / CPL] += v.x * xo[i0 % CPL];
+      part[i1 / CPL] += v.y * xo[i1 % CPL];
     }
-    const double2 dv = b8_lds(rb + 64 + 2 * t);
+    double dn[CPL];
+    if (CPL == 2) {
+      const double2 dv = bq_lds(rb + BLK + 2 * t);
+      dn[0] = dv.x;
+      dn[CPL - 1] = dv.y;
+    } else {
+      dn[0] = rb[BLK + t];
+    }
     if (ADJ) {
-      const double *ub = wreg + slot * kB8BackSlot + 8 * kB8BackRec + sw * 8;
+      const double *ub = wreg + slot * SLOT + 8 * BREC + sw * M;
 #pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const double2 v = n > 0 ? b8_lds(ub + 2 * h) : make_double2(0.0, 0.0);
+      for (int h = 0; h < HPR; ++h) {
+        const double2 v = n > 0 ? bq_lds(ub + 2 * h) : make_double2(0.0, 0.0);
         u_pv[2 * h] = v.x;
         u_pv[2 * h + 1] = v.y;
       }
     }
     __syncwarp();  // the slot is read: the next issue may overwrite it
-    double s0, s1;
-    b8_reduce_scatter(part, t, s0, s1);
-    x0 = dv.x - s0;
-    x1 = dv.y - s1;
+    double sum[CPL];
+    bq_reduce_scatter<M>(part, t, sum);
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) xo[c] = dn[c] - sum[c];
     emit(n);
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Dynamic shared memory of the M = 8 kernels, set once per device.
-static cudaError_t block8_prepare() {
+// Dynamic shared memory of the four-lanes kernels, set once per device.
+template <int M>
+static cudaError_t blockq_prepare() {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   static bool done[64] = {};
   if (!done[dev]) {
-    e = cudaFuncSetAttribute(block8_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kB8Smem);
+    e = cudaFuncSetAttribute(blockq_kernel<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             BQL<M>::kSmem);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(block8_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               kB8Smem);
+      e = cudaFuncSetAttribute(blockq_kernel<M, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, BQL<M>::kSmem);
     if (e != cudaSuccess) return e;
     done[dev] = true;
   }
   return cudaSuccess;
+}
+
+template <int M, bool ADJ>
+static cudaError_t launch_blockq(const BlkArgs<double> &a, cudaStream_t st) {
+  const int64_t blocks = (a.P + BQL<M>::kSys - 1) / BQL<M>::kSys;
+  if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
+  cudaError_t e = blockq_prepare<M>();
+  if (e != cudaSuccess) return e;
+  blockq_kernel<M, ADJ><<<dim3((unsigned)blocks), dim3(BQ<M>::kWarps * 32), BQL<M>::kSmem, st>>>(a);
+  return cudaGetLastError();
 }
 
 template <typename T, bool ADJ>
@@ -1332,8 +1397,9 @@ cudaError_t launch_block(const BlkArgs<T> &a, int M, cudaStream_t st) {
       return cudaGetLastError();
     }
     // M = 3, 4: one thread per system as well (16-byte accesses need M = 4
-    // and aligned arrays; M = 3 reads element by element)
-    if (M == 3 || (M == 4 && (bits & 15) == 0)) {
+    // and aligned arrays; M = 3 reads element by element); FP64 M = 4 takes
+    // the four-lanes kernel below
+    if (M == 3 || (M == 4 && (bits & 15) == 0 && sizeof(T) != 8)) {
       const int64_t blocks = (a.P + 127) / 128;
       if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
       const dim3 g((unsigned)blocks), b(128);
@@ -1348,20 +1414,15 @@ cudaError_t launch_block(const BlkArgs<T> &a, int M, cudaStream_t st) {
     }
   }
   if constexpr (sizeof(T) == 8) {
-    // M = 8 FP64: four lanes per system (16-byte copies and accesses: every
-    // array 16-byte aligned, a null gradient output counts as aligned)
+    // M = 4, 8 FP64: four lanes per system (16-byte copies and accesses:
+    // every array 16-byte aligned, a null gradient output counts as aligned)
     const uintptr_t bits = (uintptr_t)a.A | (uintptr_t)a.B | (uintptr_t)a.C | (uintptr_t)a.d |
                            (uintptr_t)a.u | (uintptr_t)a.x | (uintptr_t)a.dA | (uintptr_t)a.dB |
                            (uintptr_t)a.dC | (uintptr_t)a.dd | (uintptr_t)a.Cs | (uintptr_t)a.ds;
-    if (M == 8 && (bits & 15) == 0) {
-      const int64_t blocks = (a.P + kB8Sys - 1) / kB8Sys;
-      if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
-      cudaError_t e = block8_prepare();
-      if (e != cudaSuccess) return e;
-      block8_kernel<ADJ><<<dim3((unsigned)blocks), dim3(kB8Warps * 32), kB8Smem, st>>>(
-          reinterpret_cast<const BlkArgs<double> &>(a));
-      return cudaGetLastError();
-    }
+    if (M == 8 && (bits & 15) == 0)
+      return launch_blockq<8, ADJ>(reinterpret_cast<const BlkArgs<double> &>(a), st);
+    if (M == 4 && (bits & 15) == 0)
+      return launch_blockq<4, ADJ>(reinterpret_cast<const BlkArgs<double> &>(a), st);
   }
   switch (M) {
     case 1: return go(block_thomas_kernel<T, 1, ADJ>, 1);
