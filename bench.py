@@ -491,7 +491,7 @@ def measure_differentiation(torch, tb, steps, seed=99):
         "target_ratio": 2.2,
         "grad_err_vs_fd": float(f"{max(errs) / max(1.0, gmax):.3e}"),
         "fd": "central, h=1e-6, 64 sampled entries of a, b, c, d; error relative to max(1, max|g|)",
-        "bytes_per_unknown": {"fwd": 40, "fwd_adj": 80, "autograd": "40 + 16 (copy of d) + 72"},
+        "bytes_per_unknown": {"fwd": 40, "fwd_adj": 80, "autograd": "40 (out-of-place forward) + 72 (adjoint)"},
     }
 
 

@@ -165,6 +165,19 @@ TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchAdjoint(const float *a, const fl
                                                         float *dc, float *dd, int ndim,
                                                         int solvedim, int *dims, int *pads);
 
+/* ---- out-of-place forward solve (no reference counterpart) ----------------
+ * x = A^{-1} d with d left intact (one pads array for every operand; x may
+ * be d, which is then the ordinary in-place solve).  Saves the copy of d a
+ * caller that must keep its right-hand side (an autograd forward) would
+ * otherwise make: on axis 0 up to 4096 rows the one-CTA kernel writes x
+ * directly, elsewhere the blocked partition reads d and writes x. */
+TRID_EXTERN_C tridStatus_t tridDmtsvStridedBatchOut(const double *a, const double *b,
+                                                    const double *c, const double *d, double *x,
+                                                    int ndim, int solvedim, int *dims, int *pads);
+TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchOut(const float *a, const float *b, const float *c,
+                                                    const float *d, float *x, int ndim,
+                                                    int solvedim, int *dims, int *pads);
+
 /* ---- forward solve + adjoint in one call (no reference counterpart) -------
  * x = A^{-1} d and, for the cotangent w = dL/dx, the gradients of the
  * adjoint above at that x (dd = A^{-T} w, da, db, dc), in one call.  For

@@ -210,3 +210,23 @@ def test_long_padded_per_array():
                                         t["d"], pads["d"], t["u"], pads["u"], 2, 0, dims, sync=1)
     assert st == 0
     assert rel_err(host(t["d"]), expect) <= RTOL[np.float64]
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("dims,solvedim", [([32, 50], 0), ([300, 21], 0), ([1024, 9], 0),
+                                           ([5000, 3], 0), ([40, 129, 3], 1), ([24, 5, 70], 2)])
+def test_out_of_place_solve(dtype, dims, solvedim):
+    """tridX mtsvStridedBatchOut: x = A^{-1} d written next to d, d intact."""
+    rng = np.random.default_rng(sum(dims) + solvedim)
+    size = int(np.prod(dims))
+    a, b, c, d = rand_coeffs(rng, size, dtype)
+    expect = oracle.mtsv(a, b, c, d, dims=dims, solvedim=solvedim)
+    td = dev(d)
+    x = torch.full_like(td, float("nan"))
+    fn = tb.tridDmtsvStridedBatchOut if dtype == np.float64 else tb.tridSmtsvStridedBatchOut
+    assert fn(dev(a), dev(b), dev(c), td, x, len(dims), solvedim, dims, dims) == 0
+    assert np.array_equal(host(td), d)
+    assert rel_err(host(x), expect) <= (1e-12 if dtype == np.float64 else 1e-5)
+    # x may be d: the in-place solve
+    assert fn(dev(a), dev(b), dev(c), td, td, len(dims), solvedim, dims, dims) == 0
+    assert rel_err(host(td), expect) <= (1e-12 if dtype == np.float64 else 1e-5)

@@ -29,6 +29,8 @@ from .scalar import (  # noqa: F401
     tridSmtsvStridedBatchAdjoint,
     tridDmtsvStridedBatchFwdAdj,
     tridSmtsvStridedBatchFwdAdj,
+    tridDmtsvStridedBatchOut,
+    tridSmtsvStridedBatchOut,
     solve_fwd_adj,
     tridDmtsvStridedBatchInc,
     tridDmtsvStridedBatchPadded,

@@ -46,6 +46,8 @@ _COMMON = {
     "tridDmtsvStridedBatchAdjoint": (c_int, _ADJ),
     "tridSmtsvStridedBatchAdjoint": (c_int, _ADJ),
     "tridDmtsvStridedBatchFwdAdj": (c_int, _FWDADJ),
+    "tridDmtsvStridedBatchOut": (c_int, [vp] * 5 + [c_int, c_int, ip, ip]),
+    "tridSmtsvStridedBatchOut": (c_int, [vp] * 5 + [c_int, c_int, ip, ip]),
     "tridSmtsvStridedBatchFwdAdj": (c_int, _FWDADJ),
     "tridDmtsvStridedBatchSplitReduce": (c_int, _SPLIT_REDUCE),
     "tridSmtsvStridedBatchSplitReduce": (c_int, _SPLIT_REDUCE),

@@ -3,8 +3,9 @@
 ``trid_solve(a, b, c, d, dim=-1)`` returns x with A x = d along torch
 dimension ``dim`` (A tridiagonal with sub-diagonal a, diagonal b,
 super-diagonal c; a[0] and c[n-1] of every system unused).  The forward pass
-is tridDmtsvStridedBatch / tridSmtsvStridedBatch on a copy of d; the
-backward pass is one call of the hand-written adjoint kernel
+is the out-of-place solve tridDmtsvStridedBatchOut / tridSmtsvStridedBatchOut
+(x written next to d, which autograd keeps, so no copy of d); the backward
+pass is one call of the hand-written adjoint kernel
 (tridXmtsvStridedBatchAdjoint): it solves A^T g = dL/dx in place and forms
 dL/da_i = -g_i x_{i-1}, dL/db_i = -g_i x_i, dL/dc_i = -g_i x_{i+1},
 dL/dd = g in the same pass.
@@ -13,8 +14,8 @@ dL/dd = g in the same pass.
 import torch
 
 from ._lib import TridError
-from .scalar import (tridDmtsvStridedBatch, tridDmtsvStridedBatchAdjoint,
-                     tridSmtsvStridedBatch, tridSmtsvStridedBatchAdjoint)
+from .scalar import (tridDmtsvStridedBatchAdjoint, tridDmtsvStridedBatchOut,
+                     tridSmtsvStridedBatchAdjoint, tridSmtsvStridedBatchOut)
 
 
 def _layout(t, dim):
@@ -32,10 +33,10 @@ class TridSolve(torch.autograd.Function):
             raise ValueError("a, b, c, d must have one shape")
         if d.dtype not in (torch.float32, torch.float64) or not d.is_cuda:
             raise TypeError("CUDA float32/float64 tensors only")
-        x = d.clone()
+        x = torch.empty_like(d)
         ndim, sd, dims = _layout(x, dim)
-        fn = tridDmtsvStridedBatch if x.dtype == torch.float64 else tridSmtsvStridedBatch
-        st = fn(a, b, c, x, None, ndim, sd, dims, dims)
+        fn = tridDmtsvStridedBatchOut if x.dtype == torch.float64 else tridSmtsvStridedBatchOut
+        st = fn(a, b, c, d, x, ndim, sd, dims, dims)
         if st != 0:
             raise TridError(st, fn.__name__)
         ctx.save_for_backward(a, b, c, x)

@@ -490,6 +490,43 @@ tridStatus_t solve_fwd_adj(const T *a, const T *b, const T *c, const T *d, const
   if (s1 != TRID_STATUS_SUCCESS) return s1;
   return solve_adjoint<T>(a, b, c, x, w, ga, gb, gc, gd, ndim, solvedim, dims, pads);
 }
+// Out-of-place forward solve x = A^{-1} d (d left intact, one pads array
+// for every operand): the one-CTA kernel on axis 0 up to 4096 rows, the
+// blocked partition (which reads the right-hand side and writes the
+// solution separately) elsewhere; x == d is the ordinary in-place solve.
+template <typename T>
+static tridStatus_t solve_out(const T *a, const T *b, const T *c, const T *d, T *x, int ndim,
+                              int solvedim, const int *dims, const int *pads) {
+  const int *p[5] = {pads, pads, pads, pads, pads};
+  if (x == d) return solve_level<T, 0>(a, b, c, x, nullptr, ndim, solvedim, dims, p, nullptr, 0, 0);
+  Geom g;
+  const tridStatus_t st = make_geom(ndim, solvedim, dims, p, true, g);
+  if (st != TRID_STATUS_SUCCESS) return st;
+  if (!aligned_ptr(a) || !aligned_ptr(b) || !aligned_ptr(c) || !aligned_ptr(d) ||
+      !aligned_ptr((const T *)x))
+    return TRID_STATUS_INVALID_VALUE;
+  if (g.n == 0 || g.nsys == 0) return TRID_STATUS_SUCCESS;
+  const cudaStream_t stream = current_stream();
+  const int axis = axis_class(g, solvedim, (int)sizeof(T));
+  MethodChoice m = choose_method((int)sizeof(T), axis, g.n, 0);
+  if (m.chunk == 0) m.chunk = 8;
+  if (m.spc == 0) m.spc = 8;
+  if (axis == 0 && m.method != 1) {
+    const cudaError_t e = launch_x_whole<T, kXcFwd>(
+        g, XArgs<T>{a, b, c, d, nullptr, nullptr, x, nullptr, nullptr, nullptr, nullptr}, m,
+        stream);
+    if (e != cudaErrorNotSupported)
+      return e == cudaSuccess ? TRID_STATUS_SUCCESS : TRID_STATUS_EXECUTION_FAILED;
+  }
+  GenArgs<T> A = {};
+  A.a = a;
+  A.b = b;
+  A.c = c;
+  A.rhs = d;
+  A.out = x;
+  return run_general<T, kGenFwd>(g, A, axis, m.chunk, narrow_spc(m), 0, stream);
+}
+
 template tridStatus_t solve_fwd_adj<float>(const float *, const float *, const float *,
                                            const float *, const float *, float *, float *, float *,
                                            float *, float *, int, int, const int *, const int *);
@@ -634,6 +671,17 @@ extern "C" tridStatus_t tridSmtsvStridedBatchAdjoint(const float *a, const float
                                                      float *dc, float *dd, int ndim, int solvedim,
                                                      int *dims, int *pads) {
   return solve_adjoint<float>(a, b, c, u, w, da, db, dc, dd, ndim, solvedim, dims, pads);
+}
+
+extern "C" tridStatus_t tridDmtsvStridedBatchOut(const double *a, const double *b,
+                                                 const double *c, const double *d, double *x,
+                                                 int ndim, int solvedim, int *dims, int *pads) {
+  return solve_out<double>(a, b, c, d, x, ndim, solvedim, dims, pads);
+}
+extern "C" tridStatus_t tridSmtsvStridedBatchOut(const float *a, const float *b, const float *c,
+                                                 const float *d, float *x, int ndim, int solvedim,
+                                                 int *dims, int *pads) {
+  return solve_out<float>(a, b, c, d, x, ndim, solvedim, dims, pads);
 }
 
 extern "C" tridStatus_t tridDmtsvStridedBatchFwdAdj(const double *a, const double *b,

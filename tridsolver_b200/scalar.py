@@ -117,6 +117,21 @@ def _fwdadj(name):
     return f
 
 
+def _out(name):
+    def f(a, b, c, d, x, ndim, solvedim, dims, pads):
+        L = lib()
+        _bind_stream(L)
+        return getattr(L, name)(_ptr(a), _ptr(b), _ptr(c), _ptr(d), _ptr(x), int(ndim),
+                                int(solvedim), int_array(dims), int_array(pads))
+    f.__name__ = name
+    f.__doc__ = (f"{name}(a, b, c, d, x, ndim, solvedim, dims, pads) -> status: "
+                 "x = A^{-1} d, d left intact")
+    return f
+
+
+tridDmtsvStridedBatchOut = _out("tridDmtsvStridedBatchOut")
+tridSmtsvStridedBatchOut = _out("tridSmtsvStridedBatchOut")
+
 tridDmtsvStridedBatchFwdAdj = _fwdadj("tridDmtsvStridedBatchFwdAdj")
 tridSmtsvStridedBatchFwdAdj = _fwdadj("tridSmtsvStridedBatchFwdAdj")
 
