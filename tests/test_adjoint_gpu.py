@@ -174,10 +174,30 @@ def test_autograd_finite_differences():
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 @pytest.mark.parametrize("n", [513, 1000, 1024, 4097, 8192, 20000])
 @pytest.mark.parametrize("inc", [False, True])
-def test_long_axis0(dtype, n, inc):
-    """8192 rows: whole 256-row blocks (the guard-free block kernels)."""
+@pytest.mark.parametrize("method", [None, (3, 8, 0)])
+def test_long_axis0(dtype, n, inc, method):
+    """8192 rows: whole 256-row blocks (the guard-free block kernels); method 3
+    takes the blocked partition from 513 rows on (no one-CTA kernel)."""
     from test_scalar_gpu import run_case
-    run_case(np.random.default_rng(n), dtype, [n, 9], 0, inc=inc)
+    run_case(np.random.default_rng(n), dtype, [n, 9], 0, inc=inc, method=method)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("n,nsys", [(4097, 400), (5000, 300), (65536, 20), (65535, 19)])
+@pytest.mark.parametrize("inc", [False, True])
+def test_long_axis0_many_steps(dtype, n, nsys, inc):
+    """Batches of long systems whose block rows span many CTAs (the reduce
+    and finish launches of the blocked partition and the block system solved
+    as its own batch), ragged last blocks included."""
+    from test_scalar_gpu import run_case
+    run_case(np.random.default_rng(n + nsys), dtype, [n, nsys], 0, inc=inc)
+
+
+@pytest.mark.parametrize("inc", [False, True])
+def test_long_axis0_padded_outer(inc):
+    """Padded outer axes (3-D arrays) on the blocked partition."""
+    from test_scalar_gpu import run_case
+    run_case(np.random.default_rng(7), np.float64, [6000, 5, 3], 0, pads=[6000, 7, 4], inc=inc)
 
 
 @pytest.mark.parametrize("n", [600, 2000])
@@ -195,10 +215,11 @@ def test_long_65536_batch():
     run_case(np.random.default_rng(65536), np.float64, [65536, 16], 0)
 
 
-def test_long_padded_per_array():
+@pytest.mark.parametrize("n", [1500, 9000])
+def test_long_padded_per_array(n):
     rng = np.random.default_rng(12)
-    dims = [1500, 5]
-    pads = {k: [1500 + 3 * i, 5] for i, k in enumerate("abcdu")}
+    dims = [n, 5]
+    pads = {k: [n + 3 * i, 5] for i, k in enumerate("abcdu")}
     arrs = {}
     for k in "abcdu":
         nn = int(np.prod(pads[k]))
