@@ -377,6 +377,17 @@ static tridStatus_t solve_level(const T *a, const T *b, const T *c, T *d, T *u, 
         unsigned *err = device_error_flags();
         if (!err) return TRID_STATUS_ALLOC_FAILED;
         e = launch_xsolve_tma<T, INC>(g, pads, ndim, a, b, c, d, u, m.chunk, err, stream);
+        // rows off the TMA grid (pads[0] not a multiple of the 128-byte
+        // row): past 128 rows the one-CTA kernel beats the plain
+        // one-warp-per-system loads (B200 sweep, FP64 / FP32: 300 rows
+        // 5.19 / 3.49 TB/s against 2.10 / 1.99, 500 rows 6.56 / 5.70 against
+        // 2.14 / 1.97; at 100 rows the plain kernel wins, 5.02 / 4.68 against
+        // 4.23 / 3.35)
+        if (e == cudaErrorNotSupported && g.n > 128)
+          e = launch_xcta<T, INC ? kXcFwdInc : kXcFwd>(
+              g, XArgs<T>{a, b, c, d, nullptr, nullptr, INC ? u : d, nullptr, nullptr, nullptr,
+                          nullptr},
+              0, stream);
       }
       if (e == cudaErrorNotSupported) e = launch_xsolve<T, INC>(g, a, b, c, d, u, m.chunk, stream);
     } else {
