@@ -1,8 +1,16 @@
-// Variable-length packed batch: one persistent launch (sm_100a).
+// Variable-length packed batch (sm_100a): length-bucketed work, persistent
+// launches.
 //
 // System s occupies rows [offsets[s], offsets[s+1]) of every array (unit
-// stride, int64 offsets).  Two work queues in system order, served by the
-// same persistent warps one after the other:
+// stride, int64 offsets).  Three length classes:
+//   * 257 .. 4096 rows: the one-CTA buckets (launch_xcta_varlen,
+//     kern_xcta.cu): bucket W holds the systems that need W = ceil(n/512)
+//     warps at 16 rows per lane; one persistent launch per bucket, CTA = W
+//     warps solving one system at a time with every row read once.  (In the
+//     block items below they moved 72 bytes per FP64 unknown at 1.9-2.3
+//     TB/s algorithmic; 300-row systems at 1.4.)
+//   * at most 256 rows, and 4097 .. 8192 rows: two work queues in system
+//     order, served by the same persistent warps one after the other:
 //   * the reduce queue: a system of at most 256 rows is one item, solved
 //     whole by one warp with the partitioned Thomas of partition.cuh, the
 //     rows-per-lane chunk M picked from the length (2/4/8: the length
@@ -28,8 +36,8 @@
 // kern_general.cu.
 //
 // Three preparation launches (launch_varlen_prep) turn offsets into the
-// prefix sums and item tables of both queues and clear the queues and the
-// per-system counters.
+// prefix sums and item tables of both queues and the one-CTA bucket lists,
+// and clear the queues and the per-system counters.
 // Malformed offsets (decreasing or past `total`) and systems longer than
 // 8192 rows are skipped and recorded in the device error word (bits 4 and 8).
 // The item tables hold `cap` = nsys + total/256 + 1 entries, which bounds the
@@ -46,7 +54,9 @@
 namespace tridb200 {
 
 constexpr int kVLBlock = 256;   // rows per block of a long system (M = 8)
-constexpr int kVLShort = 256;   // longest system solved as one item
+constexpr int kVLShort = kVarlenShort;  // longest system solved as one item
+// systems of kVLShort+1 .. kVLMid rows go to the one-CTA buckets
+constexpr int kVLMid = 512 * kVarlenCtaBuckets;
 constexpr int kVLMaxBlocks = 32;
 constexpr int kVLWarps = 8;     // warps per CTA
 constexpr int kVLRegion = 32 * (8 + 1);  // elements per staged array and warp
@@ -59,15 +69,23 @@ __device__ __forceinline__ bool vl_bad(int64_t lo, int64_t hi, int64_t total) {
   return hi < lo || lo < 0 || hi > total;
 }
 
-// reduce items of a system of len rows
+// a system for the one-CTA buckets (launch_xcta_varlen, kern_xcta.cu)
+__device__ __forceinline__ bool vl_mid(int64_t len) { return len > kVLShort && len <= kVLMid; }
+// a system for the long-system CTAs (varlen_long_kernel)
+__device__ __forceinline__ bool vl_long(int64_t len) {
+  return len > kVLMid && len <= (int64_t)kVLBlock * kVLMaxBlocks;
+}
+
+// reduce items of a system of len rows (none for the CTA classes)
 __device__ __forceinline__ int64_t vl_items(int64_t len) {
   if (len <= kVLShort) return 1;
+  if (vl_mid(len) || vl_long(len)) return 0;
   return (len + kVLBlock - 1) / kVLBlock;
 }
 
 // finish items: one per block of a long system that can be solved
 __device__ __forceinline__ int64_t vl_fitems(int64_t len) {
-  if (len <= kVLShort) return 0;
+  if (len <= kVLShort || vl_mid(len) || vl_long(len)) return 0;
   const int64_t nb = (len + kVLBlock - 1) / kVLBlock;
   return nb <= kVLMaxBlocks ? nb : 0;
 }
@@ -130,7 +148,8 @@ __global__ void __launch_bounds__(kPrepThreads) varlen_prep_count(const int64_t 
 __global__ void __launch_bounds__(1024) varlen_prep_scan(int64_t *__restrict__ bsum, int64_t nblocks,
                                                          int64_t nsys, int64_t *__restrict__ item_off,
                                                          int64_t *__restrict__ fitem_off,
-                                                         unsigned long long *__restrict__ queue) {
+                                                         unsigned long long *__restrict__ queue,
+                                                         unsigned *__restrict__ mid_count) {
   __shared__ int64_t part[1024], fpart[1024];
   const int tid = threadIdx.x;
   const int64_t per = (nblocks + 1023) / 1024;
@@ -156,6 +175,7 @@ __global__ void __launch_bounds__(1024) varlen_prep_scan(int64_t *__restrict__ b
     fitem_off[nsys] = frun;
     queue[0] = 0ull;
     queue[1] = 0ull;
+    for (int k = 0; k <= kVarlenCtaBuckets; ++k) mid_count[k] = 0u;
   }
   __syncthreads();
   int64_t run = part[tid], frun = fpart[tid];
@@ -172,7 +192,8 @@ __global__ void __launch_bounds__(kPrepThreads) varlen_prep_fill(
     const int64_t *__restrict__ offsets, int64_t nsys, int64_t total, int64_t cap,
     const int64_t *__restrict__ bsum, int64_t *__restrict__ item_off,
     int64_t *__restrict__ fitem_off, int *__restrict__ item_sys, int *__restrict__ fitem_sys,
-    unsigned *__restrict__ sys_count, unsigned *__restrict__ err) {
+    unsigned *__restrict__ sys_count, int *__restrict__ mid_list, unsigned *__restrict__ mid_count,
+    unsigned *__restrict__ err) {
   __shared__ int64_t wt[kPrepThreads / 32];
   const int64_t s = (int64_t)blockIdx.x * kPrepThreads + threadIdx.x;
   int64_t ni, nf;
@@ -190,6 +211,15 @@ __global__ void __launch_bounds__(kPrepThreads) varlen_prep_fill(
   const int tag = fits ? (int)s : -1;
   for (int64_t k = ri; k < ri + ni && k < cap; ++k) item_sys[k] = tag;
   for (int64_t k = rf; k < rf + nf && k < cap; ++k) fitem_sys[k] = tag;
+  // a system for the one-CTA buckets: listed in bucket ceil(len/512) - 1
+  // (each bucket holds up to nsys entries; a system is listed once)
+  // and a long system in the list after them
+  const int64_t lo = offsets[s], hi = offsets[s + 1];
+  if (!vl_bad(lo, hi, total) && (vl_mid(hi - lo) || vl_long(hi - lo))) {
+    const int wb = vl_mid(hi - lo) ? (int)((hi - lo + 511) / 512) - 1 : kVarlenCtaBuckets;
+    const unsigned pos = atomicAdd(&mid_count[wb], 1u);
+    mid_list[(int64_t)wb * nsys + pos] = (int)s;
+  }
 }
 
 // Capacity of the item tables: enough for any monotone offsets
@@ -199,19 +229,22 @@ static inline int64_t varlen_cap(int64_t nsys, int64_t total) {
 }
 
 // the three preparation launches; bsum holds 2*ceil(nsys/256) int64, the
-// item tables cap = varlen_cap(nsys, total) entries each
+// item tables cap = varlen_cap(nsys, total) entries each, mid_list
+// (kVarlenCtaBuckets+1)*nsys ints, mid_count kVarlenCtaBuckets+1 counters
 static cudaError_t launch_varlen_prep(const int64_t *offsets, int64_t nsys, int64_t total,
                                       int64_t *bsum, int64_t *item_off, int64_t *fitem_off,
                                       int *item_sys, int *fitem_sys, unsigned *sys_count,
-                                      unsigned long long *queue, unsigned *err, cudaStream_t st) {
+                                      unsigned long long *queue, int *mid_list,
+                                      unsigned *mid_count, unsigned *err, cudaStream_t st) {
   const int64_t nb = (nsys + kPrepThreads - 1) / kPrepThreads;
   if (nb > 0x7fffffff) return cudaErrorInvalidValue;
   const int64_t cap = varlen_cap(nsys, total);
   varlen_prep_count<<<(unsigned)nb, kPrepThreads, 0, st>>>(offsets, nsys, total, cap, bsum);
-  varlen_prep_scan<<<1, 1024, 0, st>>>(bsum, nb, nsys, item_off, fitem_off, queue);
+  varlen_prep_scan<<<1, 1024, 0, st>>>(bsum, nb, nsys, item_off, fitem_off, queue, mid_count);
   varlen_prep_fill<<<(unsigned)nb, kPrepThreads, 0, st>>>(offsets, nsys, total, cap, bsum,
                                                           item_off, fitem_off, item_sys,
-                                                          fitem_sys, sys_count, err);
+                                                          fitem_sys, sys_count, mid_list,
+                                                          mid_count, err);
   return cudaGetLastError();
 }
 
@@ -532,6 +565,131 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_kernel(VLArgs<T> A) {
   }
 }
 
+// Systems of 4097 .. 8192 rows (17 .. 32 blocks of 256): one CTA of
+// kVLLongWarps warps per system, two CTAs per SM, each looping over the
+// long systems' list.  Thread 0 first asks L2 for the whole system (one bulk
+// prefetch per array, so its DRAM reads are all in flight at once); every
+// warp reduces its blocks (warp w: blocks w, w+8, ...) to their block rows
+// in shared memory; warp 0 solves the block system (lane t = block t); every
+// warp then stages its blocks again -- from L2, a few microseconds after
+// the first read -- and finishes them.  DRAM moves each input once (40 bytes
+// per FP64 unknown); the second pass costs L2 reads and the chunk
+// reductions again.
+constexpr int kVLLongWarps = 8;
+
+template <typename T>
+__device__ __forceinline__ void vl_prefetch_rows(const T *p, int64_t n) {
+  // the 16-byte aligned interior of the rows, one bulk prefetch
+  const uintptr_t b = ((uintptr_t)p + 15) & ~(uintptr_t)15;
+  const uintptr_t e = (uintptr_t)(p + n) & ~(uintptr_t)15;
+  if (e > b)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b), "r"((uint32_t)(e - b))
+                 : "memory");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVLLongWarps * 32, 2)
+    varlen_long_kernel(VLArgs<T> A, const int *__restrict__ list, const unsigned *__restrict__ count) {
+  extern __shared__ __align__(16) unsigned char vll_dyn[];
+  __shared__ T brow[kVLMaxBlocks * 8];  // block rows; then the block unknowns at [8t], [8t+1]
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int w = threadIdx.x / kWarp;
+  T *reg = reinterpret_cast<T *>(vll_dyn) + (size_t)w * 5 * kVLRegion;
+  const int64_t cnt = (int64_t)*count;
+  for (int64_t i = blockIdx.x; i < cnt; i += gridDim.x) {
+    const int s = list[i];
+    const int64_t lo = A.offsets[s];
+    const int64_t len = A.offsets[s + 1] - lo;
+    const int nblk = (int)((len + kVLBlock - 1) / kVLBlock);
+    if (threadIdx.x == 0) {
+      vl_prefetch_rows(A.a + lo, len);
+      vl_prefetch_rows(A.b + lo, len);
+      vl_prefetch_rows(A.c + lo, len);
+      vl_prefetch_rows(A.d + lo, len);
+    }
+    // ---- the warp's blocks reduced to their block rows
+    for (int blk = w; blk < nblk; blk += kVLLongWarps) {
+      const int64_t rb = (int64_t)blk * kVLBlock;
+      vl_issue<T, 8>(A, reg, lo, rb, len, lane);
+      T al[8], be[8], ga[8], de[8], bF[3], bL[3];
+      vl_read<T, 8>(reg, rb, len, lane, al, be, ga, de);
+      Row<T> F, L, FB, LB;
+      chunk_reduce<T, 8>(al, be, ga, de, F, L);
+      warp_block_basis(F, L, lane, bF, bL);
+      block_rows(F, L, bF, bL, lane, FB, LB);
+      if (lane == 0) {
+        T *q = brow + 8 * blk;
+        q[0] = FB.a; q[1] = FB.b; q[2] = FB.c; q[3] = FB.d;
+        q[4] = LB.a; q[5] = LB.b; q[6] = LB.c; q[7] = LB.d;
+      }
+    }
+    __syncthreads();
+    // ---- the block system (2 rows per block, lane t = block t)
+    if (w == 0) {
+      Row<T> RF{T(0), T(1), T(0), T(0)}, RL{T(0), T(1), T(0), T(0)};
+      if (lane < nblk) {
+        const T *q = brow + 8 * lane;
+        RF = {q[0], q[1], q[2], q[3]};
+        RL = {q[4], q[5], q[6], q[7]};
+      }
+      T f, l;
+      warp_interface_solve(RF, RL, f, l, lane);
+      __syncwarp();
+      if (lane < nblk) {
+        brow[8 * lane] = f;
+        brow[8 * lane + 1] = l;
+      }
+    }
+    __syncthreads();
+    // ---- the warp's blocks again (L2), back-substituted from their two
+    // boundary unknowns
+    for (int blk = w; blk < nblk; blk += kVLLongWarps) {
+      const int64_t rb = (int64_t)blk * kVLBlock;
+      vl_issue<T, 8>(A, reg, lo, rb, len, lane);
+      T al[8], be[8], ga[8], de[8], bF[3], bL[3];
+      vl_read<T, 8>(reg, rb, len, lane, al, be, ga, de);
+      Row<T> F, L;
+      chunk_reduce<T, 8>(al, be, ga, de, F, L);
+      warp_block_basis(F, L, lane, bF, bL);
+      const T f = brow[8 * blk], l = brow[8 * blk + 1];
+      const T xF = bF[0] + f * bF[1] + l * bF[2];
+      const T xL = bL[0] + f * bL[1] + l * bL[2];
+      chunk_backsub<T, 8>(al, ga, de, xF, xL);
+      vl_store<T, 8>(A, reg, lo, rb, len, lane, de);
+    }
+    __syncthreads();  // brow is rewritten by the next system
+  }
+}
+
+template <typename T>
+static cudaError_t launch_varlen_long(const VLArgs<T> &A, const int *list, const unsigned *count,
+                                      cudaStream_t st) {
+  const int smem = kVLLongWarps * 5 * kVLRegion * (int)sizeof(T);
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  static int per_sm[64];
+  if (per_sm[dev] == 0) {
+    e = cudaFuncSetAttribute(varlen_long_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem);
+    if (e != cudaSuccess) return e;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, varlen_long_kernel<T>,
+                                                      kVLLongWarps * 32, smem) != cudaSuccess ||
+        nb < 1) {
+      cudaGetLastError();
+      nb = 1;
+    }
+    per_sm[dev] = nb;
+  }
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  varlen_long_kernel<T><<<(unsigned)(sms * per_sm[dev]), kVLLongWarps * 32, smem, st>>>(A, list,
+                                                                                       count);
+  return cudaGetLastError();
+}
+
 template <typename T>
 static int varlen_smem_bytes() {
   return kVLWarps * 5 * kVLRegion * (int)sizeof(T);
@@ -576,11 +734,15 @@ cudaError_t launch_varlen(const T *a, const T *b, const T *c, T *d, const int64_
   const size_t b_rows = sizeof(T) * 8 * (size_t)max_items;
   const size_t b_map = sizeof(int) * (size_t)max_items;
   const size_t b_bsum = sizeof(int64_t) * 2 * (size_t)((nsys + kPrepThreads - 1) / kPrepThreads);
+  const size_t b_mid = sizeof(int) * (kVarlenCtaBuckets + 1) * (size_t)nsys;
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-  unsigned char *w = (unsigned char *)scratch(
-      2 * al(b_off) + al(b_cnt) + al(b_q) + al(b_rows) + 2 * al(b_map) + al(b_bsum), 0);
+  const size_t at_bsum = 2 * al(b_off) + al(b_cnt) + al(b_q) + al(b_rows) + 2 * al(b_map);
+  const size_t at_mid = at_bsum + al(b_bsum);
+  unsigned char *w = (unsigned char *)scratch(at_mid + al(b_mid) + 256, 0);
   if (!w) return cudaErrorMemoryAllocation;
-  int64_t *bsum = (int64_t *)(w + 2 * al(b_off) + al(b_cnt) + al(b_q) + al(b_rows) + 2 * al(b_map));
+  int64_t *bsum = (int64_t *)(w + at_bsum);
+  int *mid_list = (int *)(w + at_mid);
+  unsigned *mid_count = (unsigned *)(w + at_mid + al(b_mid));
   VLArgs<T> A;
   A.a = a;
   A.b = b;
@@ -604,7 +766,12 @@ cudaError_t launch_varlen(const T *a, const T *b, const T *c, T *d, const int64_
   if (e != cudaSuccess) return e;
   e = launch_varlen_prep(offsets, nsys, total, bsum, (int64_t *)A.item_off,
                          (int64_t *)A.fitem_off, (int *)A.item_sys, (int *)A.fitem_sys,
-                         A.sys_count, A.queue, err, st);
+                         A.sys_count, A.queue, mid_list, mid_count, err, st);
+  if (e != cudaSuccess) return e;
+  e = launch_xcta_varlen<T>(a, b, c, d, offsets, mid_list, nsys, mid_count, st);
+  if (e != cudaSuccess) return e;
+  e = launch_varlen_long<T>(A, mid_list + (size_t)kVarlenCtaBuckets * nsys,
+                            mid_count + kVarlenCtaBuckets, st);
   if (e != cudaSuccess) return e;
   varlen_kernel<T><<<dim3((unsigned)grid), dim3(kVLWarps * 32), varlen_smem_bytes<T>(), st>>>(A);
   return cudaGetLastError();
@@ -698,7 +865,7 @@ unsigned *noalloc_error_word() {
 
 // Bytes of work space a solve of nsys systems / total rows needs (0 when it
 // does not fit in the static array).
-static size_t noalloc_layout(int64_t nsys, int64_t total, size_t off[5]) {
+static size_t noalloc_layout(int64_t nsys, int64_t total, size_t off[6]) {
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const int64_t max_items = varlen_cap(nsys, total);
   size_t at = 0;
@@ -714,6 +881,8 @@ static size_t noalloc_layout(int64_t nsys, int64_t total, size_t off[5]) {
                 // the preparation's per-CTA sums
   at += al(sizeof(double) * 8 * (size_t)max_items) + 2 * al(sizeof(int) * (size_t)max_items);
   at += al(sizeof(int64_t) * 2 * (size_t)((nsys + kPrepThreads - 1) / kPrepThreads));
+  off[5] = at;  // the CTA classes: counters, then kVarlenCtaBuckets+1 lists of nsys
+  at += 256 + al(sizeof(int) * (kVarlenCtaBuckets + 1) * (size_t)nsys);
   return at <= kNoAllocScratchBytes ? at : 0;
 }
 
@@ -728,7 +897,7 @@ extern "C" tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const doubl
     return TRID_STATUS_INVALID_VALUE;
   if (nsys == 0 || total == 0) return TRID_STATUS_SUCCESS;
   if (nsys >= ((int64_t)1 << 31) || total > ((int64_t)1 << 46)) return TRID_STATUS_INVALID_VALUE;
-  size_t off[5];
+  size_t off[6];
   if (noalloc_layout(nsys, total, off) == 0) return TRID_STATUS_INVALID_VALUE;  // too large
   unsigned char *w = (unsigned char *)noalloc_scratch_address();
   if (!w) return TRID_STATUS_EXECUTION_FAILED;
@@ -762,9 +931,16 @@ extern "C" tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const doubl
   // so whatever the previous call left in the array does not matter
   int grid = 0;
   if (varlen_grid<double>(grid) != cudaSuccess) return TRID_STATUS_EXECUTION_FAILED;
+  unsigned *mid_count = (unsigned *)(w + off[5]);
+  int *mid_list = (int *)(w + off[5] + 256);
   if (launch_varlen_prep(A.offsets, nsys, total, bsum, (int64_t *)A.item_off,
                          (int64_t *)A.fitem_off, (int *)A.item_sys, (int *)A.fitem_sys,
-                         A.sys_count, A.queue, A.err, st) != cudaSuccess)
+                         A.sys_count, A.queue, mid_list, mid_count, A.err, st) != cudaSuccess)
+    return TRID_STATUS_EXECUTION_FAILED;
+  if (launch_xcta_varlen<double>(a, b, c, d, A.offsets, mid_list, nsys, mid_count, st) !=
+          cudaSuccess ||
+      launch_varlen_long<double>(A, mid_list + (size_t)kVarlenCtaBuckets * nsys,
+                                 mid_count + kVarlenCtaBuckets, st) != cudaSuccess)
     return TRID_STATUS_EXECUTION_FAILED;
   varlen_kernel<double><<<dim3((unsigned)grid), dim3(kVLWarps * 32), varlen_smem_bytes<double>(),
                           st>>>(A);

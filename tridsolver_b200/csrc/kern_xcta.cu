@@ -173,17 +173,19 @@ __device__ __forceinline__ void prefetch_system_l2(const T *p, int n) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-template <typename T, int M, int MODE, bool FULL>
-__device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int dist) {
+// One system of n rows whose arrays start at off[] (rows past n are
+// identity rows), solved by the whole CTA: the body of the strided-batch
+// kernel below and of the variable-length batch's one-CTA systems
+// (kern_varlen.cu).  prefetch() runs on every thread once the system's
+// copies are issued.  n <= blockDim.x / 32 * 32 * M.
+template <typename T, int M, int MODE, bool FULL, typename PF>
+__device__ __forceinline__ void xcta_system(const XArgs<T> &A, const int64_t (&off)[5], const int n,
+                                            PF &&prefetch) {
   extern __shared__ __align__(16) unsigned char xcta_dyn[];
   __shared__ T sm[128 + 32 + 2 * 16];
   const int lane = threadIdx.x & (kWarp - 1);
   const int w = threadIdx.x / kWarp;
   const int nw = blockDim.x / kWarp;
-  const int64_t sys = blockIdx.x;
-  int64_t off[5];
-  system_offsets(g, sys, off);
-  const int n = g.n;
   const int r0 = w * kWarp * M + lane * M;
   const Stage<T, M> S{reinterpret_cast<T *>(xcta_dyn), nw};
   // staged arrays: 0 a, 1 b, 2 c, 3 d (forward modes) or the solution
@@ -197,15 +199,7 @@ __device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int 
   else
     stage_in<T, M, FULL>(S, 3, w, lane, A.d + off[kD], n);
   if (kHasW) stage_in<T, M, FULL>(S, 4, w, lane, A.w + off[kD], n);
-  if (dist > 0 && threadIdx.x == 0 && blockIdx.x + (int64_t)dist < g.nsys) {
-    int64_t po[5];
-    system_offsets(g, blockIdx.x + (int64_t)dist, po);
-    prefetch_system_l2(A.a + po[kA], n);
-    prefetch_system_l2(A.b + po[kB], n);
-    prefetch_system_l2(A.c + po[kC], n);
-    prefetch_system_l2(MODE == kXAdj ? A.usol + po[kU] : A.d + po[kD], n);
-    if (kHasW) prefetch_system_l2(A.w + po[kD], n);
-  }
+  prefetch();
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();  // neighbouring rows are read across warp regions
 
@@ -336,11 +330,26 @@ __device__ __forceinline__ void xcta_body(const Geom &g, const XArgs<T> &A, int 
   if (A.gd) stage_out<T, M, false, FULL>(S, 4, w, lane, gsol, A.gd + off[kD], n);
 }
 
-// The kernel: register use bounded by its launch bounds (MAXW warps, MINB
-// CTAs per SM).
+// The strided-batch kernel: CTA = system blockIdx.x; thread 0 warms L2 with
+// the system `dist` CTAs ahead.  Register use bounded by its launch bounds
+// (MAXW warps, MINB CTAs per SM).
 template <typename T, int M, int MODE, int MAXW, int MINB, bool FULL>
 __global__ void __launch_bounds__(MAXW * 32, MINB) xcta_kernel(Geom g, XArgs<T> A, int dist) {
-  xcta_body<T, M, MODE, FULL>(g, A, dist);
+  int64_t off[5];
+  system_offsets(g, (int64_t)blockIdx.x, off);
+  const int n = g.n;
+  xcta_system<T, M, MODE, FULL>(A, off, n, [&] {
+    if (dist > 0 && threadIdx.x == 0 && blockIdx.x + (int64_t)dist < g.nsys) {
+      constexpr bool kHasW = (MODE == kXAdj || MODE == kXFused);
+      int64_t po[5];
+      system_offsets(g, blockIdx.x + (int64_t)dist, po);
+      prefetch_system_l2(A.a + po[kA], n);
+      prefetch_system_l2(A.b + po[kB], n);
+      prefetch_system_l2(A.c + po[kC], n);
+      prefetch_system_l2(MODE == kXAdj ? A.usol + po[kU] : A.d + po[kD], n);
+      if (kHasW) prefetch_system_l2(A.w + po[kD], n);
+    }
+  });
 }
 
 template <typename T, int M, int MODE, auto kern>
@@ -409,6 +418,103 @@ cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, int chunk, cudaStream_
   }
   return launch_xcta_m<T, 16, MODE, 8>(g, A, warps, st);
 }
+
+// ------------------------------------------- variable-length batch buckets --
+// Systems of 257 .. 4096 rows of a variable-length batch (kern_varlen.cu),
+// bucketed by the warps they need at 16 rows per lane (W = ceil(n / 512),
+// bucket W-1 of lists / counts): one persistent launch per bucket, CTA = W
+// warps, each CTA looping over the bucket's systems (every row read once,
+// as in the strided batch), thread 0 warming L2 with its next system.
+template <typename T>
+__device__ __forceinline__ void prefetch_rows_l2(const T *p, int n) {
+  // the 16-byte aligned interior of the rows, one bulk prefetch
+  const uintptr_t b = ((uintptr_t)p + 15) & ~(uintptr_t)15;
+  const uintptr_t e = (uintptr_t)(p + n) & ~(uintptr_t)15;
+  if (e > b)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b), "r"((uint32_t)(e - b))
+                 : "memory");
+}
+
+template <typename T, int MAXW, int MINB>
+__global__ void __launch_bounds__(MAXW * 32, MINB)
+    xcta_varlen_kernel(XArgs<T> A, const int64_t *__restrict__ offsets,
+                       const int *__restrict__ list, const unsigned *__restrict__ count) {
+  const int64_t cnt = (int64_t)*count;
+  for (int64_t i = blockIdx.x; i < cnt; i += gridDim.x) {
+    const int s = list[i];
+    const int64_t lo = offsets[s];
+    const int n = (int)(offsets[s + 1] - lo);
+    const int64_t off[5] = {lo, lo, lo, lo, lo};
+    const int64_t nxt = i + gridDim.x;
+    xcta_system<T, 16, kXFwd, false>(A, off, n, [&] {
+      if (threadIdx.x == 0 && nxt < cnt) {
+        const int s2 = list[nxt];
+        const int64_t lo2 = offsets[s2];
+        const int n2 = (int)(offsets[s2 + 1] - lo2);
+        prefetch_rows_l2(A.a + lo2, n2);
+        prefetch_rows_l2(A.b + lo2, n2);
+        prefetch_rows_l2(A.c + lo2, n2);
+        prefetch_rows_l2(A.d + lo2, n2);
+      }
+    });
+    __syncthreads();  // the staged regions are refilled for the next system
+  }
+}
+
+template <typename T, int MAXW, int MINB>
+static cudaError_t launch_xcta_varlen_w(const XArgs<T> &A, const int64_t *offsets, const int *list,
+                                        const unsigned *count, int W, int dev, int sms,
+                                        cudaStream_t st) {
+  auto kern = xcta_varlen_kernel<T, MAXW, MINB>;
+  const size_t smem = (size_t)4 * W * Stage<T, 16>::R * sizeof(T);
+  static bool attr_set[64] = {};
+  static int per_sm[64][9] = {};  // resident CTAs per SM by W, per device
+  if (!attr_set[dev]) {
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               4 * MAXW * Stage<T, 16>::R * (int)sizeof(T));
+    if (e != cudaSuccess) return e;
+    attr_set[dev] = true;
+  }
+  if (per_sm[dev][W] == 0) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, W * kWarp, smem) != cudaSuccess ||
+        nb < 1) {
+      cudaGetLastError();
+      nb = 1;
+    }
+    per_sm[dev][W] = nb;
+  }
+  kern<<<(unsigned)(sms * per_sm[dev][W]), W * kWarp, smem, st>>>(A, offsets, list, count);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_xcta_varlen(const T *a, const T *b, const T *c, T *d, const int64_t *offsets,
+                               const int *lists, int64_t list_stride, const unsigned *counts,
+                               cudaStream_t st) {
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const XArgs<T> A{a, b, c, d, nullptr, nullptr, d, nullptr, nullptr, nullptr, nullptr};
+  // register caps as for the strided batch: 6 CTAs per SM up to two warps
+  for (int W = kVarlenCtaBuckets; W >= 1; --W) {
+    const int *list = lists + (size_t)(W - 1) * (size_t)list_stride;
+    e = W <= 2 ? launch_xcta_varlen_w<T, 2, 6>(A, offsets, list, counts + W - 1, W, dev, sms, st)
+               : launch_xcta_varlen_w<T, 8, 1>(A, offsets, list, counts + W - 1, W, dev, sms, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+template cudaError_t launch_xcta_varlen<float>(const float *, const float *, const float *,
+                                               float *, const int64_t *, const int *, int64_t,
+                                               const unsigned *, cudaStream_t);
+template cudaError_t launch_xcta_varlen<double>(const double *, const double *, const double *,
+                                                double *, const int64_t *, const int *, int64_t,
+                                                const unsigned *, cudaStream_t);
 
 #define TRID_XCTA_INSTANTIATE(T)                                                               \
   template cudaError_t launch_xcta<T, kXFwd>(const Geom &, const XArgs<T> &, int, cudaStream_t); \
