@@ -646,14 +646,12 @@ __global__ void __launch_bounds__(kVLLongWarps * 32, 2)
     for (int blk = w; blk < nblk; blk += kVLLongWarps) {
       const int64_t rb = (int64_t)blk * kVLBlock;
       vl_issue<T, 8>(A, reg, lo, rb, len, lane);
-      T al[8], be[8], ga[8], de[8], bF[3], bL[3];
+      T al[8], be[8], ga[8], de[8];
       vl_read<T, 8>(reg, rb, len, lane, al, be, ga, de);
       Row<T> F, L;
       chunk_reduce<T, 8>(al, be, ga, de, F, L);
-      warp_block_basis(F, L, lane, bF, bL);
-      const T f = brow[8 * blk], l = brow[8 * blk + 1];
-      const T xF = bF[0] + f * bF[1] + l * bF[2];
-      const T xL = bL[0] + f * bL[1] + l * bL[2];
+      T xF, xL;
+      warp_block_finish(F, L, brow[8 * blk], brow[8 * blk + 1], lane, xF, xL);
       chunk_backsub<T, 8>(al, ga, de, xF, xL);
       vl_store<T, 8>(A, reg, lo, rb, len, lane, de);
     }

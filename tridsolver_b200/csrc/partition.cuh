@@ -436,6 +436,19 @@ __device__ __forceinline__ void warp_block_basis(const Row<T> &F, const Row<T> &
   warp_interface_solve_n<T, 3>(F3, L3, bF, bL, lane);
 }
 
+// A block's interface unknowns once its first unknown F^B = f (lane 0's F)
+// and last unknown L^B = l (lane 31's L) are known: the interface system with
+// those two rows replaced by identity rows, one right-hand side (a third of
+// warp_block_basis's work; the same values up to rounding).
+template <typename T>
+__device__ __forceinline__ void warp_block_finish(const Row<T> &F, const Row<T> &L, T f, T l,
+                                                  int lane, T &xF, T &xL) {
+  Row<T> F1 = F, L1 = L;
+  if (lane == 0) F1 = {T(0), T(1), T(0), f};
+  if (lane == kWarp - 1) L1 = {T(0), T(1), T(0), l};
+  warp_interface_solve(F1, L1, xF, xL, lane);
+}
+
 // The two rows of a block's reduced equations, from the original interface
 // rows of lanes 0 and 31 and the basis of warp_block_basis:
 //   FB row: fa*L^B_{k-1} + (fb + fc*UF(L_0))*F^B + fc*UL(L_0)*L^B = fd - fc*P(L_0)
