@@ -243,12 +243,14 @@ TRID_EXTERN_C tridStatus_t tridSmtsvStridedBatchSplitFinish(const float *a, cons
  * array of nsys+1 int64 values and total = offsets[nsys] (the number of
  * rows, passed so that the call needs no device-to-host read).  Each system's
  * first a and last c are never read.  The solution overwrites d.  Systems of
- * up to 8192 rows; one persistent launch (after three short preparation
- * launches) with length-bucketed work items.  Malformed offsets and longer
+ * up to 8192 rows: three short preparation launches sort them into
+ * length-bucketed work queues (up to 256 rows, one warp each; 257 .. 4096
+ * rows, one CTA of ceil(n/512) warps each, by bucket; 4097 .. 8192 rows, one
+ * CTA each), each served by persistent CTAs.  Malformed offsets and longer
  * systems are skipped and reported by tridGetDeviceErrors (bits 4 and 8).
  * Offsets must increase monotonically: where they do not, valid-looking
- * systems may overlap, and those whose work items would not fit in the
- * tables sized for monotone offsets are skipped as malformed (bit 4). */
+ * systems may overlap (each is solved in place in turn, in no fixed order);
+ * no work table can overflow, whatever the offsets hold. */
 TRID_EXTERN_C tridStatus_t tridDmtsvVarlenBatch(const double *a, const double *b, const double *c,
                                                 double *d, const long long *offsets,
                                                 long long nsys, long long total);
@@ -264,9 +266,8 @@ TRID_EXTERN_C tridStatus_t tridSmtsvVarlenBatch(const float *a, const float *b, 
  * cudaMalloc/cudaFree.  Same arguments and result as tridDmtsvVarlenBatch,
  * but every scratch byte comes from one fixed 32 MiB array per device that
  * the library holds from load to process exit; no call allocates.
- * Limit: the work space must fit in 32 MiB, roughly
- *   20*(nsys+1) + 72*(nsys + total/256 + 1) bytes plus alignment
- * (e.g. 100,000 systems with up to 80 million rows in total); larger
+ * Limit: the work space must fit in 32 MiB, roughly 40*nsys bytes plus
+ * alignment (about 830,000 systems, whatever their total length); larger
  * problems return TRID_STATUS_INVALID_VALUE and should use
  * tridDmtsvVarlenBatch.
  * The first call on each device looks up the array's device address (a
@@ -274,11 +275,11 @@ TRID_EXTERN_C tridStatus_t tridSmtsvVarlenBatch(const float *a, const float *b, 
  * first call before any stream capture.  Every call uses the same array and
  * leaves its contents behind (the next call clears what must start at zero),
  * so calls that overlap on the GPU -- concurrent streams or threads on one
- * device -- race and must be serialised by the caller.  Malformed offsets,
- * over-long systems and finish waits that gave up are skipped as in
- * tridDmtsvVarlenBatch and recorded in an error word inside the same array,
- * which tridGetDeviceErrors reads and clears together with the library's
- * word (bits 1, 4 and 8; that call allocates nothing either). */
+ * device -- race and must be serialised by the caller.  Malformed offsets
+ * and over-long systems are skipped as in tridDmtsvVarlenBatch and recorded
+ * in an error word inside the same array, which tridGetDeviceErrors reads
+ * and clears together with the library's word (bits 4 and 8; that call
+ * allocates nothing either).  No kernel of the solve waits on another CTA. */
 TRID_EXTERN_C tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const double *b,
                                                        const double *c, double *d,
                                                        const long long *offsets, long long nsys,

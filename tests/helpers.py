@@ -51,11 +51,11 @@ def overlapping_varlen_problem(seed, ngood=600, npairs=400, extra=8192):
     """A variable-length batch whose offsets stop increasing: ngood ordinary
     systems packed in rows [0, G), then npairs of systems alternating between
     [G, G + extra] (valid-looking, every one overlapping the others) and
-    [G + extra, G] (decreasing).  The valid-looking ones would need about
-    npairs * extra / 256 work items, far more than the tables sized for
-    monotone offsets hold, so the solver must skip the ones past its capacity
-    and flag bit 4, while the ngood systems stay solved.  Returns the FP64
-    arrays, the offsets and G."""
+    [G + extra, G] (decreasing).  The decreasing ones must be flagged (bit 4)
+    and skipped, the valid-looking ones must not drive any work table past
+    its size (a layout of 256-row block items would need about
+    npairs * extra / 256 entries), and the ngood systems must stay solved.
+    Returns the FP64 arrays, the offsets and G."""
     rng = np.random.default_rng(seed)
     lens = np.floor(np.exp(rng.uniform(np.log(8), np.log(2048), ngood))).astype(np.int64)
     good = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)

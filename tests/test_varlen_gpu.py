@@ -83,10 +83,11 @@ def test_rejects_and_flags():
 
 
 def test_non_monotone_offsets_past_capacity_are_skipped():
-    """Offsets that stop increasing can ask for many more work items than the
-    tables hold; the systems past the capacity are skipped and flagged (bit
-    4), nothing is written out of bounds, and the ordinary systems before
-    them are solved."""
+    """Offsets that stop increasing: the decreasing systems are skipped and
+    flagged (bit 4), the valid-looking ones (all overlapping the same 8192
+    rows) go to the long-system CTAs without any table passing nsys, nothing
+    is written out of bounds, and the ordinary systems before them are
+    solved."""
     flags = ctypes.c_uint()
     tb.lib().tridGetDeviceErrors(ctypes.byref(flags))  # clear
     (a, b, c, d), off, G = overlapping_varlen_problem(21)

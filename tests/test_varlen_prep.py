@@ -1,108 +1,105 @@
 """The variable-length batch's preparation restated in numpy (CPU): the
-per-system item counts, their prefix sums and the item tables of the reduce
-and finish queues (varlen_prep_count / _scan / _fill in
-tridsolver_b200/csrc/kern_varlen.cu), including the capacity guard.
+length classes and the work tables the three preparation launches build
+(varlen_prep_count / _scan / _fill in tridsolver_b200/csrc/kern_varlen.cu).
 
-The item tables are sized for cap = nsys + total/256 + 1 entries.  These
-tests pin the two facts the guard rests on: monotone offsets never need more
-than cap items (so no valid input is ever skipped), and offsets that do not
-increase monotonically can ask for far more (0, T, 0, T, ...), in which case
-every system whose items would end past cap is skipped whole, no table index
-reaches cap, and the systems before it keep exactly the items they would
-have had without the guard.
+Systems of at most 256 rows go to the short queue, in system order (a prefix
+scan); 257 .. 4096 rows to the one-CTA bucket ceil(len/512) - 1; 4097 ..
+8192 rows to the long list; empty systems nowhere; malformed offsets and
+longer systems nowhere, with their error bits.  These tests pin the facts
+the kernels rely on: every system lands in at most one table, so no table
+index can reach nsys whatever the offsets hold (decreasing, out of range,
+or 0, T, 0, T, ... overlapping), and every solvable system lands in exactly
+one.
 """
 
 import numpy as np
 import pytest
 
-BLOCK = 256      # rows per block of a long system
-SHORT = 256      # longest system solved as one item
-MAX_BLOCKS = 32  # longest solvable system: 32 blocks
+SHORT = 256
+MID = 512 * 8       # one-CTA buckets: 8 of them, 512 rows per warp
+LONGEST = 256 * 32  # longest solvable system
+ERR_BAD, ERR_TOO_LONG = 4, 8
+N_LISTS = 9         # the 8 buckets, then the long list
 
 
-def cap_of(nsys, total):
-    return nsys + total // BLOCK + 1
-
-
-def counts(offsets, total, cap):
-    """Per-system reduce/finish items (vl_counts), clamped to cap + 1."""
+def classify(offsets, total):
+    """Per system: ('short', None), ('list', index), ('empty', None),
+    ('bad', None) or ('long+', None) -- vl_class."""
     lo, hi = offsets[:-1], offsets[1:]
-    bad = (hi < lo) | (lo < 0) | (hi > total)
-    ln = np.where(bad, 0, hi - lo)
-    nblk = (ln + BLOCK - 1) // BLOCK
-    ni = np.where(ln <= SHORT, 1, nblk)
-    nf = np.where((ln > SHORT) & (nblk <= MAX_BLOCKS), nblk, 0)
-    return np.minimum(ni, cap + 1), np.minimum(nf, cap + 1), bad
+    out = []
+    for a, b in zip(lo, hi):
+        if b < a or a < 0 or b > total:
+            out.append(("bad", None))
+        elif b == a:
+            out.append(("empty", None))
+        elif b - a <= SHORT:
+            out.append(("short", None))
+        elif b - a <= MID:
+            out.append(("list", int((b - a + 511) // 512) - 1))
+        elif b - a <= LONGEST:
+            out.append(("list", N_LISTS - 1))
+        else:
+            out.append(("long+", None))
+    return out
 
 
 def prepare(offsets, total):
-    """Item tables as the three preparation launches leave them.  Returns
-    (item_sys, fitem_sys, item_off, fitem_off, skipped, flagged)."""
+    """The tables as the preparation leaves them: (short queue, lists, error
+    bits).  List order is the order of arrival (atomic appends), so the lists
+    are compared as sets."""
     offsets = np.asarray(offsets, dtype=np.int64)
     nsys = offsets.size - 1
-    cap = cap_of(nsys, total)
-    ni, nf, bad = counts(offsets, total, cap)
-    ri = np.concatenate([[0], np.cumsum(ni)])
-    rf = np.concatenate([[0], np.cumsum(nf)])
-    item_sys = np.full(cap, -2, dtype=np.int64)   # -2: never written
-    fitem_sys = np.full(cap, -2, dtype=np.int64)
-    skipped = np.zeros(nsys, dtype=bool)
-    for s in range(nsys):
-        fits = ri[s] + ni[s] <= cap and rf[s] + nf[s] <= cap
-        skipped[s] = not fits
-        tag = s if fits else -1
-        for k in range(ri[s], min(ri[s] + ni[s], cap)):
-            item_sys[k] = tag
-        for k in range(rf[s], min(rf[s] + nf[s], cap)):
-            fitem_sys[k] = tag
-    flagged = bool(bad.any() or skipped.any())
-    return item_sys, fitem_sys, ri, rf, skipped, flagged
+    cls = classify(offsets, total)
+    queue = [s for s, (k, _) in enumerate(cls) if k == "short"]  # the prefix scan keeps order
+    lists = [[] for _ in range(N_LISTS)]
+    err = 0
+    for s, (k, li) in enumerate(cls):
+        if k == "list":
+            lists[li].append(s)
+        elif k == "bad":
+            err |= ERR_BAD
+        elif k == "long+":
+            err |= ERR_TOO_LONG
+    assert len(queue) <= nsys and all(len(x) <= nsys for x in lists)
+    return queue, lists, err
 
 
-def test_monotone_offsets_never_reach_cap():
+def test_monotone_offsets_every_system_once():
     rng = np.random.default_rng(0)
     for trial in range(200):
         nsys = int(rng.integers(1, 400))
-        # lengths from 0 up to past the longest solvable system
-        lens = np.floor(np.exp(rng.uniform(0, np.log(12000), nsys))).astype(np.int64)
+        lens = np.floor(np.exp(rng.uniform(0, np.log(8192), nsys))).astype(np.int64)
         lens[rng.random(nsys) < 0.1] = 0
         off = np.concatenate([[0], np.cumsum(lens)])
-        total = int(off[-1]) + int(rng.integers(0, 1000))  # total may exceed the last offset
-        cap = cap_of(nsys, total)
-        ni, nf, bad = counts(off, total, cap)
-        assert not bad.any()
-        assert ni.sum() <= cap - 1 and nf.sum() <= ni.sum()
-        item_sys, fitem_sys, ri, rf, skipped, flagged = prepare(off, total)
-        assert not skipped.any() and not flagged
-        # every reduce item names its system, in system order
-        assert np.array_equal(item_sys[: ri[-1]], np.repeat(np.arange(nsys), ni))
-        assert np.array_equal(fitem_sys[: rf[-1]], np.repeat(np.arange(nsys), nf))
+        total = int(off[-1]) + int(rng.integers(0, 1000))
+        queue, lists, err = prepare(off, total)
+        assert err == 0
+        seen = queue + [s for x in lists for s in x]
+        assert sorted(seen) == [s for s in range(nsys) if lens[s] > 0]
+        assert queue == sorted(queue)
+        for li, x in enumerate(lists[:-1]):
+            assert all(SHORT < lens[s] <= MID and (lens[s] + 511) // 512 == li + 1 for s in x)
+        assert all(MID < lens[s] <= LONGEST for s in lists[-1])
 
 
-def test_alternating_offsets_are_capped():
-    # 0, T, 0, T, ...: systems 0, 2, 4, ... are valid and T rows long, the
-    # others decreasing.  Without the guard they would need far more items
-    # than cap.
-    T, nsys = 8192, 301
-    off = np.array([0 if k % 2 == 0 else T for k in range(nsys + 1)], dtype=np.int64)
-    cap = cap_of(nsys, T)
-    ni, nf, bad = counts(off, T, cap)
-    assert ni.sum() > 10 * cap  # what the unguarded tables would have held
-    item_sys, fitem_sys, ri, rf, skipped, flagged = prepare(off, T)
-    assert flagged
-    # no entry at or past cap exists (the tables are cap long) and every entry
-    # below the prefix total was written
-    assert (item_sys[: min(ri[-1], cap)] != -2).all()
-    # systems are skipped from the first one that does not fit onwards
-    first = int(np.argmax(skipped))
-    assert skipped[first:].all() and not skipped[:first].any()
-    # the systems that fit keep their full item range, below cap
-    for s in range(first):
-        assert ri[s] + ni[s] <= cap
-        assert (item_sys[ri[s]: ri[s] + ni[s]] == s).all()
-    # the kernel serves min(prefix, cap) items; skipped ones read -1
-    served = item_sys[: min(ri[-1], cap)]
-    assert set(np.unique(served)) <= set(range(first)) | {-1}
+def test_alternating_offsets_stay_within_nsys():
+    # 0, T, 0, T, ...: systems 0, 2, 4, ... valid and T rows long (a block
+    # layout would have asked for far more entries than the tables hold), the
+    # others decreasing
+    for T in (100, 3000, 8192):
+        nsys = 301
+        off = np.array([0 if k % 2 == 0 else T for k in range(nsys + 1)], dtype=np.int64)
+        queue, lists, err = prepare(off, T)
+        assert err == ERR_BAD
+        valid = list(range(0, nsys, 2))
+        assert sorted(queue + [s for x in lists for s in x]) == valid
+
+
+def test_too_long_systems_are_flagged_not_listed():
+    off = np.array([0, 100, 100 + 8193, 100 + 8193 + 8192], dtype=np.int64)
+    queue, lists, err = prepare(off, int(off[-1]))
+    assert err == ERR_TOO_LONG
+    assert queue == [0] and lists[-1] == [2] and all(not x for x in lists[:-1])
 
 
 @pytest.mark.parametrize("seed", range(5))
@@ -111,14 +108,12 @@ def test_random_malformed_offsets_stay_in_bounds(seed):
     nsys = 500
     total = int(rng.integers(1000, 200000))
     off = rng.integers(0, total + 1, nsys + 1)
-    # some out of range, some negative
     off[rng.random(nsys + 1) < 0.02] = total + 5
     off[rng.random(nsys + 1) < 0.02] = -3
-    item_sys, fitem_sys, ri, rf, skipped, flagged = prepare(off, total)
-    cap = cap_of(nsys, total)
-    assert item_sys.size == cap and fitem_sys.size == cap
-    assert flagged  # random offsets are never monotone here
-    # a system served by the kernel fits whole below cap
-    for s in np.unique(item_sys[: min(ri[-1], cap)]):
-        if s >= 0:
-            assert ri[s + 1] <= cap
+    queue, lists, err = prepare(off, total)
+    assert err & ERR_BAD
+    # every entry names a valid system of its class, each at most once
+    seen = queue + [s for x in lists for s in x]
+    assert len(seen) == len(set(seen))
+    for s in seen:
+        assert 0 <= off[s] <= off[s + 1] <= total
