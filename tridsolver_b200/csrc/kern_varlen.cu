@@ -31,8 +31,9 @@
 // no table index can pass nsys whatever the offsets hold.
 //
 // Measured on B200 (FP64, 120 M unknowns, lengths log-uniform): 8 .. 256
-// rows 2.0 TB/s, 257 .. 1024 4.3, 1025 .. 4096 3.6, 4097 .. 8192 2.7, the
-// whole 8 .. 8192 range 2.9 TB/s algorithmic.  Before the classes (every
+// rows 2.7 TB/s, 257 .. 1024 4.3, 1025 .. 4096 3.6, 4097 .. 8192 2.7, the
+// whole 8 .. 8192 range 3.0 TB/s algorithmic (200,000 systems: 3.12 TB/s).
+// Before the classes (every
 // system past 256 rows as 256-row block items reduced, published and
 // finished by a second queue across SMs, 72 B moved per unknown) the same
 // ranges ran at 1.9, 2.3 and 2.4 TB/s, and 8 .. 8192 at 2.25.
