@@ -173,22 +173,24 @@ __device__ __forceinline__ void prefetch_system_l2(const T *p, int n) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-// Arrays staged per system: 0 a, 1 b, 2 c, 3 d (forward modes) or the
-// solution (kXAdj), 4 w (kXAdj, kXFused); the staging buffer holds
-// xcta_arrays(MODE) * warps regions of Stage::R elements.
-template <int MODE>
-constexpr int xcta_arrays() {
-  return (MODE == kXAdj || MODE == kXFused) ? 5 : 4;
-}
-
-// Issue (only) the copies of one system's arrays (n rows at off[]) into the
-// staging buffer at base.
-template <typename T, int M, int MODE, bool FULL>
-__device__ __forceinline__ void xcta_stage(T *base, const XArgs<T> &A, const int64_t (&off)[5],
-                                           const int n) {
+// One system of n rows whose arrays start at off[] (rows past n are
+// identity rows), solved by the whole CTA: the body of the strided-batch
+// kernel below and of the variable-length batch's one-CTA systems
+// (kern_varlen.cu).  prefetch() runs on every thread once the system's
+// copies are issued.  n <= blockDim.x / 32 * 32 * M.
+template <typename T, int M, int MODE, bool FULL, typename PF>
+__device__ __forceinline__ void xcta_system(const XArgs<T> &A, const int64_t (&off)[5], const int n,
+                                            PF &&prefetch) {
+  extern __shared__ __align__(16) unsigned char xcta_dyn[];
+  __shared__ T sm[128 + 32 + 2 * 16];
   const int lane = threadIdx.x & (kWarp - 1);
   const int w = threadIdx.x / kWarp;
-  const Stage<T, M> S{base, (int)(blockDim.x / kWarp)};
+  const int nw = blockDim.x / kWarp;
+  const int r0 = w * kWarp * M + lane * M;
+  const Stage<T, M> S{reinterpret_cast<T *>(xcta_dyn), nw};
+  // staged arrays: 0 a, 1 b, 2 c, 3 d (forward modes) or the solution
+  // (kXAdj), 4 w (kXAdj, kXFused)
+  constexpr bool kHasW = (MODE == kXAdj || MODE == kXFused);
   stage_in<T, M, FULL>(S, 0, w, lane, A.a + off[kA], n);
   stage_in<T, M, FULL>(S, 1, w, lane, A.b + off[kB], n);
   stage_in<T, M, FULL>(S, 2, w, lane, A.c + off[kC], n);
@@ -196,22 +198,10 @@ __device__ __forceinline__ void xcta_stage(T *base, const XArgs<T> &A, const int
     stage_in<T, M, FULL>(S, 3, w, lane, A.usol + off[kU], n);
   else
     stage_in<T, M, FULL>(S, 3, w, lane, A.d + off[kD], n);
-  if (xcta_arrays<MODE>() == 5) stage_in<T, M, FULL>(S, 4, w, lane, A.w + off[kD], n);
-}
-
-// Solve one system of n rows whose arrays start at off[] (rows past n are
-// identity rows) from the staging buffer at base, whole CTA, once its copies
-// have landed and every thread has passed a CTA barrier since.
-// n <= blockDim.x / 32 * 32 * M.
-template <typename T, int M, int MODE, bool FULL>
-__device__ __forceinline__ void xcta_solve_staged(T *base, const XArgs<T> &A,
-                                                  const int64_t (&off)[5], const int n) {
-  __shared__ T sm[128 + 32 + 2 * 16];
-  const int lane = threadIdx.x & (kWarp - 1);
-  const int w = threadIdx.x / kWarp;
-  const int nw = blockDim.x / kWarp;
-  const int r0 = w * kWarp * M + lane * M;
-  const Stage<T, M> S{base, nw};
+  if (kHasW) stage_in<T, M, FULL>(S, 4, w, lane, A.w + off[kD], n);
+  prefetch();
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();  // neighbouring rows are read across warp regions
 
   const T *ra = S.region(0, w) + lane * (M + 1);
   const T *rb = S.region(1, w) + lane * (M + 1);
@@ -340,21 +330,6 @@ __device__ __forceinline__ void xcta_solve_staged(T *base, const XArgs<T> &A,
   if (A.gd) stage_out<T, M, false, FULL>(S, 4, w, lane, gsol, A.gd + off[kD], n);
 }
 
-// One system, staged and solved by the whole CTA: the body of the
-// strided-batch kernel below.  prefetch() runs on every thread once the
-// system's copies are issued.
-template <typename T, int M, int MODE, bool FULL, typename PF>
-__device__ __forceinline__ void xcta_system(const XArgs<T> &A, const int64_t (&off)[5], const int n,
-                                            PF &&prefetch) {
-  extern __shared__ __align__(16) unsigned char xcta_dyn[];
-  T *base = reinterpret_cast<T *>(xcta_dyn);
-  xcta_stage<T, M, MODE, FULL>(base, A, off, n);
-  prefetch();
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-  __syncthreads();  // neighbouring rows are read across warp regions
-  xcta_solve_staged<T, M, MODE, FULL>(base, A, off, n);
-}
-
 // The strided-batch kernel: CTA = system blockIdx.x; thread 0 warms L2 with
 // the system `dist` CTAs ahead.  Register use bounded by its launch bounds
 // (MAXW warps, MINB CTAs per SM).
@@ -449,47 +424,41 @@ cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, int chunk, cudaStream_
 // bucketed by the warps they need at 16 rows per lane (W = ceil(n / 512),
 // bucket W-1 of lists / counts): one persistent launch per bucket, CTA = W
 // warps, each CTA looping over the bucket's systems (every row read once,
-// as in the strided batch).  Two staging buffers: the next system's copies
-// are issued into one while the current system is solved from the other.
+// as in the strided batch), thread 0 warming L2 with its next system.
+template <typename T>
+__device__ __forceinline__ void prefetch_rows_l2(const T *p, int n) {
+  // the 16-byte aligned interior of the rows, one bulk prefetch
+  const uintptr_t b = ((uintptr_t)p + 15) & ~(uintptr_t)15;
+  const uintptr_t e = (uintptr_t)(p + n) & ~(uintptr_t)15;
+  if (e > b)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b), "r"((uint32_t)(e - b))
+                 : "memory");
+}
+
 template <typename T, int MAXW, int MINB>
 __global__ void __launch_bounds__(MAXW * 32, MINB)
     xcta_varlen_kernel(XArgs<T> A, const int64_t *__restrict__ offsets,
                        const int *__restrict__ list, const unsigned *__restrict__ count) {
-  extern __shared__ __align__(16) unsigned char xcv_dyn[];
-  T *buf[2] = {reinterpret_cast<T *>(xcv_dyn),
-               reinterpret_cast<T *>(xcv_dyn) + (size_t)4 * (blockDim.x / kWarp) * Stage<T, 16>::R};
   const int64_t cnt = (int64_t)*count;
-  auto sys = [&](int64_t i, int64_t (&off)[5], int &n) {
+  for (int64_t i = blockIdx.x; i < cnt; i += gridDim.x) {
     const int s = list[i];
     const int64_t lo = offsets[s];
-    n = (int)(offsets[s + 1] - lo);
-    for (int q = 0; q < 5; ++q) off[q] = lo;
-  };
-  int64_t off[5];
-  int n = 0;
-  if ((int64_t)blockIdx.x < cnt) {
-    sys(blockIdx.x, off, n);
-    xcta_stage<T, 16, kXFwd, false>(buf[0], A, off, n);
-  }
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-  int k = 0;
-  for (int64_t i = blockIdx.x; i < cnt; i += gridDim.x, k ^= 1) {
+    const int n = (int)(offsets[s + 1] - lo);
+    const int64_t off[5] = {lo, lo, lo, lo, lo};
     const int64_t nxt = i + gridDim.x;
-    int64_t noff[5];
-    int nn = 0;
-    if (nxt < cnt) {
-      sys(nxt, noff, nn);
-      xcta_stage<T, 16, kXFwd, false>(buf[k ^ 1], A, noff, nn);
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this system's copies
-    __syncthreads();
-    xcta_solve_staged<T, 16, kXFwd, false>(buf[k], A, off, n);
-    __syncthreads();  // buf[k] is refilled two systems later
-    for (int q = 0; q < 5; ++q) off[q] = noff[q];
-    n = nn;
+    xcta_system<T, 16, kXFwd, false>(A, off, n, [&] {
+      if (threadIdx.x == 0 && nxt < cnt) {
+        const int s2 = list[nxt];
+        const int64_t lo2 = offsets[s2];
+        const int n2 = (int)(offsets[s2 + 1] - lo2);
+        prefetch_rows_l2(A.a + lo2, n2);
+        prefetch_rows_l2(A.b + lo2, n2);
+        prefetch_rows_l2(A.c + lo2, n2);
+        prefetch_rows_l2(A.d + lo2, n2);
+      }
+    });
+    __syncthreads();  // the staged regions are refilled for the next system
   }
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 template <typename T, int MAXW, int MINB>
@@ -497,12 +466,12 @@ static cudaError_t launch_xcta_varlen_w(const XArgs<T> &A, const int64_t *offset
                                         const unsigned *count, int W, int dev, int sms,
                                         cudaStream_t st) {
   auto kern = xcta_varlen_kernel<T, MAXW, MINB>;
-  const size_t smem = (size_t)2 * 4 * W * Stage<T, 16>::R * sizeof(T);  // two staging buffers
+  const size_t smem = (size_t)4 * W * Stage<T, 16>::R * sizeof(T);
   static bool attr_set[64] = {};
   static int per_sm[64][9] = {};  // resident CTAs per SM by W, per device
   if (!attr_set[dev]) {
     const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               2 * 4 * MAXW * Stage<T, 16>::R * (int)sizeof(T));
+                                               4 * MAXW * Stage<T, 16>::R * (int)sizeof(T));
     if (e != cudaSuccess) return e;
     attr_set[dev] = true;
   }
