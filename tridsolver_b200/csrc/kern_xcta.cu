@@ -404,14 +404,22 @@ cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, int chunk, cudaStream_
   if (M == 8)
     return warps <= 8 ? launch_xcta_m<T, 8, MODE, 8>(g, A, warps, st)
                       : launch_xcta_m<T, 8, MODE, 16>(g, A, warps, st);
-  // forward modes up to 1024 rows (two warps): registers capped for 6 CTAs
-  // per SM (the adjoint modes spill under such caps, and measured slower);
-  // systems of whole warp blocks (n = 512 * warps) drop every row guard
+  // forward modes up to 3072 rows (six warps): registers capped near 170
+  // (6 CTAs per SM up to two warps, 3 up to four, 2 up to six; uncapped the
+  // 3..6-warp CTAs take 254 registers and fit once or twice per SM); the
+  // adjoint modes spill under such caps and measured slower.  Systems of
+  // whole warp blocks (n = 512 * warps) drop every row guard.
   const bool full = n == warps * 32 * 16;
   if constexpr (MODE == kXFwd || MODE == kXFwdInc) {
     if (warps <= 2)
       return full ? launch_xcta_m<T, 16, MODE, 2, 6, true>(g, A, warps, st)
                   : launch_xcta_m<T, 16, MODE, 2, 6>(g, A, warps, st);
+    if (warps <= 4)
+      return full ? launch_xcta_m<T, 16, MODE, 4, 3, true>(g, A, warps, st)
+                  : launch_xcta_m<T, 16, MODE, 4, 3>(g, A, warps, st);
+    if (warps <= 6)
+      return full ? launch_xcta_m<T, 16, MODE, 6, 2, true>(g, A, warps, st)
+                  : launch_xcta_m<T, 16, MODE, 6, 2>(g, A, warps, st);
   }
   if constexpr (MODE == kXFused) {  // (the adjoint measured slower without guards)
     if (full) return launch_xcta_m<T, 16, MODE, 8, 1, true>(g, A, warps, st);
@@ -499,11 +507,19 @@ cudaError_t launch_xcta_varlen(const T *a, const T *b, const T *c, T *d, const i
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
   const XArgs<T> A{a, b, c, d, nullptr, nullptr, d, nullptr, nullptr, nullptr, nullptr};
-  // register caps as for the strided batch: 6 CTAs per SM up to two warps
+  // register caps as for the strided batch: near 170 registers up to six
+  // warps (6, 3 and 2 CTAs per SM for 2, 4 and 6 warps)
   for (int W = kVarlenCtaBuckets; W >= 1; --W) {
     const int *list = lists + (size_t)(W - 1) * (size_t)list_stride;
-    e = W <= 2 ? launch_xcta_varlen_w<T, 2, 6>(A, offsets, list, counts + W - 1, W, dev, sms, st)
-               : launch_xcta_varlen_w<T, 8, 1>(A, offsets, list, counts + W - 1, W, dev, sms, st);
+    const unsigned *cnt = counts + W - 1;
+    if (W <= 2)
+      e = launch_xcta_varlen_w<T, 2, 6>(A, offsets, list, cnt, W, dev, sms, st);
+    else if (W <= 4)
+      e = launch_xcta_varlen_w<T, 4, 3>(A, offsets, list, cnt, W, dev, sms, st);
+    else if (W <= 6)
+      e = launch_xcta_varlen_w<T, 6, 2>(A, offsets, list, cnt, W, dev, sms, st);
+    else
+      e = launch_xcta_varlen_w<T, 8, 1>(A, offsets, list, cnt, W, dev, sms, st);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
