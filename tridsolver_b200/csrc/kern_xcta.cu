@@ -396,6 +396,24 @@ cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, int chunk, cudaStream_
   // 4096 -- else 8 or 4); at most 16 warps, so n <= 512*M
   const int n = g.n;
   if (n > 4096 || g.nsys > 0x7fffffff) return cudaErrorNotSupported;
+  if constexpr (MODE == kXFwd || MODE == kXFwdInc) {
+    // 12 rows per lane (384 per warp) where that pads fewer rows than 16
+    // and takes at most four warps: the kernel is issue-bound on row slots
+    // (warps x 32 x M), not on the system's rows, e.g. 700 rows fill 768
+    // slots instead of 1024 (B200, same box: 257 rows 4.04 -> 4.72 TB/s, 700
+    // 4.64 -> 5.21, 1100 4.86 -> 5.49; with five 12-row warps, 1700 and 1920
+    // rows ran 14-20% slower than four 16-row warps, so those keep 16)
+    const int w12 = (n + 383) / 384, w16 = (n + 511) / 512;
+    if (chunk == 12 || (chunk == 0 && n > 256 && w12 <= 4 && w12 * 384 < w16 * 512)) {
+      if (w12 > 4) return cudaErrorNotSupported;
+      const bool full12 = n == w12 * 384;
+      if (w12 <= 2)
+        return full12 ? launch_xcta_m<T, 12, MODE, 2, 6, true>(g, A, w12, st)
+                      : launch_xcta_m<T, 12, MODE, 2, 6>(g, A, w12, st);
+      return full12 ? launch_xcta_m<T, 12, MODE, 4, 3, true>(g, A, w12, st)
+                    : launch_xcta_m<T, 12, MODE, 4, 3>(g, A, w12, st);
+    }
+  }
   int M = chunk;
   if (M != 4 && M != 8 && M != 16) M = (n > 256) ? 16 : (n > 128 ? 8 : 4);
   while (n > 512 * M) M *= 2;
@@ -443,7 +461,7 @@ __device__ __forceinline__ void prefetch_rows_l2(const T *p, int n) {
                  : "memory");
 }
 
-template <typename T, int MAXW, int MINB>
+template <typename T, int M, int MAXW, int MINB>
 __global__ void __launch_bounds__(MAXW * 32, MINB)
     xcta_varlen_kernel(XArgs<T> A, const int64_t *__restrict__ offsets,
                        const int *__restrict__ list, const unsigned *__restrict__ count) {
@@ -454,7 +472,7 @@ __global__ void __launch_bounds__(MAXW * 32, MINB)
     const int n = (int)(offsets[s + 1] - lo);
     const int64_t off[5] = {lo, lo, lo, lo, lo};
     const int64_t nxt = i + gridDim.x;
-    xcta_system<T, 16, kXFwd, false>(A, off, n, [&] {
+    xcta_system<T, M, kXFwd, false>(A, off, n, [&] {
       if (threadIdx.x == 0 && nxt < cnt) {
         const int s2 = list[nxt];
         const int64_t lo2 = offsets[s2];
@@ -469,17 +487,17 @@ __global__ void __launch_bounds__(MAXW * 32, MINB)
   }
 }
 
-template <typename T, int MAXW, int MINB>
+template <typename T, int M, int MAXW, int MINB>
 static cudaError_t launch_xcta_varlen_w(const XArgs<T> &A, const int64_t *offsets, const int *list,
                                         const unsigned *count, int W, int dev, int sms,
                                         cudaStream_t st) {
-  auto kern = xcta_varlen_kernel<T, MAXW, MINB>;
-  const size_t smem = (size_t)4 * W * Stage<T, 16>::R * sizeof(T);
+  auto kern = xcta_varlen_kernel<T, M, MAXW, MINB>;
+  const size_t smem = (size_t)4 * W * Stage<T, M>::R * sizeof(T);
   static bool attr_set[64] = {};
   static int per_sm[64][9] = {};  // resident CTAs per SM by W, per device
   if (!attr_set[dev]) {
     const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               4 * MAXW * Stage<T, 16>::R * (int)sizeof(T));
+                                               4 * MAXW * Stage<T, M>::R * (int)sizeof(T));
     if (e != cudaSuccess) return e;
     attr_set[dev] = true;
   }
@@ -508,20 +526,24 @@ cudaError_t launch_xcta_varlen(const T *a, const T *b, const T *c, T *d, const i
   if (e != cudaSuccess) return e;
   const XArgs<T> A{a, b, c, d, nullptr, nullptr, d, nullptr, nullptr, nullptr, nullptr};
   // register caps as for the strided batch: near 170 registers up to six
-  // warps (6, 3 and 2 CTAs per SM for 2, 4 and 6 warps)
+  // warps (6, 3 and 2 CTAs per SM for 2, 4 and 6 warps).  (Buckets at 12
+  // rows per lane where that pads fewer rows, as the strided batch chooses,
+  // measured no gain here: 300-row systems +8%, 1025..4096 rows -2%, the
+  // 8..8192 mix -0.7%, three more launches against the padding saved.)
   for (int W = kVarlenCtaBuckets; W >= 1; --W) {
     const int *list = lists + (size_t)(W - 1) * (size_t)list_stride;
     const unsigned *cnt = counts + W - 1;
     if (W <= 2)
-      e = launch_xcta_varlen_w<T, 2, 6>(A, offsets, list, cnt, W, dev, sms, st);
+      e = launch_xcta_varlen_w<T, 16, 2, 6>(A, offsets, list, cnt, W, dev, sms, st);
     else if (W <= 4)
-      e = launch_xcta_varlen_w<T, 4, 3>(A, offsets, list, cnt, W, dev, sms, st);
+      e = launch_xcta_varlen_w<T, 16, 4, 3>(A, offsets, list, cnt, W, dev, sms, st);
     else if (W <= 6)
-      e = launch_xcta_varlen_w<T, 6, 2>(A, offsets, list, cnt, W, dev, sms, st);
+      e = launch_xcta_varlen_w<T, 16, 6, 2>(A, offsets, list, cnt, W, dev, sms, st);
     else
-      e = launch_xcta_varlen_w<T, 8, 1>(A, offsets, list, cnt, W, dev, sms, st);
+      e = launch_xcta_varlen_w<T, 16, 8, 1>(A, offsets, list, cnt, W, dev, sms, st);
     if (e != cudaSuccess) return e;
   }
+
   return cudaSuccess;
 }
 
