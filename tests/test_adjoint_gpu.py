@@ -183,6 +183,19 @@ def test_long_axis0(dtype, n, inc, method):
 
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("n", [257, 300, 384, 385, 700, 768, 1100, 1152, 1153, 1536, 2048, 2500,
+                               3000, 3072, 3073, 4000, 4096])
+@pytest.mark.parametrize("inc", [False, True])
+def test_one_cta_row_layouts(dtype, n, inc):
+    """Axis-0 systems solved whole by one CTA: 12 rows per lane where that
+    pads fewer rows (257..384, 513..768, 1025..1152), 16 otherwise, with the
+    register-capped variants for 3..6 warps (1025..3072 rows) and the
+    uncapped ones past them; pads[0] = n + 3 keeps the rows off the TMA grid."""
+    from test_scalar_gpu import run_case
+    run_case(np.random.default_rng(n + inc), dtype, [n, 23], 0, pads=[n + 3, 23], inc=inc)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
 @pytest.mark.parametrize("n,nsys", [(4097, 400), (5000, 300), (65536, 20), (65535, 19)])
 @pytest.mark.parametrize("inc", [False, True])
 def test_long_axis0_many_steps(dtype, n, nsys, inc):
