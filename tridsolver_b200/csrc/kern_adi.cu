@@ -53,58 +53,17 @@ __device__ __forceinline__ void adi_row(const AdiArgs<T> &g, int axis, int i, in
 }
 
 // ------------------------------------------------------------- x lines --
+// x lines, one warp per line (4 per CTA), every load coalesced: lane l
+// holds the points i = q*32 + l (q < M) of the right-hand side -- with
+// STENCIL formed there from the five lines the 7-point stencil reads (the
+// line, j-1, j+1, k-1, k+1; the x neighbours i-1, i+1 by shuffles) -- which
+// passes through the warp's shared-memory slot into the lane-per-chunk layout
+// of the solve (lane l: points l*M .. l*M+M-1; point i at i + i/M,
+// conflict-free both ways); the solution leaves the same way.  (Reading the
+// stencil lane by lane -- 4 consecutive points per lane, 7 loads each,
+// strided across the warp -- took 49-51 us per 128^3 step against 45.)
 template <typename T, int M, bool STENCIL, bool TRANS>
 __global__ void __launch_bounds__(128) adi_x_kernel(AdiArgs<T> g) {
-  const int lane = threadIdx.x & (kWarp - 1);
-  const int64_t line = (int64_t)blockIdx.x * 4 + threadIdx.x / kWarp;
-  if (line >= (int64_t)g.ny * g.nz) return;
-  const int j = (int)(line % g.ny), k = (int)(line / g.ny);
-  const int64_t sxy = (int64_t)g.nx * g.ny;
-  const int64_t base = (int64_t)k * sxy + (int64_t)j * g.nx;
-  T al[M], be[M], ga[M], de[M];
-#pragma unroll
-  for (int q = 0; q < M; ++q) {
-    const int i = lane * M + q;
-    if (i < g.nx) {
-      adi_row<T, TRANS>(g, 0, i, j, k, al[q], be[q], ga[q]);
-      const int64_t p = base + i;
-      if (STENCIL) {
-        de[q] = adi_inside(g, i, j, k)
-                    ? g.lam * (g.rhs[p - 1] + g.rhs[p + 1] + g.rhs[p - g.nx] + g.rhs[p + g.nx] +
-                               g.rhs[p - sxy] + g.rhs[p + sxy] - T(6) * g.rhs[p])
-                    : T(0);
-      } else {
-        de[q] = g.rhs[p];
-      }
-    } else {
-      al[q] = T(0);
-      be[q] = T(1);
-      ga[q] = T(0);
-      de[q] = T(0);
-    }
-  }
-  Row<T> F, L;
-  chunk_reduce<T, M>(al, be, ga, de, F, L);
-  T xF, xL;
-  warp_interface_solve(F, L, xF, xL, lane);
-  chunk_backsub<T, M>(al, ga, de, xF, xL);
-#pragma unroll
-  for (int q = 0; q < M; ++q) {
-    const int i = lane * M + q;
-    if (i < g.nx) g.out[base + i] = de[q];
-  }
-}
-
-// The x solve with the stencil fused, every load coalesced: lane l holds
-// the points i = q*32 + l (q < M) of the five lines the 7-point stencil needs
-// (the line, j-1, j+1, k-1, k+1), forms r there (the x neighbours i-1, i+1
-// by shuffles), passes r through the warp's shared-memory slot into the
-// lane-per-chunk layout of the solve (lane l: points l*M .. l*M+M-1; point i
-// at i + i/M, conflict-free both ways), and the solution leaves the same
-// way.  (adi_x_kernel with STENCIL read the stencil lane by lane: 4 points
-// per lane, 7 loads each, strided across the warp.)
-template <typename T, int M>
-__global__ void __launch_bounds__(128) adi_xs_kernel(AdiArgs<T> g) {
   __shared__ T sbuf[4][32 * (M + 1)];
   constexpr unsigned kFull = 0xffffffffu;
   const int lane = threadIdx.x & (kWarp - 1);
@@ -116,8 +75,15 @@ __global__ void __launch_bounds__(128) adi_xs_kernel(AdiArgs<T> g) {
   const int64_t base = (int64_t)k * sxy + (int64_t)j * g.nx;
   const T *u = g.rhs + base;
   T *sb = sbuf[wi];
+  if (!STENCIL) {
+#pragma unroll
+    for (int q = 0; q < M; ++q) {
+      const int i = q * kWarp + lane;
+      sb[i + i / M] = i < g.nx ? u[i] : T(0);
+    }
+  }
   // interior line (its points off the x faces are interior points)
-  const bool line_in = j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1;
+  const bool line_in = STENCIL && j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1;
   T c[M];
 #pragma unroll
   for (int q = 0; q < M; ++q) {
@@ -125,7 +91,7 @@ __global__ void __launch_bounds__(128) adi_xs_kernel(AdiArgs<T> g) {
     c[q] = (line_in && i < g.nx) ? u[i] : T(0);
   }
 #pragma unroll
-  for (int q = 0; q < M; ++q) {
+  for (int q = 0; STENCIL && q < M; ++q) {
     const int i = q * kWarp + lane;
     T left = __shfl_up_sync(kFull, c[q], 1);
     const T lq = __shfl_sync(kFull, c[q > 0 ? q - 1 : 0], kWarp - 1);
@@ -145,7 +111,7 @@ __global__ void __launch_bounds__(128) adi_xs_kernel(AdiArgs<T> g) {
   for (int q = 0; q < M; ++q) {
     const int i = lane * M + q;
     if (i < g.nx) {
-      adi_row<T, false>(g, 0, i, j, k, al[q], be[q], ga[q]);
+      adi_row<T, TRANS>(g, 0, i, j, k, al[q], be[q], ga[q]);
       de[q] = sb[lane * (M + 1) + q];
     } else {
       al[q] = T(0);
@@ -346,7 +312,7 @@ static cudaError_t adi_x_m(const AdiArgs<T> &g, bool stencil, bool trans, bool i
                            cudaStream_t st) {
   const int64_t lines = (int64_t)g.ny * g.nz;
   const dim3 grid((unsigned)((lines + 3) / 4)), block(128);
-  if (stencil && !trans && !inc) adi_xs_kernel<T, M><<<grid, block, 0, st>>>(g);
+  if (stencil && !trans && !inc) adi_x_kernel<T, M, true, false><<<grid, block, 0, st>>>(g);
   else if (!stencil && !trans && !inc) adi_x_kernel<T, M, false, false><<<grid, block, 0, st>>>(g);
   else if (!stencil && trans && !inc) adi_x_kernel<T, M, false, true><<<grid, block, 0, st>>>(g);
   else return cudaErrorInvalidValue;
