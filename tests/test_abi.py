@@ -206,6 +206,11 @@ def test_method_override_and_query():
     assert (m.value, ch.value) == (2, 8)
     assert L.tridQueryMethod(8, 0, 65536, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
     assert (m.value, ch.value) == (2, 8)
+    # FP32 along axis 0: 512-row blocks
+    assert L.tridQueryMethod(4, 0, 65536, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+    assert (m.value, ch.value) == (2, 16)
+    assert L.tridQueryMethod(4, 1, 65536, ctypes.byref(m), ctypes.byref(ch), ctypes.byref(spc)) == 0
+    assert (m.value, ch.value) == (2, 8)
     # strided axes, every stride class: streamed tiles of one 128-byte line of
     # systems (16 FP64, 32 FP32)
     for cls in (1, 2, 3):
