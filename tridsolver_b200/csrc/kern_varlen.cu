@@ -49,7 +49,7 @@ constexpr int kVLShort = kVarlenShort;   // longest system of the short queue
 constexpr int kVLMid = 512 * kVarlenCtaBuckets;  // longest system of the one-CTA buckets
 constexpr int kVLMaxBlocks = 32;         // longest solvable system: 32 blocks
 constexpr int kVLWarps = 8;              // warps per CTA of the short queue
-constexpr int kVLLongWarps = 8;          // warps per CTA of the long systems
+constexpr int kVLLongWarps = 4;          // warps per CTA of the long systems (four CTAs per SM)
 constexpr int kVLRegion = 32 * (8 + 1);  // elements per staged array and warp
 constexpr int kVLLists = kVarlenCtaBuckets + 1;  // the one-CTA buckets, then the long list
 constexpr unsigned kErrBadOffsets = 4u;
@@ -377,8 +377,11 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_short_kernel(VLArgs<T
 
 // ----------------------------------------------------------- long systems --
 // Systems of 4097 .. 8192 rows (17 .. 32 blocks of 256): one CTA of
-// kVLLongWarps warps per system, two CTAs per SM, each looping over the
-// long systems' list.  Thread 0 first asks L2 for the whole system (one bulk
+// kVLLongWarps warps per system, four CTAs per SM, each looping over the
+// long systems' list (four 4-warp CTAs per SM measured ahead of two of 8
+// warps by 2-7% on 4097..8192-row mixes, 5% behind on uniform 8192-row
+// batches, whose four systems per SM crowd L2 before their second pass; one
+// CTA of 16 warps and three or two 4-warp CTAs per SM were slower).  Thread 0 first asks L2 for the whole system (one bulk
 // prefetch per array, so its DRAM reads are all in flight at once); every
 // warp reduces its blocks (warp w: blocks w, w+8, ...) to their block rows
 // in shared memory; warp 0 solves the block system (lane t = block t); every
@@ -397,7 +400,7 @@ __device__ __forceinline__ void vl_prefetch_rows(const T *p, int64_t n) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kVLLongWarps * 32, 2)
+__global__ void __launch_bounds__(kVLLongWarps * 32, 4)
     varlen_long_kernel(VLArgs<T> A, const int *__restrict__ list, const unsigned *__restrict__ count) {
   extern __shared__ __align__(16) unsigned char vll_dyn[];
   __shared__ T brow[kVLMaxBlocks * 8];  // block rows; then the block unknowns at [8t], [8t+1]
@@ -509,9 +512,11 @@ static cudaError_t launch_varlen_work(const VLArgs<T> &A, const VLSpace &sp, int
       launch_xcta_varlen<T>(A.a, A.b, A.c, A.d, A.offsets, sp.lists, nsys, sp.list_count, st);
   if (e != cudaSuccess) return e;
   int grid = 0;
-  e = persistent_grid(varlen_long_kernel<T>, kVLLongWarps * 32, smem, grid, attr_long);
+  const int lsmem = kVLLongWarps * 5 * kVLRegion * (int)sizeof(T);
+  e = persistent_grid(varlen_long_kernel<T>, kVLLongWarps * 32, lsmem, grid, attr_long);
   if (e != cudaSuccess) return e;
-  varlen_long_kernel<T><<<(unsigned)grid, kVLLongWarps * 32, smem, st>>>(
+
+  varlen_long_kernel<T><<<(unsigned)grid, kVLLongWarps * 32, lsmem, st>>>(
       A, sp.lists + (size_t)(kClsLong - 1) * nsys, sp.list_count + (kClsLong - 1));
   e = persistent_grid(varlen_short_kernel<T>, kVLWarps * 32, smem, grid, attr_short);
   if (e != cudaSuccess) return e;
