@@ -404,8 +404,7 @@ cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, int chunk, cudaStream_
     // 4.64 -> 5.21, 1100 4.86 -> 5.49; with five 12-row warps, 1700 and 1920
     // rows ran 14-20% slower than four 16-row warps, so those keep 16)
     const int w12 = (n + 383) / 384, w16 = (n + 511) / 512;
-    if (chunk == 12 || (chunk == 0 && n > 256 && w12 <= 4 && w12 * 384 < w16 * 512)) {
-      if (w12 > 4) return cudaErrorNotSupported;
+    if (chunk == 0 && n > 256 && w12 <= 4 && w12 * 384 < w16 * 512) {
       const bool full12 = n == w12 * 384;
       if (w12 <= 2)
         return full12 ? launch_xcta_m<T, 12, MODE, 2, 6, true>(g, A, w12, st)
