@@ -25,6 +25,16 @@
  *     managed memory) aligned to their element size.
  *   - Work is enqueued on the calling thread's stream (tridSetStream, default
  *     the legacy default stream) and the call returns without synchronising.
+ *   - Solves that need device scratch (systems too long for one pass, which
+ *     are solved in blocks; method 1; the variable-length batch; the block
+ *     solver; ADI without a work buffer) take it from a buffer the library
+ *     keeps per device and stream, grown on demand (a growing call waits for
+ *     that stream's queued work), so calls on different streams or threads
+ *     may run concurrently.  A call made while its stream is being captured
+ *     into a CUDA graph allocates and frees its scratch in stream order
+ *     instead (graph memory nodes), so a captured call needs no earlier
+ *     warm-up call and the graph holds no pointer to the kept buffers.
+ *     tridReleaseScratch frees the kept buffers.
  *
  * Differences from the reference, all on error paths: invalid arguments
  * return TRID_STATUS_INVALID_VALUE instead of printing and calling exit()
@@ -294,8 +304,7 @@ TRID_EXTERN_C tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const do
  *
  * tridXadiSteps: nsteps steps u <- u + Z^{-1} Y^{-1} X^{-1} rhs(u), three
  *   launches per step (stencil fused into the x solve, u += in the z solve).
- *   work holds 2*nx*ny*nz elements (NULL = library scratch; pass a buffer when
- *   capturing the calls into a CUDA graph).
+ *   work holds 2*nx*ny*nz elements (NULL = library scratch).
  * tridXadiSolve: one axis solve out = T^{-1} rhs with T the generated
  *   operator along `axis` (0, 1, 2); stencil=1 (axis 0 only) takes u in rhs
  *   and solves for the step RHS; transpose=1 solves with T^T (adjoint);
@@ -338,6 +347,12 @@ TRID_EXTERN_C void initTridMultiDimBatchSolve(int ndim, int *dims, int *pads);
  * NULL = legacy default stream). */
 TRID_EXTERN_C tridStatus_t tridSetStream(void *stream);
 TRID_EXTERN_C void *tridGetStream(void);
+
+/* Free the scratch buffers the library keeps for the current device (every
+ * stream's), after waiting for the device to finish its queued work.  Call
+ * it when no other thread is calling into the library on this device; the
+ * next solve that needs scratch allocates again. */
+TRID_EXTERN_C tridStatus_t tridReleaseScratch(void);
 
 /* Human-readable name of a status code. */
 TRID_EXTERN_C const char *tridGetStatusString(tridStatus_t status);

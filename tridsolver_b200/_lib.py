@@ -60,6 +60,7 @@ _COMMON = {
     "initTridMultiDimBatchSolve": (None, [c_int, ip, ip]),
     "tridSetStream": (c_int, [vp]),
     "tridGetStream": (vp, []),
+    "tridReleaseScratch": (c_int, []),
     "tridGetStatusString": (ctypes.c_char_p, [c_int]),
     "tridSetMethod": (c_int, [c_int, c_int, c_int]),
     "tridGetDeviceErrors": (c_int, [ctypes.POINTER(ctypes.c_uint)]),

@@ -1,12 +1,15 @@
 // Scalar strided-batch C ABI (9-argument form over device pointers) and the
-// library's host runtime: per-thread stream and method override, per-device
+// library's host runtime: per-thread stream and method override, per-stream
 // scratch, tuning table, argument validation and dispatch.
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
+#include <thread>
+#include <tuple>
 #include <vector>
 
 #include "dispatch.cuh"
@@ -25,21 +28,26 @@ struct ScratchBuf {
 };
 constexpr int kScratchLevels = 5;
 constexpr int kSplitScratch = kScratchLevels - 1;  // split finish (the solves recurse below it)
+// One buffer per (device, stream, nesting level): calls on different streams
+// may run at the same time on the GPU, so they never share scratch.  The
+// per-thread default stream is one stream per thread under a single handle,
+// so for it the calling thread is part of the key.
+using ScratchKey = std::tuple<int, uintptr_t, std::thread::id, int>;
 static std::mutex g_scratch_mu;
-static std::vector<ScratchBuf> g_scratch;  // [device * kScratchLevels + level]
+static std::map<ScratchKey, ScratchBuf> g_scratch;
 
-void *scratch(size_t bytes, int level) {
+static void *persistent_scratch(size_t bytes, int level, cudaStream_t st) {
   int dev = 0;
-  if (level < 0 || level >= kScratchLevels) return nullptr;
   if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  const ScratchKey key{dev, (uintptr_t)st,
+                       st == cudaStreamPerThread ? std::this_thread::get_id() : std::thread::id(),
+                       level};
   std::lock_guard<std::mutex> lk(g_scratch_mu);
-  const size_t slot = (size_t)dev * kScratchLevels + level;
-  if (g_scratch.size() <= slot) g_scratch.resize(slot + 1);
-  ScratchBuf &s = g_scratch[slot];
+  ScratchBuf &s = g_scratch[key];
   if (s.bytes >= bytes) return s.ptr;
   if (s.ptr) {
-    // kernels already queued may still read the old buffer
-    cudaDeviceSynchronize();
+    // only work queued on this stream may still read the old buffer
+    if (cudaStreamSynchronize(st) != cudaSuccess) return nullptr;
     cudaFree(s.ptr);
     s.ptr = nullptr;
     s.bytes = 0;
@@ -52,6 +60,48 @@ void *scratch(size_t bytes, int level) {
   s.ptr = p;
   s.bytes = bytes;
   return p;
+}
+
+Scratch::Scratch(size_t bytes, int level, cudaStream_t stream) : stream_(stream) {
+  if (bytes == 0 || level < 0 || level >= kScratchLevels) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream_, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    cs = cudaStreamCaptureStatusNone;
+  }
+  if (cs == cudaStreamCaptureStatusNone) {
+    ptr_ = persistent_scratch(bytes, level, stream_);
+    return;
+  }
+  // captured: allocate and free in stream order (graph memory nodes)
+  if (cudaMallocAsync(&ptr_, bytes, stream_) != cudaSuccess) {
+    cudaGetLastError();
+    ptr_ = nullptr;
+    return;
+  }
+  stream_ordered_ = true;
+}
+
+Scratch::~Scratch() {
+  if (stream_ordered_ && ptr_) cudaFreeAsync(ptr_, stream_);
+}
+
+// Frees every scratch buffer of the current device (after the work queued on
+// it has finished).
+static tridStatus_t release_scratch() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return TRID_STATUS_EXECUTION_FAILED;
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (cudaDeviceSynchronize() != cudaSuccess) return TRID_STATUS_EXECUTION_FAILED;
+  for (auto it = g_scratch.begin(); it != g_scratch.end();) {
+    if (std::get<0>(it->first) == dev) {
+      if (it->second.ptr) cudaFree(it->second.ptr);
+      it = g_scratch.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  return TRID_STATUS_SUCCESS;
 }
 
 static std::mutex g_err_mu;
@@ -300,7 +350,8 @@ static tridStatus_t run_general(const Geom &g, GenArgs<T> A, int axis, int chunk
                : TRID_STATUS_EXECUTION_FAILED;
   }
   const int64_t len = g.nsys * 2 * nblk;
-  T *red = (T *)scratch((size_t)4 * len * sizeof(T), level);
+  const Scratch sc((size_t)4 * len * sizeof(T), level, stream);
+  T *red = (T *)sc.get();
   if (!red) return TRID_STATUS_ALLOC_FAILED;
   A.red = red;
   if (launch_general_phase<T, MODE>(g, A, ax, chunk, spc, kGenReduce, stream) != cudaSuccess)
@@ -410,7 +461,8 @@ static tridStatus_t solve_level(const T *a, const T *b, const T *c, T *d, T *u, 
     const size_t per_sys = (size_t)2 * g.n * sizeof(T);
     int64_t ws = (int64_t)(((size_t)1 << 30) / per_sys);
     ws = std::max<int64_t>(1, std::min<int64_t>(ws, g.nsys));
-    T *work = (T *)scratch(per_sys * (size_t)ws, level);
+    const Scratch sc(per_sys * (size_t)ws, level, stream);
+    T *work = (T *)sc.get();
     if (!work) return TRID_STATUS_ALLOC_FAILED;
     e = launch_generic<T, INC>(g, a, b, c, d, u, work, ws, stream);
   }
@@ -586,11 +638,10 @@ static tridStatus_t split_finish(const T *a, const T *b, const T *c, T *d, T *u,
   if (g.nsys == 0) return TRID_STATUS_SUCCESS;
   if (g.n < 2) return TRID_STATUS_INVALID_VALUE;
   const cudaStream_t stream = current_stream();
-  T *saved = nullptr;  // Inc leaves d as it was: the patched entries come back
-  if (INC) {
-    saved = (T *)scratch((size_t)2 * g.nsys * sizeof(T), kSplitScratch);
-    if (!saved) return TRID_STATUS_ALLOC_FAILED;
-  }
+  // Inc leaves d as it was: the patched entries come back
+  const Scratch sc(INC ? (size_t)2 * g.nsys * sizeof(T) : 0, kSplitScratch, stream);
+  T *saved = (T *)sc.get();
+  if (INC && !saved) return TRID_STATUS_ALLOC_FAILED;
   if (launch_split_patch<T>(g, a, c, d, bnd_all, nranks, rank, saved, stream) != cudaSuccess)
     return TRID_STATUS_EXECUTION_FAILED;
   st = solve_level<T, INC>(a, b, c, d, u, ndim, solvedim, dims, p, nullptr, 0, 0);
@@ -742,6 +793,8 @@ extern "C" tridStatus_t tridSetStream(void *stream) {
 }
 
 extern "C" void *tridGetStream(void) { return (void *)tl_stream; }
+
+extern "C" tridStatus_t tridReleaseScratch(void) { return release_scratch(); }
 
 extern "C" const char *tridGetStatusString(tridStatus_t s) {
   switch (s) {

@@ -382,7 +382,8 @@ cudaError_t adi_vjp(AdiVjpArgs<T> v, T *lbar, cudaStream_t st) {
   const int64_t total = (int64_t)v.nx * v.ny * v.nz;
   int64_t blocks = (total + 255) / 256;
   if (blocks > 148 * 8) blocks = 148 * 8;
-  v.partial = (T *)scratch((size_t)blocks * sizeof(T), 0);
+  const Scratch sc((size_t)blocks * sizeof(T), 0, st);
+  v.partial = (T *)sc.get();
   if (!v.partial) return cudaErrorMemoryAllocation;
   adi_vjp_kernel<T><<<dim3((unsigned)blocks), dim3(256), 0, st>>>(v);
   adi_vjp_sum_kernel<T><<<1, 256, 0, st>>>(v.partial, (int)blocks, lbar);
@@ -414,12 +415,13 @@ static tridStatus_t adi_steps_entry(T *u, T *work, int nx, int ny, int nz, int n
                                     T cb, T cc) {
   if (!adi_dims_ok(nx, ny, nz) || !u || nsteps < 0) return TRID_STATUS_INVALID_VALUE;
   const size_t npts = (size_t)nx * ny * nz;
+  const cudaStream_t st = current_stream();
+  const Scratch sc(work ? 0 : 2 * npts * sizeof(T), 0, st);
   if (!work) {
-    work = (T *)scratch(2 * npts * sizeof(T), 0);
+    work = (T *)sc.get();
     if (!work) return TRID_STATUS_ALLOC_FAILED;
   }
   T *w1 = work, *w2 = work + npts;
-  const cudaStream_t st = current_stream();
   for (int s = 0; s < nsteps; ++s) {
     AdiArgs<T> gx = {nx, ny, nz, lam, ca, cb, cc, u, w1};
     AdiArgs<T> gy = {nx, ny, nz, lam, ca, cb, cc, w1, w2};

@@ -1447,15 +1447,17 @@ static tridStatus_t blk_solve(const T *A, const T *B, const T *C, const T *d, T 
     return TRID_STATUS_INVALID_VALUE;
   if (P == 0) return TRID_STATUS_SUCCESS;
   const size_t ne = (size_t)N * P * M * M, nv = (size_t)N * P * M;
+  const cudaStream_t st = current_stream();
+  const Scratch sc((!Cs || !ds) ? (ne + nv) * sizeof(T) : 0, 0, st);
   if (!Cs || !ds) {
-    T *w = (T *)scratch((ne + nv) * sizeof(T), 0);
+    T *w = (T *)sc.get();
     if (!w) return TRID_STATUS_ALLOC_FAILED;
     Cs = w;
     ds = w + ne;
   }
   BlkArgs<T> a = {A, B, C, d, nullptr, x, nullptr, nullptr, nullptr, nullptr, Cs, ds, N, P};
-  return launch_block<T, false>(a, M, current_stream()) == cudaSuccess ? TRID_STATUS_SUCCESS
-                                                                      : TRID_STATUS_EXECUTION_FAILED;
+  return launch_block<T, false>(a, M, st) == cudaSuccess ? TRID_STATUS_SUCCESS
+                                                         : TRID_STATUS_EXECUTION_FAILED;
 }
 
 template <typename T>
@@ -1465,11 +1467,13 @@ static tridStatus_t blk_adjoint(const T *A, const T *B, const T *C, const T *u, 
     return TRID_STATUS_INVALID_VALUE;
   if (P == 0) return TRID_STATUS_SUCCESS;
   const size_t ne = (size_t)N * P * M * M, nv = (size_t)N * P * M;
-  T *s = (T *)scratch((ne + nv) * sizeof(T), 0);
+  const cudaStream_t st = current_stream();
+  const Scratch sc((ne + nv) * sizeof(T), 0, st);
+  T *s = (T *)sc.get();
   if (!s) return TRID_STATUS_ALLOC_FAILED;
   BlkArgs<T> a = {A, B, C, w, u, nullptr, dA, dB, dC, dd, s, s + ne, N, P};
-  return launch_block<T, true>(a, M, current_stream()) == cudaSuccess ? TRID_STATUS_SUCCESS
-                                                                     : TRID_STATUS_EXECUTION_FAILED;
+  return launch_block<T, true>(a, M, st) == cudaSuccess ? TRID_STATUS_SUCCESS
+                                                        : TRID_STATUS_EXECUTION_FAILED;
 }
 
 }  // namespace tridb200

@@ -542,7 +542,8 @@ cudaError_t launch_ext(const Geom &g, int solvedim, const S *a, const S *b, cons
   const size_t per_sys = (size_t)2 * g.n * sizeof(T);
   int64_t ws = (int64_t)(((size_t)1 << 30) / per_sys);
   ws = ws < 1 ? 1 : (ws > g.nsys ? g.nsys : ws);
-  T *work = (T *)scratch(per_sys * (size_t)ws, 0);
+  const Scratch sc(per_sys * (size_t)ws, 0, st);
+  T *work = (T *)sc.get();
   if (!work) return cudaErrorMemoryAllocation;
   for (int64_t s0 = 0; s0 < g.nsys; s0 += ws) {
     const int64_t ns = (g.nsys - s0 < ws) ? (g.nsys - s0) : ws;

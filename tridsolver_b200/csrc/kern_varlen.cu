@@ -543,7 +543,8 @@ static VLArgs<T> varlen_args(const T *a, const T *b, const T *c, T *d, const int
 template <typename T>
 cudaError_t launch_varlen(const T *a, const T *b, const T *c, T *d, const int64_t *offsets,
                           int64_t nsys, int64_t total, unsigned *err, cudaStream_t st) {
-  unsigned char *w = (unsigned char *)scratch(vl_space(nsys, nullptr, nullptr), 0);
+  const Scratch sc(vl_space(nsys, nullptr, nullptr), 0, st);
+  unsigned char *w = (unsigned char *)sc.get();
   if (!w) return cudaErrorMemoryAllocation;
   VLSpace sp;
   vl_space(nsys, w, &sp);

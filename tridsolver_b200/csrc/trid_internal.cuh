@@ -112,11 +112,29 @@ __device__ __forceinline__ float rcp(float x) {
 // Per-thread library state (stream), defined in api_scalar.cu.
 cudaStream_t current_stream();
 
-// Device scratch owned by the library (grow-only, per device and nesting
-// level: a long-system solve at level L solves its block system at level
-// L+1, so levels never share a buffer).  Returns nullptr on allocation
-// failure.
-void *scratch(size_t bytes, int level = 0);
+// Device scratch held for the duration of one call on `stream` (the object
+// lives in the scope that enqueues every launch using it).  Outside stream capture it is a
+// grow-only buffer kept per (device, stream, nesting level): calls on one
+// stream run in order and share it, calls on other streams get their own, and
+// a long-system solve at level L solves its block system at level L+1, so
+// levels never share a buffer.  While the stream is being
+// captured into a CUDA graph it is a stream-ordered allocation freed when the
+// object goes out of scope, so the graph carries its own allocate and free
+// nodes and never refers to a buffer that a later call may replace.  get() is
+// nullptr for 0 bytes and on allocation failure.
+class Scratch {
+ public:
+  Scratch(size_t bytes, int level, cudaStream_t stream);
+  ~Scratch();
+  Scratch(const Scratch &) = delete;
+  Scratch &operator=(const Scratch &) = delete;
+  void *get() const { return ptr_; }
+
+ private:
+  void *ptr_ = nullptr;
+  cudaStream_t stream_ = nullptr;
+  bool stream_ordered_ = false;
+};
 
 // Per-device word of error bits set by kernels whose bounded waits gave up
 // (read and cleared by tridGetDeviceErrors).  nullptr if it cannot be made.
