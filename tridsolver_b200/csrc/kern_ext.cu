@@ -25,6 +25,8 @@
 //  ext_thomas_kernel  longer systems: one thread per system, Thomas with
 //                     c'/d' in library scratch laid out [row][system] (in T).
 // The longest chunk is 16 rows for 8-byte T and 8 for complex<double>.
+#include <type_traits>
+
 #include "partition.cuh"
 #include "tma.cuh"
 #include "trid_b200.h"
@@ -269,12 +271,14 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // rows of every array stream into shared memory by per-element cp.async
 // (consecutive threads take consecutive systems of a row: coalesced), each
 // thread copies its chunk rows into registers, the buffer is released and
-// the next tile's copies are issued before the current tile is solved (as
-// ext_strided_kernel), so the copies overlap the arithmetic.
+// a later tile's copies are issued into it before the current tile is
+// solved, so the copies overlap the arithmetic.  NBUF tile buffers: with
+// two, two tiles' copies are in flight while one is solved (FP32 storage
+// tiles are small, and one tile in flight per SM keeps too few bytes moving).
 // VEC: every tile is SB consecutive systems of one axis-0 row with 16-byte
 // aligned rows (dims[0] a multiple of SB, row strides multiples of 16 bytes),
 // so the copies move 16 bytes (16/sizeof(S) systems) each.
-template <typename S, typename T, int M, int SB, int INC, bool VEC>
+template <typename S, typename T, int M, int SB, int INC, bool VEC, int NBUF>
 __global__ void __launch_bounds__(SB * kWarp, 1) ext_stream_kernel(Geom g, const S *__restrict__ a,
                                                                    const S *__restrict__ b,
                                                                    const S *__restrict__ c,
@@ -283,50 +287,57 @@ __global__ void __launch_bounds__(SB * kWarp, 1) ext_stream_kernel(Geom g, const
                                                                    int64_t ntiles) {
   using E = Elem<S, T>;
   constexpr int NA = INC ? 5 : 4;
+  constexpr int NSET = NBUF + 1;  // offset sets: the tiles in flight and the one being solved
   extern __shared__ __align__(16) unsigned char ext_smem[];
-  // per array, the tile's system offsets (-1: past the last system); two
-  // sets, the next tile's written while the current one is in use
-  __shared__ int64_t soff[2][NA][SB];
+  // per array, a tile's system offsets (-1: past the last system)
+  __shared__ int64_t soff[NSET][NA][SB];
   const int n = g.n;
   const size_t tsz = (size_t)n * SB;  // [row][system] per array
-  S *tile = reinterpret_cast<S *>(ext_smem);
-  T *red = reinterpret_cast<T *>(tile + NA * tsz);  // [8][32][SB+1]
-  T *sol = red + 8 * kWarp * (SB + 1);               // [2][32][SB+1]
+  S *const tiles = reinterpret_cast<S *>(ext_smem);  // [NBUF][NA][tsz]
+  T *red = reinterpret_cast<T *>(tiles + NBUF * NA * tsz);  // [8][32][SB+1]
+  T *sol = red + 8 * kWarp * (SB + 1);                      // [2][32][SB+1]
   const S *src[5] = {a, b, c, d, u};
   const int tid = threadIdx.x;
   const int sl = tid % SB;
   const int t = tid / SB;
-  auto offsets = [&](int64_t blk, int buf) {
+  auto offsets = [&](int64_t blk, int set) {
     if (tid < SB) {
       const int64_t s = blk * SB + tid;
       int64_t off[5] = {-1, -1, -1, -1, -1};
       if (s < g.nsys) system_offsets(g, s, off);
 #pragma unroll
-      for (int q = 0; q < NA; ++q) soff[buf][q][tid] = s < g.nsys ? off[q] : -1;
+      for (int q = 0; q < NA; ++q) soff[set][q][tid] = s < g.nsys ? off[q] : -1;
     }
   };
-  auto issue = [&](int buf) {
-    if constexpr (VEC) {
-      constexpr int V = 16 / (int)sizeof(S);  // systems per copy
-      constexpr int PR = SB / V;              // copies per row
+  // copies of the tile whose offsets are in `set` into buffer `tb`; always
+  // closes a commit group (possibly empty) so that the group count per loop
+  // iteration stays fixed
+  auto issue = [&](int tb, int set, bool any) {
+    S *tile = tiles + (size_t)tb * NA * tsz;
+    if (any) {
+      if constexpr (VEC) {
+        constexpr int V = 16 / (int)sizeof(S);  // systems per copy
+        constexpr int PR = SB / V;              // copies per row
 #pragma unroll
-      for (int q = 0; q < NA; ++q) {
-        const int64_t base = soff[buf][q][0];
-        const int64_t str = g.stride[q];
-        for (int i = tid; i < n * PR; i += SB * kWarp) {
-          const int r = i / PR, v = i % PR;
-          cp_async_elem<16>(tile + q * tsz + (size_t)r * SB + v * V, src[q] + base + r * str + v * V);
+        for (int q = 0; q < NA; ++q) {
+          const int64_t base = soff[set][q][0];
+          const int64_t str = g.stride[q];
+          for (int i = tid; i < n * PR; i += SB * kWarp) {
+            const int r = i / PR, v = i % PR;
+            cp_async_elem<16>(tile + q * tsz + (size_t)r * SB + v * V,
+                              src[q] + base + r * str + v * V);
+          }
         }
-      }
-    } else {
+      } else {
 #pragma unroll
-      for (int q = 0; q < NA; ++q) {
-        const int64_t base = soff[buf][q][sl];
-        if (base < 0) continue;
-        const int64_t str = g.stride[q];
-        for (int r = t; r < n; r += kWarp)
-          cp_async_elem<(int)sizeof(S)>(tile + q * tsz + (size_t)r * SB + sl,
-                                        src[q] + base + r * str);
+        for (int q = 0; q < NA; ++q) {
+          const int64_t base = soff[set][q][sl];
+          if (base < 0) continue;
+          const int64_t str = g.stride[q];
+          for (int r = t; r < n; r += kWarp)
+            cp_async_elem<(int)sizeof(S)>(tile + q * tsz + (size_t)r * SB + sl,
+                                          src[q] + base + r * str);
+        }
       }
     }
     cp_async_commit();
@@ -337,19 +348,30 @@ __global__ void __launch_bounds__(SB * kWarp, 1) ext_stream_kernel(Geom g, const
 
   int64_t blk = blockIdx.x;
   if (blk >= ntiles) return;
-  offsets(blk, 0);
+  const int64_t G = gridDim.x;
+#pragma unroll
+  for (int k = 0; k < NBUF; ++k)
+    if (blk + k * G < ntiles) offsets(blk + k * G, k);
   __syncthreads();
-  issue(0);
-  int buf = 0;
+#pragma unroll
+  for (int k = 0; k < NBUF; ++k) issue(k, k, blk + k * G < ntiles);
+  int tb = 0, set = 0;
   const int r0 = t * M;
   const int64_t so = INC ? g.stride[kU] : g.stride[kD];
   S *const out = INC ? u : d;
-  for (; blk < ntiles; blk += gridDim.x) {
-    const int64_t nxt = blk + gridDim.x;
-    if (nxt < ntiles) offsets(nxt, buf ^ 1);
-    cp_async_wait_all();
+  for (; blk < ntiles; blk += G) {
+    // the tile NBUF steps ahead takes this tile's buffer once it is read
+    const int64_t ahead = blk + NBUF * G;
+    const int aset = (set + NBUF) % NSET;
+    if (ahead < ntiles) offsets(ahead, aset);
+    // this tile's group is the oldest of the NBUF outstanding ones
+    if constexpr (NBUF == 2)
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    else
+      cp_async_wait_all();
     __syncthreads();  // every thread's copies of this tile have landed
-    const int64_t obase = soff[buf][INC ? kU : kD][sl];
+    const S *tile = tiles + (size_t)tb * NA * tsz;
+    const int64_t obase = soff[set][INC ? kU : kD][sl];
     const bool valid = obase >= 0;
     T al[M], be[M], ga[M], de[M], uo[INC ? M : 1];
 #pragma unroll
@@ -363,8 +385,8 @@ __global__ void __launch_bounds__(SB * kWarp, 1) ext_stream_kernel(Geom g, const
       de[j] = in ? E::cv(tile[3 * tsz + o]) : T(0);
       if constexpr (INC) uo[j] = in ? E::cv(tile[4 * tsz + o]) : T(0);
     }
-    __syncthreads();  // the tile is free: the next one streams in meanwhile
-    if (nxt < ntiles) issue(buf ^ 1);
+    __syncthreads();  // the buffer is free: a later tile streams into it meanwhile
+    issue(tb, aset, ahead < ntiles);
 
     Row<T> F, L;
     chunk_reduce<T, M>(al, be, ga, de, F, L);
@@ -397,8 +419,10 @@ __global__ void __launch_bounds__(SB * kWarp, 1) ext_stream_kernel(Geom g, const
         if (r < n) E::st(out + obase + r * so, INC ? uo[INC ? j : 0] + de[j] : de[j]);
       }
     }
-    buf ^= 1;
+    tb = (tb + 1) % NBUF;
+    set = (set + 1) % NSET;
   }
+  cp_async_wait_all();  // empty groups only; nothing may be left in flight at exit
 }
 
 // Thomas in the reference's operation order (scalar/src/cpu/trid_cpu.cpp:
@@ -452,8 +476,8 @@ __global__ void __launch_bounds__(128) ext_thomas_kernel(Geom g, const S *__rest
 // Largest chunk (rows per lane) of the partitioned kernels: 16 for 8-byte
 // arithmetic, 8 for complex<double> (16 rows of 16 bytes per array exceed the
 // register file at one CTA per SM).
-// dynamic shared memory of the streamed kernel: tile plus interface rows
-constexpr size_t kExtStreamSmem = 200 * 1024;
+// dynamic shared memory of the streamed kernel: tiles plus interface rows
+constexpr size_t kExtStreamSmem = 220 * 1024;
 
 template <typename T>
 constexpr int ext_max_chunk() {
@@ -485,9 +509,12 @@ cudaError_t launch_ext(const Geom &g, int solvedim, const S *a, const S *b, cons
     // register-resident values per thread need 256-thread CTAs), else 16
     constexpr int SB = sizeof(T) >= 16 ? 8 : 16;
     if (M <= 8) {
-      // streamed tiles, one CTA per SM
+      // streamed tiles, one CTA per SM; two tile buffers when they fit
       constexpr int NA = INC ? 5 : 4;
-      const size_t smem = (size_t)NA * g.n * SB * sizeof(S) + (size_t)10 * kWarp * (SB + 1) * sizeof(T);
+      const size_t tile_bytes = (size_t)NA * g.n * SB * sizeof(S);
+      const size_t red_bytes = (size_t)10 * kWarp * (SB + 1) * sizeof(T);
+      const bool two = 2 * tile_bytes + red_bytes <= kExtStreamSmem;
+      const size_t smem = (two ? 2 : 1) * tile_bytes + red_bytes;
       int dev = 0, sms = 0;
       if (smem <= kExtStreamSmem && cudaGetDevice(&dev) == cudaSuccess &&
           cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess) {
@@ -509,18 +536,21 @@ cudaError_t launch_ext(const Geom &g, int solvedim, const S *a, const S *b, cons
           vec = ((uintptr_t)ptrs[q] & 15) == 0 && g.stride[q] % kV == 0;
           for (int k = 1; k < g.nod && vec; ++k) vec = g.ocum[q][k] % kV == 0;
         }
-        if (vec) {
+        auto pick = [&](auto vec_tag, auto nbuf_tag) {
+          constexpr bool V = decltype(vec_tag)::value;
+          constexpr int NB = decltype(nbuf_tag)::value;
           switch (M) {
-            case 2: return go(ext_stream_kernel<S, T, 2, SB, INC, true>);
-            case 4: return go(ext_stream_kernel<S, T, 4, SB, INC, true>);
-            default: return go(ext_stream_kernel<S, T, 8, SB, INC, true>);
+            case 2: return go(ext_stream_kernel<S, T, 2, SB, INC, V, NB>);
+            case 4: return go(ext_stream_kernel<S, T, 4, SB, INC, V, NB>);
+            default: return go(ext_stream_kernel<S, T, 8, SB, INC, V, NB>);
           }
-        }
-        switch (M) {
-          case 2: return go(ext_stream_kernel<S, T, 2, SB, INC, false>);
-          case 4: return go(ext_stream_kernel<S, T, 4, SB, INC, false>);
-          default: return go(ext_stream_kernel<S, T, 8, SB, INC, false>);
-        }
+        };
+        using V1 = std::true_type;
+        using V0 = std::false_type;
+        using B2 = std::integral_constant<int, 2>;
+        using B1 = std::integral_constant<int, 1>;
+        if (vec) return two ? pick(V1{}, B2{}) : pick(V1{}, B1{});
+        return two ? pick(V0{}, B2{}) : pick(V0{}, B1{});
       }
     }
     auto go = [&](auto kern, int sb) {
