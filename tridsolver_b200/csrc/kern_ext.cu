@@ -275,10 +275,12 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // solved, so the copies overlap the arithmetic.  NBUF tile buffers: with
 // two, two tiles' copies are in flight while one is solved (FP32 storage
 // tiles are small, and one tile in flight per SM keeps too few bytes moving).
-// VEC: every tile is SB consecutive systems of one axis-0 row with 16-byte
-// aligned rows (dims[0] a multiple of SB, row strides multiples of 16 bytes),
-// so the copies move 16 bytes (16/sizeof(S) systems) each.
-template <typename S, typename T, int M, int SB, int INC, bool VEC, int NBUF>
+// CP >= 1: every tile is SB consecutive systems of one axis-0 row with
+// 16-byte aligned rows (dims[0] a multiple of SB, row strides multiples of
+// 16 bytes), so the copies move 16 bytes (16/sizeof(S) systems) each;
+// CP == 2 adds n == 32*M (whole chunks): no row or system guards, and the
+// copy loops have fixed trip counts.
+template <typename S, typename T, int M, int SB, int INC, int CP, int NBUF>
 __global__ void __launch_bounds__(SB * kWarp, 1) ext_stream_kernel(Geom g, const S *__restrict__ a,
                                                                    const S *__restrict__ b,
                                                                    const S *__restrict__ c,
@@ -287,11 +289,13 @@ __global__ void __launch_bounds__(SB * kWarp, 1) ext_stream_kernel(Geom g, const
                                                                    int64_t ntiles) {
   using E = Elem<S, T>;
   constexpr int NA = INC ? 5 : 4;
+  constexpr bool VEC = CP >= 1;
+  constexpr bool FULL = CP == 2;
   constexpr int NSET = NBUF + 1;  // offset sets: the tiles in flight and the one being solved
   extern __shared__ __align__(16) unsigned char ext_smem[];
   // per array, a tile's system offsets (-1: past the last system)
   __shared__ int64_t soff[NSET][NA][SB];
-  const int n = g.n;
+  const int n = FULL ? kWarp * M : g.n;
   const size_t tsz = (size_t)n * SB;  // [row][system] per array
   S *const tiles = reinterpret_cast<S *>(ext_smem);  // [NBUF][NA][tsz]
   T *red = reinterpret_cast<T *>(tiles + NBUF * NA * tsz);  // [8][32][SB+1]
@@ -372,18 +376,28 @@ __global__ void __launch_bounds__(SB * kWarp, 1) ext_stream_kernel(Geom g, const
     __syncthreads();  // every thread's copies of this tile have landed
     const S *tile = tiles + (size_t)tb * NA * tsz;
     const int64_t obase = soff[set][INC ? kU : kD][sl];
-    const bool valid = obase >= 0;
+    const bool valid = FULL || obase >= 0;
     T al[M], be[M], ga[M], de[M], uo[INC ? M : 1];
 #pragma unroll
     for (int j = 0; j < M; ++j) {
       const int r = r0 + j;
-      const bool in = valid && r < n;
-      const size_t o = (size_t)(r < n ? r : n - 1) * SB + sl;
-      al[j] = (in && r != 0) ? E::cv(tile[o]) : T(0);
-      be[j] = in ? E::cv(tile[tsz + o]) : T(1);
-      ga[j] = (in && r != n - 1) ? E::cv(tile[2 * tsz + o]) : T(0);
-      de[j] = in ? E::cv(tile[3 * tsz + o]) : T(0);
-      if constexpr (INC) uo[j] = in ? E::cv(tile[4 * tsz + o]) : T(0);
+      if constexpr (FULL) {
+        const size_t o = (size_t)r * SB + sl;
+        const T va = E::cv(tile[o]), vc = E::cv(tile[2 * tsz + o]);
+        al[j] = (j == 0 && t == 0) ? T(0) : va;
+        be[j] = E::cv(tile[tsz + o]);
+        ga[j] = (j == M - 1 && t == kWarp - 1) ? T(0) : vc;
+        de[j] = E::cv(tile[3 * tsz + o]);
+        if constexpr (INC) uo[j] = E::cv(tile[4 * tsz + o]);
+      } else {
+        const bool in = valid && r < n;
+        const size_t o = (size_t)(r < n ? r : n - 1) * SB + sl;
+        al[j] = (in && r != 0) ? E::cv(tile[o]) : T(0);
+        be[j] = in ? E::cv(tile[tsz + o]) : T(1);
+        ga[j] = (in && r != n - 1) ? E::cv(tile[2 * tsz + o]) : T(0);
+        de[j] = in ? E::cv(tile[3 * tsz + o]) : T(0);
+        if constexpr (INC) uo[j] = in ? E::cv(tile[4 * tsz + o]) : T(0);
+      }
     }
     __syncthreads();  // the buffer is free: a later tile streams into it meanwhile
     issue(tb, aset, ahead < ntiles);
@@ -416,7 +430,7 @@ __global__ void __launch_bounds__(SB * kWarp, 1) ext_stream_kernel(Geom g, const
 #pragma unroll
       for (int j = 0; j < M; ++j) {
         const int r = r0 + j;
-        if (r < n) E::st(out + obase + r * so, INC ? uo[INC ? j : 0] + de[j] : de[j]);
+        if (FULL || r < n) E::st(out + obase + r * so, INC ? uo[INC ? j : 0] + de[j] : de[j]);
       }
     }
     tb = (tb + 1) % NBUF;
@@ -528,29 +542,32 @@ cudaError_t launch_ext(const Geom &g, int solvedim, const S *a, const S *b, cons
           return cudaGetLastError();
         };
         // 16-byte copies: whole tiles in one row, 16-byte aligned bases and
-        // row strides (elements narrower than 16 bytes only)
-        bool vec = sizeof(S) < 16 && g.odims[0] % SB == 0;
+        // row strides (always so for 16-byte elements, whose copies are one
+        // element either way; the mode also admits the guard-free variant)
+        bool vec = g.odims[0] % SB == 0;
         const void *ptrs[5] = {a, b, c, d, u};
         constexpr int64_t kV = 16 / (int64_t)sizeof(S);
         for (int q = 0; q < NA && vec; ++q) {
           vec = ((uintptr_t)ptrs[q] & 15) == 0 && g.stride[q] % kV == 0;
           for (int k = 1; k < g.nod && vec; ++k) vec = g.ocum[q][k] % kV == 0;
         }
-        auto pick = [&](auto vec_tag, auto nbuf_tag) {
-          constexpr bool V = decltype(vec_tag)::value;
+        auto pick = [&](auto cp_tag, auto nbuf_tag) {
+          constexpr int CP = decltype(cp_tag)::value;
           constexpr int NB = decltype(nbuf_tag)::value;
           switch (M) {
-            case 2: return go(ext_stream_kernel<S, T, 2, SB, INC, V, NB>);
-            case 4: return go(ext_stream_kernel<S, T, 4, SB, INC, V, NB>);
-            default: return go(ext_stream_kernel<S, T, 8, SB, INC, V, NB>);
+            case 2: return go(ext_stream_kernel<S, T, 2, SB, INC, CP, NB>);
+            case 4: return go(ext_stream_kernel<S, T, 4, SB, INC, CP, NB>);
+            default: return go(ext_stream_kernel<S, T, 8, SB, INC, CP, NB>);
           }
         };
-        using V1 = std::true_type;
-        using V0 = std::false_type;
+        using C2 = std::integral_constant<int, 2>;
+        using C1 = std::integral_constant<int, 1>;
+        using C0 = std::integral_constant<int, 0>;
         using B2 = std::integral_constant<int, 2>;
         using B1 = std::integral_constant<int, 1>;
-        if (vec) return two ? pick(V1{}, B2{}) : pick(V1{}, B1{});
-        return two ? pick(V0{}, B2{}) : pick(V0{}, B1{});
+        if (vec && g.n == kWarp * M) return two ? pick(C2{}, B2{}) : pick(C2{}, B1{});
+        if (vec) return two ? pick(C1{}, B2{}) : pick(C1{}, B1{});
+        return two ? pick(C0{}, B2{}) : pick(C0{}, B1{});
       }
     }
     auto go = [&](auto kern, int sb) {
