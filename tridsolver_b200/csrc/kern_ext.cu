@@ -25,6 +25,8 @@
 //  ext_thomas_kernel  longer systems: one thread per system, Thomas with
 //                     c'/d' in library scratch laid out [row][system] (in T).
 // The longest chunk is 16 rows for 8-byte T and 8 for complex<double>.
+#include <string.h>
+
 #include <type_traits>
 
 #include "partition.cuh"
@@ -141,8 +143,48 @@ __device__ __forceinline__ void ext_out(S *d, S *u, T x) {
     E::st(d, x);
 }
 
+// Element-wise asynchronous global -> shared copies of 4, 8 or 16 bytes
+// (cp.async; 16-byte copies bypass L1)
+template <int B>
+__device__ __forceinline__ void cp_async_elem(void *dst, const void *src) {
+  if constexpr (B == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src),
+                 "n"(B)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // ------------------------------------------------------------- kernels --
-template <typename S, typename T, int M, int INC>
+// M consecutive elements as 16-byte accesses (M * sizeof(S) a multiple of 16,
+// p 16-byte aligned)
+template <typename S, int M, bool NC>
+__device__ __forceinline__ void load16(const S *p, S (&v)[M]) {
+  constexpr int K = M * (int)sizeof(S) / 16;
+  static_assert(K * 16 == M * (int)sizeof(S), "whole 16-byte words");
+  const uint4 *q = reinterpret_cast<const uint4 *>(p);
+  uint4 w[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) w[k] = NC ? __ldg(q + k) : q[k];
+  memcpy(v, w, sizeof(w));
+}
+template <typename S, int M>
+__device__ __forceinline__ void store16(S *p, const S (&v)[M]) {
+  constexpr int K = M * (int)sizeof(S) / 16;
+  uint4 w[K];
+  memcpy(w, v, sizeof(w));
+  uint4 *q = reinterpret_cast<uint4 *>(p);
+#pragma unroll
+  for (int k = 0; k < K; ++k) q[k] = w[k];
+}
+
+// Axis 0: one warp per system, lane = chunk of M rows.  VEC: n == 32*M and
+// every array's rows 16-byte aligned, so a lane reads and writes its chunk
+// as 16-byte words instead of one element at a time.
+template <typename S, typename T, int M, int INC, bool VEC>
 __global__ void __launch_bounds__(128) ext_x_kernel(Geom g, const S *__restrict__ a,
                                                     const S *__restrict__ b,
                                                     const S *__restrict__ c, S *__restrict__ d,
@@ -153,22 +195,37 @@ __global__ void __launch_bounds__(128) ext_x_kernel(Geom g, const S *__restrict_
   if (sys >= g.nsys) return;  // uniform per warp
   int64_t off[5];
   system_offsets(g, sys, off);
-  const int n = g.n;
+  const int n = VEC ? kWarp * M : g.n;
   const int r0 = lane * M;
   T al[M], be[M], ga[M], de[M];
+  if constexpr (VEC) {
+    S va[M], vb[M], vc[M], vd[M];
+    load16<S, M, true>(a + off[kA] + r0, va);
+    load16<S, M, true>(b + off[kB] + r0, vb);
+    load16<S, M, true>(c + off[kC] + r0, vc);
+    load16<S, M, false>(d + off[kD] + r0, vd);
 #pragma unroll
-  for (int j = 0; j < M; ++j) {
-    const int r = r0 + j;
-    if (r < n) {
-      al[j] = (r == 0) ? T(0) : E::ld(a + off[kA] + r);
-      be[j] = E::ld(b + off[kB] + r);
-      ga[j] = (r == n - 1) ? T(0) : E::ld(c + off[kC] + r);
-      de[j] = E::ldw(d + off[kD] + r);
-    } else {
-      al[j] = T(0);
-      be[j] = T(1);
-      ga[j] = T(0);
-      de[j] = T(0);
+    for (int j = 0; j < M; ++j) {
+      al[j] = (j == 0 && lane == 0) ? T(0) : E::cv(va[j]);
+      be[j] = E::cv(vb[j]);
+      ga[j] = (j == M - 1 && lane == kWarp - 1) ? T(0) : E::cv(vc[j]);
+      de[j] = E::cv(vd[j]);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int r = r0 + j;
+      if (r < n) {
+        al[j] = (r == 0) ? T(0) : E::ld(a + off[kA] + r);
+        be[j] = E::ld(b + off[kB] + r);
+        ga[j] = (r == n - 1) ? T(0) : E::ld(c + off[kC] + r);
+        de[j] = E::ldw(d + off[kD] + r);
+      } else {
+        al[j] = T(0);
+        be[j] = T(1);
+        ga[j] = T(0);
+        de[j] = T(0);
+      }
     }
   }
   Row<T> F, L;
@@ -176,10 +233,82 @@ __global__ void __launch_bounds__(128) ext_x_kernel(Geom g, const S *__restrict_
   T xF, xL;
   warp_interface_solve(F, L, xF, xL, lane);
   chunk_backsub<T, M>(al, ga, de, xF, xL);
+  if constexpr (VEC) {
+    S vx[M];
+    if constexpr (INC) load16<S, M, false>(u + off[kU] + r0, vx);
+#pragma unroll
+    for (int j = 0; j < M; ++j) E::st(vx + j, INC ? E::cv(vx[j]) + de[j] : de[j]);
+    store16<S, M>((INC ? u + off[kU] : d + off[kD]) + r0, vx);
+  } else {
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int r = r0 + j;
+      if (r < n) ext_out<S, T, INC>(d + off[kD] + r, INC ? u + off[kU] + r : nullptr, de[j]);
+    }
+  }
+}
+
+// Axis 0, whole systems (n == 32*M): one warp per system; the system's rows
+// of every array arrive by coalesced cp.async copies (32 consecutive
+// elements per warp copy) in shared memory, row i of an array at slot
+// i + i/M (one pad slot per chunk, so lane l's chunk starts at l*(M+1) and
+// the lanes' reads of a row fall in distinct banks); each lane takes its
+// chunk from there, and the solution leaves the same way (written into the
+// right-hand-side slots, then stored by coalesced warp stores).  Used for
+// elements of 16 bytes, which leave no room for wider per-lane words.
+template <typename S, typename T, int M, int INC>
+__global__ void __launch_bounds__(128) ext_x_staged_kernel(Geom g, const S *__restrict__ a,
+                                                           const S *__restrict__ b,
+                                                           const S *__restrict__ c,
+                                                           S *__restrict__ d, S *__restrict__ u) {
+  using E = Elem<S, T>;
+  constexpr int NA = INC ? 5 : 4;
+  constexpr int SL = kWarp * (M + 1);  // slots per array
+  extern __shared__ __align__(16) unsigned char xs_smem[];
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int w = threadIdx.x / kWarp;
+  const int64_t sys = (int64_t)blockIdx.x * (blockDim.x / kWarp) + w;
+  if (sys >= g.nsys) return;  // uniform per warp
+  int64_t off[5];
+  system_offsets(g, sys, off);
+  S *sm = reinterpret_cast<S *>(xs_smem) + (size_t)w * NA * SL;
+  const S *src[5] = {a + off[kA], b + off[kB], c + off[kC], d + off[kD],
+                     INC ? u + off[kU] : nullptr};
+#pragma unroll
+  for (int q = 0; q < NA; ++q)
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+      const int i = k * kWarp + lane;
+      cp_async_elem<(int)sizeof(S)>(sm + q * SL + i + i / M, src[q] + i);
+    }
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncwarp();
+  T al[M], be[M], ga[M], de[M], uo[INC ? M : 1];
+  const int s0 = lane * (M + 1);
 #pragma unroll
   for (int j = 0; j < M; ++j) {
-    const int r = r0 + j;
-    if (r < n) ext_out<S, T, INC>(d + off[kD] + r, INC ? u + off[kU] + r : nullptr, de[j]);
+    const T va = E::cv(sm[s0 + j]), vc = E::cv(sm[2 * SL + s0 + j]);
+    al[j] = (j == 0 && lane == 0) ? T(0) : va;
+    be[j] = E::cv(sm[SL + s0 + j]);
+    ga[j] = (j == M - 1 && lane == kWarp - 1) ? T(0) : vc;
+    de[j] = E::cv(sm[3 * SL + s0 + j]);
+    if constexpr (INC) uo[j] = E::cv(sm[4 * SL + s0 + j]);
+  }
+  Row<T> F, L;
+  chunk_reduce<T, M>(al, be, ga, de, F, L);
+  T xF, xL;
+  warp_interface_solve(F, L, xF, xL, lane);
+  chunk_backsub<T, M>(al, ga, de, xF, xL);
+  // each lane overwrites only the slots it read itself
+#pragma unroll
+  for (int j = 0; j < M; ++j) E::st(sm + 3 * SL + s0 + j, INC ? uo[INC ? j : 0] + de[j] : de[j]);
+  __syncwarp();
+  S *dst = INC ? u + off[kU] : d + off[kD];
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    const int i = k * kWarp + lane;
+    dst[i] = sm[3 * SL + i + i / M];
   }
 }
 
@@ -251,21 +380,6 @@ __global__ void __launch_bounds__(SB * kWarp) ext_strided_kernel(Geom g, const S
       ext_out<S, T, INC>(d + off[kD] + r * sd, INC ? u + off[kU] + r * su : nullptr, de[j]);
   }
 }
-
-// Element-wise asynchronous global -> shared copies of 4, 8 or 16 bytes
-// (cp.async; 16-byte copies bypass L1)
-template <int B>
-__device__ __forceinline__ void cp_async_elem(void *dst, const void *src) {
-  if constexpr (B == 16)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src)
-                 : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src),
-                 "n"(B)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Strided axes, persistent (one CTA per SM): tiles of SB adjacent systems x n
 // rows of every array stream into shared memory by per-element cp.async
@@ -508,16 +622,57 @@ cudaError_t launch_ext(const Geom &g, int solvedim, const S *a, const S *b, cons
       const int64_t blocks = (g.nsys + 3) / 4;
       if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
       const dim3 grid((unsigned)blocks), block(128);
-      switch (M) {
-        case 2: ext_x_kernel<S, T, 2, INC><<<grid, block, 0, st>>>(g, a, b, c, d, u); break;
-        case 4: ext_x_kernel<S, T, 4, INC><<<grid, block, 0, st>>>(g, a, b, c, d, u); break;
-        case 8: ext_x_kernel<S, T, 8, INC><<<grid, block, 0, st>>>(g, a, b, c, d, u); break;
-        default:
-          if constexpr (ext_max_chunk<T>() >= 16)
-            ext_x_kernel<S, T, 16, INC><<<grid, block, 0, st>>>(g, a, b, c, d, u);
-          break;
+      // 16-byte words per lane: whole systems, rows of every array used
+      // 16-byte aligned in every system (bases and outer strides), elements
+      // of at most 8 bytes
+      bool vec = sizeof(S) <= 8 && g.n == kWarp * M && (M * sizeof(S)) % 16 == 0;
+      const void *ptrs[5] = {a, b, c, d, u};
+      for (int q = 0; q < (INC ? 5 : 4) && vec; ++q) {
+        vec = ((uintptr_t)ptrs[q] & 15) == 0;
+        for (int k = 0; k < g.nod && vec; ++k) vec = (g.ocum[q][k] * (int64_t)sizeof(S)) % 16 == 0;
       }
-      return cudaGetLastError();
+      auto go = [&](auto kern) {
+        kern<<<grid, block, 0, st>>>(g, a, b, c, d, u);
+        return cudaGetLastError();
+      };
+      // whole systems of 16-byte elements: staged through shared memory
+      // (for narrower elements the 16-byte words per lane measured faster:
+      // 256^3 axis 0, FP32 storage 4.81 against 4.41 TB/s, complex<float>
+      // 5.65 against 4.19)
+      if constexpr (sizeof(S) == 16) {
+        auto go_staged = [&](auto kern) {
+          const size_t smem = (size_t)4 * (INC ? 5 : 4) * kWarp * (M + 1) * sizeof(S);
+          cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem);
+          if (e != cudaSuccess) return e;
+          kern<<<grid, block, smem, st>>>(g, a, b, c, d, u);
+          return cudaGetLastError();
+        };
+        if (g.n == kWarp * M) {
+          switch (M) {
+            case 2: return go_staged(ext_x_staged_kernel<S, T, 2, INC>);
+            case 4: return go_staged(ext_x_staged_kernel<S, T, 4, INC>);
+            default: return go_staged(ext_x_staged_kernel<S, T, 8, INC>);
+          }
+        }
+      }
+      switch (M) {
+        case 2:
+          if constexpr (sizeof(S) == 8) if (vec) return go(ext_x_kernel<S, T, 2, INC, true>);
+          return go(ext_x_kernel<S, T, 2, INC, false>);
+        case 4:
+          if constexpr (sizeof(S) <= 8) if (vec) return go(ext_x_kernel<S, T, 4, INC, true>);
+          return go(ext_x_kernel<S, T, 4, INC, false>);
+        case 8:
+          if constexpr (sizeof(S) <= 8) if (vec) return go(ext_x_kernel<S, T, 8, INC, true>);
+          return go(ext_x_kernel<S, T, 8, INC, false>);
+        default:
+          if constexpr (ext_max_chunk<T>() >= 16) {
+            if constexpr (sizeof(S) <= 8) if (vec) return go(ext_x_kernel<S, T, 16, INC, true>);
+            return go(ext_x_kernel<S, T, 16, INC, false>);
+          }
+          return cudaErrorInvalidValue;
+      }
     }
     // SB systems per CTA: 8 for 16-byte T and for 16-row chunks (whose 64
     // register-resident values per thread need 256-thread CTAs), else 16
