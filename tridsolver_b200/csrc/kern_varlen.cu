@@ -14,7 +14,7 @@
 //     kern_xcta.cu): bucket W lists the systems that need W = ceil(n/512)
 //     warps at 16 rows per lane; one persistent launch per bucket, CTA = W
 //     warps solving one system at a time, every row read once;
-//   * 4097 .. 8192 rows: one CTA of 8 warps per system (varlen_long_kernel):
+//   * 4097 .. 8192 rows: one CTA of 4 warps per system (varlen_long_kernel):
 //     the system's rows are requested from L2 at once, every warp reduces its
 //     256-row blocks to block rows in shared memory, one warp solves the
 //     block system, every warp stages its blocks again (L2) and finishes
@@ -31,8 +31,8 @@
 // no table index can pass nsys whatever the offsets hold.
 //
 // Measured on B200 (FP64, 120 M unknowns, lengths log-uniform): 8 .. 256
-// rows 2.7 TB/s, 257 .. 1024 4.3, 1025 .. 4096 3.6, 4097 .. 8192 2.7, the
-// whole 8 .. 8192 range 3.0 TB/s algorithmic (200,000 systems: 3.12 TB/s).
+// rows 2.7 TB/s, 257 .. 1024 4.3, 1025 .. 4096 4.2, 4097 .. 8192 2.9, the
+// whole 8 .. 8192 range 3.2 TB/s algorithmic (200,000 systems: 3.39 TB/s).
 // Before the classes (every
 // system past 256 rows as 256-row block items reduced, published and
 // finished by a second queue across SMs, 72 B moved per unknown) the same
@@ -383,11 +383,12 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_short_kernel(VLArgs<T
 // batches, whose four systems per SM crowd L2 before their second pass; one
 // CTA of 16 warps and three or two 4-warp CTAs per SM were slower).  Thread 0 first asks L2 for the whole system (one bulk
 // prefetch per array, so its DRAM reads are all in flight at once); every
-// warp reduces its blocks (warp w: blocks w, w+8, ...) to their block rows
+// warp reduces its blocks (warp w: blocks w, w+4, ...) to their block rows
 // in shared memory; warp 0 solves the block system (lane t = block t); every
 // warp then stages its blocks again -- from L2, a few microseconds after
 // the first read -- and finishes them from their two boundary unknowns
-// (warp_block_finish).  DRAM moves each input once (40 bytes per FP64
+// (warp_block_finish).  In both passes a warp requests its next block as
+// soon as the current one is in registers.  DRAM moves each input once (40 bytes per FP64
 // unknown); the second pass costs L2 reads and the chunk reductions again.
 template <typename T>
 __device__ __forceinline__ void vl_prefetch_rows(const T *p, int64_t n) {
@@ -419,12 +420,16 @@ __global__ void __launch_bounds__(kVLLongWarps * 32, 4)
       vl_prefetch_rows(A.c + lo, len);
       vl_prefetch_rows(A.d + lo, len);
     }
-    // ---- the warp's blocks reduced to their block rows
+    // ---- the warp's blocks reduced to their block rows; once a block's
+    // rows are in registers the warp's next block is requested, so its
+    // copies are in flight while this one is reduced
+    if (w < nblk) vl_issue<T, 8>(A, reg, lo, (int64_t)w * kVLBlock, len, lane);
     for (int blk = w; blk < nblk; blk += kVLLongWarps) {
       const int64_t rb = (int64_t)blk * kVLBlock;
-      vl_issue<T, 8>(A, reg, lo, rb, len, lane);
       T al[8], be[8], ga[8], de[8], bF[3], bL[3];
       vl_read<T, 8>(reg, rb, len, lane, al, be, ga, de);
+      if (blk + kVLLongWarps < nblk)
+        vl_issue<T, 8>(A, reg, lo, rb + kVLLongWarps * kVLBlock, len, lane);
       Row<T> F, L, FB, LB;
       chunk_reduce<T, 8>(al, be, ga, de, F, L);
       warp_block_basis(F, L, lane, bF, bL);
@@ -435,6 +440,8 @@ __global__ void __launch_bounds__(kVLLongWarps * 32, 4)
         q[4] = LB.a; q[5] = LB.b; q[6] = LB.c; q[7] = LB.d;
       }
     }
+    // the warp's first block of the second pass, requested before the wait
+    if (w < nblk) vl_issue<T, 8>(A, reg, lo, (int64_t)w * kVLBlock, len, lane);
     __syncthreads();
     // ---- the block system (2 rows per block, lane t = block t)
     if (w == 0) {
@@ -457,9 +464,10 @@ __global__ void __launch_bounds__(kVLLongWarps * 32, 4)
     // boundary unknowns
     for (int blk = w; blk < nblk; blk += kVLLongWarps) {
       const int64_t rb = (int64_t)blk * kVLBlock;
-      vl_issue<T, 8>(A, reg, lo, rb, len, lane);
       T al[8], be[8], ga[8], de[8];
       vl_read<T, 8>(reg, rb, len, lane, al, be, ga, de);
+      if (blk + kVLLongWarps < nblk)
+        vl_issue<T, 8>(A, reg, lo, rb + kVLLongWarps * kVLBlock, len, lane);
       Row<T> F, L;
       chunk_reduce<T, 8>(al, be, ga, de, F, L);
       T xF, xL;
