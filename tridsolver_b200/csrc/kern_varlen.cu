@@ -15,10 +15,10 @@
 //     warps at 16 rows per lane; one persistent launch per bucket, CTA = W
 //     warps solving one system at a time, every row read once;
 //   * 4097 .. 8192 rows: one CTA of 4 warps per system (varlen_long_kernel):
-//     the system's rows are requested from L2 at once, every warp reduces its
-//     256-row blocks to block rows in shared memory, one warp solves the
-//     block system, every warp stages its blocks again (L2) and finishes
-//     them; DRAM reads every input once.
+//     the first half of the system's rows is requested into L2 at once,
+//     every warp reduces its 256-row blocks to block rows in shared memory,
+//     one warp solves the block system, every warp stages its blocks again
+//     (from L2 where they are still there) and finishes them.
 // Nothing waits on another CTA.  Rows reach each warp's shared-memory regions
 // by coalesced cp.async (row q of the 32*M at q + q/M, conflict-free for the
 // lane-per-chunk reads) and leave by coalesced stores.
@@ -381,15 +381,19 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_short_kernel(VLArgs<T
 // long systems' list (four 4-warp CTAs per SM measured ahead of two of 8
 // warps by 2-7% on 4097..8192-row mixes, 5% behind on uniform 8192-row
 // batches, whose four systems per SM crowd L2 before their second pass; one
-// CTA of 16 warps and three or two 4-warp CTAs per SM were slower).  Thread 0 first asks L2 for the whole system (one bulk
-// prefetch per array, so its DRAM reads are all in flight at once); every
+// CTA of 16 warps and three or two 4-warp CTAs per SM were slower).  Thread
+// 0 first asks L2 for the first half of the system (one bulk prefetch per
+// array: the whole system measured 8% slower on uniform 8192-row batches,
+// whose 592 CTAs' systems then exceed L2 before their second pass, and no
+// prefetch 1% slower on 4097..8192-row mixes); every
 // warp reduces its blocks (warp w: blocks w, w+4, ...) to their block rows
 // in shared memory; warp 0 solves the block system (lane t = block t); every
 // warp then stages its blocks again -- from L2, a few microseconds after
 // the first read -- and finishes them from their two boundary unknowns
 // (warp_block_finish).  In both passes a warp requests its next block as
-// soon as the current one is in registers.  DRAM moves each input once (40 bytes per FP64
-// unknown); the second pass costs L2 reads and the chunk reductions again.
+// soon as the current one is in registers.  The second pass costs the chunk
+// reductions again and reads of rows that L2 still holds, the rest from
+// DRAM: four CTAs per SM keep more rows in flight than L2 holds.
 template <typename T>
 __device__ __forceinline__ void vl_prefetch_rows(const T *p, int64_t n) {
   // the 16-byte aligned interior of the rows, one bulk prefetch
@@ -415,10 +419,11 @@ __global__ void __launch_bounds__(kVLLongWarps * 32, 4)
     const int64_t len = A.offsets[s + 1] - lo;
     const int nblk = (int)((len + kVLBlock - 1) / kVLBlock);
     if (threadIdx.x == 0) {
-      vl_prefetch_rows(A.a + lo, len);
-      vl_prefetch_rows(A.b + lo, len);
-      vl_prefetch_rows(A.c + lo, len);
-      vl_prefetch_rows(A.d + lo, len);
+      const int64_t half = len / 2;
+      vl_prefetch_rows(A.a + lo, half);
+      vl_prefetch_rows(A.b + lo, half);
+      vl_prefetch_rows(A.c + lo, half);
+      vl_prefetch_rows(A.d + lo, half);
     }
     // ---- the warp's blocks reduced to their block rows; once a block's
     // rows are in registers the warp's next block is requested, so its
