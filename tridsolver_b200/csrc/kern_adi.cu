@@ -62,19 +62,12 @@ __device__ __forceinline__ void adi_row(const AdiArgs<T> &g, int axis, int i, in
 // conflict-free both ways); the solution leaves the same way.  (Reading the
 // stencil lane by lane -- 4 consecutive points per lane, 7 loads each,
 // strided across the warp -- took 49-51 us per 128^3 step against 45.)
-// Programmatic dependent launch: the ADI kernels are launched so that they
-// may be scheduled while the previous kernel on the stream finishes; each
-// waits for that kernel to complete (its writes visible) before its first
-// global access, and lets the next one be scheduled once all of its own CTAs
-// have started.  Launched without the attribute, both are no-ops.
-__device__ __forceinline__ void adi_pdl_enter() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
+// The x, y and z kernels run under programmatic dependent launch
+// (launch_pdl / pdl_enter): each may be scheduled while its predecessor
+// finishes and waits for it before its first global access.
 template <typename T, int M, bool STENCIL, bool TRANS>
 __global__ void __launch_bounds__(128) adi_x_kernel(AdiArgs<T> g) {
-  adi_pdl_enter();
+  pdl_enter();
   __shared__ T sbuf[4][32 * (M + 1)];
   constexpr unsigned kFull = 0xffffffffu;
   const int lane = threadIdx.x & (kWarp - 1);
@@ -153,7 +146,7 @@ __global__ void __launch_bounds__(128) adi_x_kernel(AdiArgs<T> g) {
 // by side in lane groups of 16)
 template <typename T, int M, int SB, int NCH, int AXIS, bool TRANS, bool INC>
 __global__ void __launch_bounds__(SB * NCH) adi_s_kernel(AdiArgs<T> g) {
-  adi_pdl_enter();
+  pdl_enter();
   __shared__ T red[8][NCH][SB + 1];
   __shared__ T sol[2][NCH][SB + 1];
   const int tid = threadIdx.x;
@@ -319,31 +312,14 @@ __global__ void __launch_bounds__(256) adi_vjp_sum_kernel(const T *__restrict__ 
 }
 
 // ------------------------------------------------------------- launchers --
-// An ADI kernel with programmatic stream serialisation (see adi_pdl_enter).
-template <typename T>
-static cudaError_t adi_launch(void (*kern)(AdiArgs<T>), dim3 grid, dim3 block, cudaStream_t st,
-                              const AdiArgs<T> &g) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kern, g);
-}
-
 template <typename T, int M>
 static cudaError_t adi_x_m(const AdiArgs<T> &g, bool stencil, bool trans, bool inc,
                            cudaStream_t st) {
   const int64_t lines = (int64_t)g.ny * g.nz;
   const dim3 grid((unsigned)((lines + 3) / 4)), block(128);
-  if (stencil && !trans && !inc) return adi_launch<T>(adi_x_kernel<T, M, true, false>, grid, block, st, g);
-  if (!stencil && !trans && !inc) return adi_launch<T>(adi_x_kernel<T, M, false, false>, grid, block, st, g);
-  if (!stencil && trans && !inc) return adi_launch<T>(adi_x_kernel<T, M, false, true>, grid, block, st, g);
+  if (stencil && !trans && !inc) return launch_pdl(adi_x_kernel<T, M, true, false>, grid, block, 0, st, g);
+  if (!stencil && !trans && !inc) return launch_pdl(adi_x_kernel<T, M, false, false>, grid, block, 0, st, g);
+  if (!stencil && trans && !inc) return launch_pdl(adi_x_kernel<T, M, false, true>, grid, block, 0, st, g);
   return cudaErrorInvalidValue;
 }
 
@@ -357,11 +333,11 @@ static cudaError_t adi_s_m(const AdiArgs<T> &g, int axis, bool trans, bool inc, 
   const dim3 grid((unsigned)((int64_t)ntx * other)), block(SB * NCH);
 #define ADI_S(AX)                                                                            \
   if (!trans && !inc)                                                                        \
-    return adi_launch<T>(adi_s_kernel<T, M, SB, NCH, AX, false, false>, grid, block, st, g); \
+    return launch_pdl(adi_s_kernel<T, M, SB, NCH, AX, false, false>, grid, block, 0, st, g);  \
   if (!trans && inc)                                                                         \
-    return adi_launch<T>(adi_s_kernel<T, M, SB, NCH, AX, false, true>, grid, block, st, g);  \
+    return launch_pdl(adi_s_kernel<T, M, SB, NCH, AX, false, true>, grid, block, 0, st, g);   \
   if (trans && !inc)                                                                         \
-    return adi_launch<T>(adi_s_kernel<T, M, SB, NCH, AX, true, false>, grid, block, st, g);  \
+    return launch_pdl(adi_s_kernel<T, M, SB, NCH, AX, true, false>, grid, block, 0, st, g);   \
   return cudaErrorInvalidValue;
   if (axis == 1) {
     ADI_S(1)

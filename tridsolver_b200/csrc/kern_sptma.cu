@@ -52,6 +52,7 @@ __global__ void __launch_bounds__(SB * kWarp) strided_part_tma_kernel(
     const __grid_constant__ CUtensorMap mc, const __grid_constant__ CUtensorMap md,
     const __grid_constant__ CUtensorMap mu, Geom g, int solvedim, int box_rows, int nbox,
     int red_off, int prefetch_dist, unsigned *err) {
+  pdl_enter();
   constexpr int NA = INC ? 5 : 4;
   extern __shared__ unsigned char smem_raw[];
   __shared__ uint64_t bar;
@@ -221,6 +222,7 @@ __global__ void __launch_bounds__(SB * NCH, 1) strided_stream_kernel(
     const __grid_constant__ CUtensorMap mu, Geom g, int solvedim, int box_rows, int nbox,
     uint32_t ntiles, uint32_t ntx_mul, uint32_t ntx_shift, T *__restrict__ d,
     T *__restrict__ u, unsigned *err) {
+  pdl_enter();
   // NCH chunks of M rows per system (32, or 16 for short systems: a warp
   // then solves the interface systems of two tile systems side by side);
   // FULL: n == NCH*M and dims[0] a multiple of SB (no row or system guards)
@@ -381,10 +383,9 @@ static cudaError_t launch_stream(const CUtensorMap *maps, const Geom &g, int sol
   const int64_t grid = std::min<int64_t>(blocks, (int64_t)per_sm * sms);
   uint32_t ntx_mul = 0, ntx_shift = 0;
   fastdiv_setup((uint32_t)((g.odims[0] + SB - 1) / SB), ntx_mul, ntx_shift);
-  kern<<<dim3((unsigned)grid), dim3(SB * NCH), smem, st>>>(
-      maps[0], maps[1], maps[2], maps[3], maps[4], g, solvedim, box_rows, nbox, (uint32_t)blocks,
-      ntx_mul, ntx_shift, d, u, err);
-  return cudaGetLastError();
+  return launch_pdl(kern, dim3((unsigned)grid), dim3(SB * NCH), smem, st, maps[0], maps[1],
+                    maps[2], maps[3], maps[4], g, solvedim, box_rows, nbox, (uint32_t)blocks,
+                    ntx_mul, ntx_shift, d, u, err);
 }
 
 template <typename T, int M, int SB, int INC>
@@ -410,10 +411,8 @@ static cudaError_t launch_sptma(const CUtensorMap *maps, const Geom &g, int solv
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SB * kWarp, smem) != cudaSuccess)
     per_sm = 0;
   const int dist = prefetch_tiles ? per_sm * sms : 0;
-  kern<<<dim3((unsigned)blocks), dim3(SB * kWarp), smem, st>>>(
-      maps[0], maps[1], maps[2], maps[3], maps[4], g, solvedim, box_rows, nbox, red_off, dist,
-      err);
-  return cudaGetLastError();
+  return launch_pdl(kern, dim3((unsigned)blocks), dim3(SB * kWarp), smem, st, maps[0], maps[1],
+                    maps[2], maps[3], maps[4], g, solvedim, box_rows, nbox, red_off, dist, err);
 }
 
 template <typename T, int M, int INC>

@@ -83,6 +83,7 @@ __global__ void __launch_bounds__(kXWarps * kWarp) xsolve_tma_kernel(
     const __grid_constant__ CUtensorMap mc, const __grid_constant__ CUtensorMap md,
     const __grid_constant__ CUtensorMap mu, Geom g, int rows, T *__restrict__ d,
     T *__restrict__ u, unsigned *err) {
+  pdl_enter();
   using Tile = XTile<T, M>;
   constexpr int NA = INC ? 5 : 4;
   extern __shared__ unsigned char smem_raw[];
@@ -190,9 +191,8 @@ static cudaError_t launch_xtma_m(const CUtensorMap *maps, const Geom &g, int row
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<dim3((unsigned)blocks), dim3(kXWarps * kWarp), smem, st>>>(
-        maps[0], maps[1], maps[2], maps[3], maps[4], g, rows, d, u, err);
-    return cudaGetLastError();
+    return launch_pdl(kern, dim3((unsigned)blocks), dim3(kXWarps * kWarp), smem, st, maps[0],
+                      maps[1], maps[2], maps[3], maps[4], g, rows, d, u, err);
   };
   if (tstore) return go(xsolve_tma_kernel<T, M, INC, true>);
   return go(xsolve_tma_kernel<T, M, INC, false>);

@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 #include "../../include/trid_b200.h"
 
 namespace tridb200 {
@@ -220,5 +222,33 @@ cudaError_t launch_split_patch(const Geom &g, const T *a, const T *c, T *d, cons
                                int nranks, int rank, T *saved, cudaStream_t st);
 template <typename T>
 cudaError_t launch_split_restore(const Geom &g, T *d, const T *saved, cudaStream_t st);
+
+// Programmatic dependent launch.  A kernel launched by launch_pdl may be
+// scheduled while the previous kernel on the stream finishes; it calls
+// pdl_enter() before its first global access, which waits for that kernel
+// to complete (its writes visible) and lets the next kernel be scheduled
+// once every CTA of this grid has started, so a dependent grid only takes
+// the slots this one has left.  Launched without the attribute, pdl_enter()
+// does nothing.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... P, typename... A>
+inline cudaError_t launch_pdl(void (*kern)(P...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t st, A &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
 
 }  // namespace tridb200
