@@ -31,8 +31,8 @@
 // no table index can pass nsys whatever the offsets hold.
 //
 // Measured on B200 (FP64, 120 M unknowns, lengths log-uniform): 8 .. 256
-// rows 2.7 TB/s, 257 .. 1024 4.3, 1025 .. 4096 4.2, 4097 .. 8192 2.9, the
-// whole 8 .. 8192 range 3.2 TB/s algorithmic (200,000 systems: 3.39 TB/s).
+// rows 2.7 TB/s, 257 .. 1024 4.35, 1025 .. 4096 4.26, 4097 .. 8192 3.1, the
+// whole 8 .. 8192 range 3.39 TB/s algorithmic (200,000 systems: 3.58 TB/s).
 // Before the classes (every
 // system past 256 rows as 256-row block items reduced, published and
 // finished by a second queue across SMs, 72 B moved per unknown) the same
@@ -52,6 +52,8 @@ constexpr int kVLWarps = 8;              // warps per CTA of the short queue
 constexpr int kVLLongWarps = 4;          // warps per CTA of the long systems (four CTAs per SM)
 constexpr int kVLRegion = 32 * (8 + 1);  // elements per staged array and warp
 constexpr int kVLLists = kVarlenCtaBuckets + 1;  // the one-CTA buckets, then the long list
+static_assert(kVLLists <= kVarlenClaims && 64 + 4 * (kVarlenClaims + kVLLists) <= 256,
+              "list and claim counters fit the 256-byte control block");
 constexpr unsigned kErrBadOffsets = 4u;
 constexpr unsigned kErrTooLong = 8u;
 
@@ -135,7 +137,10 @@ __global__ void __launch_bounds__(1024) varlen_prep_scan(int64_t *__restrict__ b
     }
     ctl[0] = run;
     ctl[1] = 0;
-    for (int k = 0; k < kVLLists; ++k) list_count[k] = 0u;
+    for (int k = 0; k < kVLLists; ++k) {
+      list_count[k] = 0u;
+      list_count[kVarlenClaims + k] = 0u;  // the lists' claim counters
+    }
   }
   __syncthreads();
   int64_t run = part[tid];
@@ -174,7 +179,7 @@ __global__ void __launch_bounds__(kPrepThreads) varlen_prep_fill(
 // The work space of one solve, carved from one buffer.
 struct VLSpace {
   int64_t *ctl;          // [0] short systems, [1] claim counter
-  unsigned *list_count;  // kVLLists counters
+  unsigned *list_count;  // kVLLists counters; kVarlenClaims on, their claim counters
   int64_t *bsum;         // ceil(nsys/256) per-CTA prefixes
   int *item_sys;         // the short queue, nsys entries
   int *lists;            // kVLLists lists of nsys entries
@@ -188,7 +193,7 @@ static size_t vl_space(int64_t nsys, unsigned char *base, VLSpace *sp) {
   const size_t nb = (size_t)((nsys + kPrepThreads - 1) / kPrepThreads);
   size_t at = 0;
   const size_t o_ctl = at;
-  at += 256;  // ctl (2 x int64), then the list counters at +64
+  at += 256;  // ctl (2 x int64), then the list counters at +64, their claim counters at +128
   const size_t o_bsum = at;
   at += vl_al(sizeof(int64_t) * nb);
   const size_t o_items = at;
@@ -406,14 +411,19 @@ __device__ __forceinline__ void vl_prefetch_rows(const T *p, int64_t n) {
 
 template <typename T>
 __global__ void __launch_bounds__(kVLLongWarps * 32, 4)
-    varlen_long_kernel(VLArgs<T> A, const int *__restrict__ list, const unsigned *__restrict__ count) {
+    varlen_long_kernel(VLArgs<T> A, const int *__restrict__ list, const unsigned *__restrict__ count,
+                       unsigned *__restrict__ claim) {
   extern __shared__ __align__(16) unsigned char vll_dyn[];
   __shared__ T brow[kVLMaxBlocks * 8];  // block rows; then the block unknowns at [8t], [8t+1]
+  __shared__ unsigned s_next;
   const int lane = threadIdx.x & (kWarp - 1);
   const int w = threadIdx.x / kWarp;
   T *reg = reinterpret_cast<T *>(vll_dyn) + (size_t)w * 5 * kVLRegion;
   const int64_t cnt = (int64_t)*count;
-  for (int64_t i = blockIdx.x; i < cnt; i += gridDim.x) {
+  // systems claimed one at a time (lengths differ by up to 2x)
+  if (threadIdx.x == 0) s_next = atomicAdd(claim, 1u);
+  __syncthreads();
+  for (int64_t i = s_next; i < cnt;) {
     const int s = list[i];
     const int64_t lo = A.offsets[s];
     const int64_t len = A.offsets[s + 1] - lo;
@@ -480,7 +490,10 @@ __global__ void __launch_bounds__(kVLLongWarps * 32, 4)
       chunk_backsub<T, 8>(al, ga, de, xF, xL);
       vl_store<T, 8>(A, reg, lo, rb, len, lane, de);
     }
-    __syncthreads();  // brow is rewritten by the next system
+    if (threadIdx.x == 0) s_next = atomicAdd(claim, 1u);
+    __syncthreads();  // brow is rewritten by the next system; s_next is seen
+    i = s_next;
+    __syncthreads();  // every thread has read s_next
   }
 }
 
@@ -530,7 +543,8 @@ static cudaError_t launch_varlen_work(const VLArgs<T> &A, const VLSpace &sp, int
   if (e != cudaSuccess) return e;
 
   varlen_long_kernel<T><<<(unsigned)grid, kVLLongWarps * 32, lsmem, st>>>(
-      A, sp.lists + (size_t)(kClsLong - 1) * nsys, sp.list_count + (kClsLong - 1));
+      A, sp.lists + (size_t)(kClsLong - 1) * nsys, sp.list_count + (kClsLong - 1),
+      sp.list_count + kVarlenClaims + (kClsLong - 1));
   e = persistent_grid(varlen_short_kernel<T>, kVLWarps * 32, smem, grid, attr_short);
   if (e != cudaSuccess) return e;
   varlen_short_kernel<T><<<(unsigned)grid, kVLWarps * 32, smem, st>>>(A);

@@ -463,15 +463,25 @@ __device__ __forceinline__ void prefetch_rows_l2(const T *p, int n) {
 template <typename T, int M, int MAXW, int MINB>
 __global__ void __launch_bounds__(MAXW * 32, MINB)
     xcta_varlen_kernel(XArgs<T> A, const int64_t *__restrict__ offsets,
-                       const int *__restrict__ list, const unsigned *__restrict__ count) {
+                       const int *__restrict__ list, const unsigned *__restrict__ count,
+                       unsigned *__restrict__ claim) {
+  // systems are claimed one at a time (a bucket's lengths differ by up to 2x,
+  // so a fixed split leaves CTAs idle at the end); the next one is claimed
+  // when the current one starts, so that its rows can be warmed in L2
+  __shared__ unsigned s_next;
   const int64_t cnt = (int64_t)*count;
-  for (int64_t i = blockIdx.x; i < cnt; i += gridDim.x) {
+  if (threadIdx.x == 0) s_next = atomicAdd(claim, 1u);
+  __syncthreads();
+  int64_t i = s_next;
+  while (i < cnt) {
+    __syncthreads();  // every thread has read s_next
+    if (threadIdx.x == 0) s_next = atomicAdd(claim, 1u);
     const int s = list[i];
     const int64_t lo = offsets[s];
     const int n = (int)(offsets[s + 1] - lo);
     const int64_t off[5] = {lo, lo, lo, lo, lo};
-    const int64_t nxt = i + gridDim.x;
     xcta_system<T, M, kXFwd, false>(A, off, n, [&] {
+      const int64_t nxt = s_next;  // thread 0's own claim
       if (threadIdx.x == 0 && nxt < cnt) {
         const int s2 = list[nxt];
         const int64_t lo2 = offsets[s2];
@@ -482,14 +492,15 @@ __global__ void __launch_bounds__(MAXW * 32, MINB)
         prefetch_rows_l2(A.d + lo2, n2);
       }
     });
-    __syncthreads();  // the staged regions are refilled for the next system
+    __syncthreads();  // the staged regions are refilled for the next system; s_next is seen
+    i = s_next;
   }
 }
 
 template <typename T, int M, int MAXW, int MINB>
 static cudaError_t launch_xcta_varlen_w(const XArgs<T> &A, const int64_t *offsets, const int *list,
-                                        const unsigned *count, int W, int dev, int sms,
-                                        cudaStream_t st) {
+                                        const unsigned *count, unsigned *claim, int W, int dev,
+                                        int sms, cudaStream_t st) {
   auto kern = xcta_varlen_kernel<T, M, MAXW, MINB>;
   const size_t smem = (size_t)4 * W * Stage<T, M>::R * sizeof(T);
   static bool attr_set[64] = {};
@@ -509,13 +520,13 @@ static cudaError_t launch_xcta_varlen_w(const XArgs<T> &A, const int64_t *offset
     }
     per_sm[dev][W] = nb;
   }
-  kern<<<(unsigned)(sms * per_sm[dev][W]), W * kWarp, smem, st>>>(A, offsets, list, count);
+  kern<<<(unsigned)(sms * per_sm[dev][W]), W * kWarp, smem, st>>>(A, offsets, list, count, claim);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_xcta_varlen(const T *a, const T *b, const T *c, T *d, const int64_t *offsets,
-                               const int *lists, int64_t list_stride, const unsigned *counts,
+                               const int *lists, int64_t list_stride, unsigned *counts,
                                cudaStream_t st) {
   int dev = 0, sms = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -532,14 +543,15 @@ cudaError_t launch_xcta_varlen(const T *a, const T *b, const T *c, T *d, const i
   for (int W = kVarlenCtaBuckets; W >= 1; --W) {
     const int *list = lists + (size_t)(W - 1) * (size_t)list_stride;
     const unsigned *cnt = counts + W - 1;
+    unsigned *clm = counts + kVarlenClaims + W - 1;
     if (W <= 2)
-      e = launch_xcta_varlen_w<T, 16, 2, 6>(A, offsets, list, cnt, W, dev, sms, st);
+      e = launch_xcta_varlen_w<T, 16, 2, 6>(A, offsets, list, cnt, clm, W, dev, sms, st);
     else if (W <= 4)
-      e = launch_xcta_varlen_w<T, 16, 4, 3>(A, offsets, list, cnt, W, dev, sms, st);
+      e = launch_xcta_varlen_w<T, 16, 4, 3>(A, offsets, list, cnt, clm, W, dev, sms, st);
     else if (W <= 6)
-      e = launch_xcta_varlen_w<T, 16, 6, 2>(A, offsets, list, cnt, W, dev, sms, st);
+      e = launch_xcta_varlen_w<T, 16, 6, 2>(A, offsets, list, cnt, clm, W, dev, sms, st);
     else
-      e = launch_xcta_varlen_w<T, 16, 8, 1>(A, offsets, list, cnt, W, dev, sms, st);
+      e = launch_xcta_varlen_w<T, 16, 8, 1>(A, offsets, list, cnt, clm, W, dev, sms, st);
     if (e != cudaSuccess) return e;
   }
 
@@ -548,10 +560,10 @@ cudaError_t launch_xcta_varlen(const T *a, const T *b, const T *c, T *d, const i
 
 template cudaError_t launch_xcta_varlen<float>(const float *, const float *, const float *,
                                                float *, const int64_t *, const int *, int64_t,
-                                               const unsigned *, cudaStream_t);
+                                               unsigned *, cudaStream_t);
 template cudaError_t launch_xcta_varlen<double>(const double *, const double *, const double *,
                                                 double *, const int64_t *, const int *, int64_t,
-                                                const unsigned *, cudaStream_t);
+                                                unsigned *, cudaStream_t);
 
 #define TRID_XCTA_INSTANTIATE(T)                                                               \
   template cudaError_t launch_xcta<T, kXFwd>(const Geom &, const XArgs<T> &, int, cudaStream_t); \

@@ -199,12 +199,15 @@ template <typename T, int MODE>
 cudaError_t launch_xcta(const Geom &g, const XArgs<T> &A, int chunk, cudaStream_t st);
 // the variable-length batch's systems of kVarlenShort+1 .. 512*kVarlenCtaBuckets
 // rows, one CTA of W = ceil(n/512) warps each: bucket W-1 lists its systems
-// (lists + (W-1)*list_stride, counts[W-1] of them); solved in place in d
+// (lists + (W-1)*list_stride, counts[W-1] of them); solved in place in d.
+// counts[kVarlenClaims + k] is list k's claim counter (zero before the
+// launch): CTAs take the list's systems one at a time from it.
 constexpr int kVarlenShort = 256;
 constexpr int kVarlenCtaBuckets = 8;
+constexpr int kVarlenClaims = 16;
 template <typename T>
 cudaError_t launch_xcta_varlen(const T *a, const T *b, const T *c, T *d, const int64_t *offsets,
-                               const int *lists, int64_t list_stride, const unsigned *counts,
+                               const int *lists, int64_t list_stride, unsigned *counts,
                                cudaStream_t st);
 template <typename T, int INC>
 cudaError_t launch_generic(const Geom &g, const T *a, const T *b, const T *c, T *d, T *u,
