@@ -109,6 +109,7 @@ __device__ __forceinline__ int64_t vl_cta_scan(int64_t v, int64_t *warp_tot) {
 __global__ void __launch_bounds__(kPrepThreads) varlen_prep_count(const int64_t *__restrict__ offsets,
                                                                   int64_t nsys, int64_t total,
                                                                   int64_t *__restrict__ bsum) {
+  pdl_enter();
   __shared__ int64_t wt[kPrepThreads / 32];
   const int64_t s = (int64_t)blockIdx.x * kPrepThreads + threadIdx.x;
   const int64_t v = (s < nsys && vl_class(offsets, total, s) == kClsShort) ? 1 : 0;
@@ -120,6 +121,7 @@ __global__ void __launch_bounds__(kPrepThreads) varlen_prep_count(const int64_t 
 __global__ void __launch_bounds__(1024) varlen_prep_scan(int64_t *__restrict__ bsum, int64_t nblocks,
                                                          int64_t *__restrict__ ctl,
                                                          unsigned *__restrict__ list_count) {
+  pdl_enter();
   __shared__ int64_t part[1024];
   const int tid = threadIdx.x;
   const int64_t per = (nblocks + 1023) / 1024;
@@ -157,6 +159,7 @@ __global__ void __launch_bounds__(kPrepThreads) varlen_prep_fill(
     const int64_t *__restrict__ offsets, int64_t nsys, int64_t total,
     const int64_t *__restrict__ bsum, int *__restrict__ item_sys, int *__restrict__ lists,
     unsigned *__restrict__ list_count, unsigned *__restrict__ err) {
+  pdl_enter();
   __shared__ int64_t wt[kPrepThreads / 32];
   const int64_t s = (int64_t)blockIdx.x * kPrepThreads + threadIdx.x;
   const int cls = s < nsys ? vl_class(offsets, total, s) : kClsEmpty;
@@ -214,12 +217,15 @@ static cudaError_t launch_varlen_prep(const int64_t *offsets, int64_t nsys, int6
                                       const VLSpace &sp, unsigned *err, cudaStream_t st) {
   const int64_t nb = (nsys + kPrepThreads - 1) / kPrepThreads;
   if (nb > 0x7fffffff) return cudaErrorInvalidValue;
-  varlen_prep_count<<<(unsigned)nb, kPrepThreads, 0, st>>>(offsets, nsys, total, sp.bsum);
-  varlen_prep_scan<<<1, 1024, 0, st>>>(sp.bsum, nb, sp.ctl, sp.list_count);
-  varlen_prep_fill<<<(unsigned)nb, kPrepThreads, 0, st>>>(offsets, nsys, total, sp.bsum,
-                                                          sp.item_sys, sp.lists, sp.list_count,
-                                                          err);
-  return cudaGetLastError();
+  cudaError_t e = launch_pdl(varlen_prep_count, dim3((unsigned)nb), dim3(kPrepThreads), 0, st,
+                             offsets, nsys, total, sp.bsum);
+  if (e != cudaSuccess) return e;
+  e = launch_pdl(varlen_prep_scan, dim3(1), dim3(1024), 0, st, sp.bsum, nb, sp.ctl,
+                 sp.list_count);
+  if (e != cudaSuccess) return e;
+  return launch_pdl(varlen_prep_fill, dim3((unsigned)nb), dim3(kPrepThreads), 0, st, offsets,
+                    nsys, total, (const int64_t *)sp.bsum, sp.item_sys, sp.lists, sp.list_count,
+                    err);
 }
 
 template <typename T>
@@ -542,6 +548,8 @@ static cudaError_t launch_varlen_work(const VLArgs<T> &A, const VLSpace &sp, int
   e = persistent_grid(varlen_long_kernel<T>, kVLLongWarps * 32, lsmem, grid, attr_long);
   if (e != cudaSuccess) return e;
 
+  // the long systems and the short queue keep the plain launch (under
+  // programmatic launch the long class measured 9% slower)
   varlen_long_kernel<T><<<(unsigned)grid, kVLLongWarps * 32, lsmem, st>>>(
       A, sp.lists + (size_t)(kClsLong - 1) * nsys, sp.list_count + (kClsLong - 1),
       sp.list_count + kVarlenClaims + (kClsLong - 1));

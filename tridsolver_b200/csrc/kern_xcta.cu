@@ -465,6 +465,7 @@ __global__ void __launch_bounds__(MAXW * 32, MINB)
     xcta_varlen_kernel(XArgs<T> A, const int64_t *__restrict__ offsets,
                        const int *__restrict__ list, const unsigned *__restrict__ count,
                        unsigned *__restrict__ claim) {
+  pdl_enter();
   // systems are claimed one at a time (a bucket's lengths differ by up to 2x,
   // so a fixed split leaves CTAs idle at the end); the next one is claimed
   // when the current one starts, so that its rows can be warmed in L2
@@ -520,8 +521,8 @@ static cudaError_t launch_xcta_varlen_w(const XArgs<T> &A, const int64_t *offset
     }
     per_sm[dev][W] = nb;
   }
-  kern<<<(unsigned)(sms * per_sm[dev][W]), W * kWarp, smem, st>>>(A, offsets, list, count, claim);
-  return cudaGetLastError();
+  return launch_pdl(kern, dim3((unsigned)(sms * per_sm[dev][W])), dim3(W * kWarp), (size_t)smem,
+                    st, A, offsets, list, count, claim);
 }
 
 template <typename T>
