@@ -165,13 +165,20 @@ __global__ void __launch_bounds__(kPrepThreads) varlen_prep_fill(
   const int cls = s < nsys ? vl_class(offsets, total, s) : kClsEmpty;
   const int64_t v = cls == kClsShort ? 1 : 0;
   const int64_t r = bsum[blockIdx.x] + vl_cta_scan(v, wt) - v;
+  // list appends aggregated per warp: the lanes bound for one list take
+  // consecutive slots from a single atomic of their leader (one atomic per
+  // list and warp instead of one per system)
+  const int li = (s < nsys && cls >= 1 && cls <= kClsLong) ? cls - 1 : -1;
+  const unsigned grp = __match_any_sync(0xffffffffu, li);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(grp) - 1;
+  unsigned base = 0;
+  if (li >= 0 && lane == leader) base = atomicAdd(&list_count[li], (unsigned)__popc(grp));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (li >= 0) lists[(int64_t)li * nsys + base + __popc(grp & ((1u << lane) - 1u))] = (int)s;
   if (s >= nsys) return;
   if (cls == kClsShort) {
     item_sys[r] = (int)s;
-  } else if (cls >= 1 && cls <= kClsLong) {
-    const int li = cls - 1;
-    const unsigned pos = atomicAdd(&list_count[li], 1u);
-    lists[(int64_t)li * nsys + pos] = (int)s;
   } else if (cls == kClsBad) {
     atomicOr(err, kErrBadOffsets);
   } else if (cls == kClsTooLong) {
