@@ -122,30 +122,24 @@ __global__ void __launch_bounds__(1024) varlen_prep_scan(int64_t *__restrict__ b
                                                          int64_t *__restrict__ ctl,
                                                          unsigned *__restrict__ list_count) {
   pdl_enter();
-  __shared__ int64_t part[1024];
+  __shared__ int64_t wt[32];
   const int tid = threadIdx.x;
   const int64_t per = (nblocks + 1023) / 1024;
   const int64_t b0 = tid * per, b1 = (b0 + per < nblocks) ? b0 + per : nblocks;
   int64_t acc = 0;
   for (int64_t b = b0; b < b1; ++b) acc += bsum[b];
-  part[tid] = acc;
-  __syncthreads();
-  if (tid == 0) {
-    int64_t run = 0;
-    for (int k = 0; k < 1024; ++k) {
-      const int64_t v = part[k];
-      part[k] = run;
-      run += v;
-    }
-    ctl[0] = run;
+  // exclusive prefix of the threads' sums (shuffles within warps, then the
+  // warp totals)
+  const int64_t incl = vl_cta_scan(acc, wt);
+  if (tid == 1023) {
+    ctl[0] = incl;
     ctl[1] = 0;
     for (int k = 0; k < kVLLists; ++k) {
       list_count[k] = 0u;
       list_count[kVarlenClaims + k] = 0u;  // the lists' claim counters
     }
   }
-  __syncthreads();
-  int64_t run = part[tid];
+  int64_t run = incl - acc;
   for (int64_t b = b0; b < b1; ++b) {
     const int64_t v = bsum[b];
     bsum[b] = run;
