@@ -31,8 +31,8 @@
 // no table index can pass nsys whatever the offsets hold.
 //
 // Measured on B200 (FP64, 120 M unknowns, lengths log-uniform): 8 .. 256
-// rows 2.7 TB/s, 257 .. 1024 4.35, 1025 .. 4096 4.26, 4097 .. 8192 3.1, the
-// whole 8 .. 8192 range 3.39 TB/s algorithmic (200,000 systems: 3.58 TB/s).
+// rows 3.46 TB/s, 257 .. 1024 4.4-4.7, 1025 .. 4096 4.26, 4097 .. 8192 3.18,
+// the whole 8 .. 8192 range 3.48 TB/s algorithmic (200,000 systems: 3.63 TB/s).
 // Before the classes (every
 // system past 256 rows as 256-row block items reduced, published and
 // finished by a second queue across SMs, 72 B moved per unknown) the same
@@ -49,6 +49,7 @@ constexpr int kVLShort = kVarlenShort;   // longest system of the short queue
 constexpr int kVLMid = 512 * kVarlenCtaBuckets;  // longest system of the one-CTA buckets
 constexpr int kVLMaxBlocks = 32;         // longest solvable system: 32 blocks
 constexpr int kVLWarps = 8;              // warps per CTA of the short queue
+constexpr int kVLBatch = 4;              // short-queue items claimed per atomic
 constexpr int kVLLongWarps = 4;          // warps per CTA of the long systems (four CTAs per SM)
 constexpr int kVLRegion = 32 * (8 + 1);  // elements per staged array and warp
 constexpr int kVLLists = kVarlenCtaBuckets + 1;  // the one-CTA buckets, then the long list
@@ -367,14 +368,30 @@ __global__ void __launch_bounds__(kVLWarps * 32, 2) varlen_short_kernel(VLArgs<T
   const int lane = threadIdx.x & (kWarp - 1);
   T *reg = reinterpret_cast<T *>(vl_dyn) + (size_t)(threadIdx.x / kWarp) * 5 * kVLRegion;
   const int64_t nitems = *A.nitems;
-  unsigned long long claim = 0;
-  if (lane == 0) claim = atomicAdd(A.queue, 1ull);
-  int64_t it = (int64_t)__shfl_sync(0xffffffffu, claim, 0);
+  // items are claimed kVLBatch at a time (consecutive queue entries, so
+  // consecutive systems in memory), and the batch after the current one is
+  // requested as soon as the current one is taken: its atomic's result is
+  // read only kVLBatch items later, so the claim latency is hidden
+  unsigned long long first = 0, pending = 0;
+  if (lane == 0) {
+    first = atomicAdd(A.queue, (unsigned long long)kVLBatch);
+    pending = atomicAdd(A.queue, (unsigned long long)kVLBatch);
+  }
+  int64_t base = (int64_t)__shfl_sync(0xffffffffu, first, 0);
+  int k = 0;
+  int64_t it = base;
   VLItem cur = vl_item(A, it, nitems);
   vl_issue_item(A, reg, cur, lane);
   while (it < nitems) {
-    if (lane == 0) claim = atomicAdd(A.queue, 1ull);
-    const int64_t nit = (int64_t)__shfl_sync(0xffffffffu, claim, 0);
+    int64_t nit;
+    if (k + 1 < kVLBatch) {
+      nit = base + ++k;
+    } else {
+      base = (int64_t)__shfl_sync(0xffffffffu, pending, 0);
+      k = 0;
+      nit = base;
+      if (lane == 0) pending = atomicAdd(A.queue, (unsigned long long)kVLBatch);
+    }
     const VLItem nxt = vl_item(A, nit, nitems);
     if (cur.m == 2)
       vl_short_solve<T, 2>(A, reg, cur, nxt, lane);
