@@ -317,7 +317,7 @@ TRID_EXTERN_C tridStatus_t tridDmtsvVarlenBatchNoAlloc(const double *a, const do
  *   g2 = Y^{-T} g3, g1 = X^{-T} g2: ubar += lambda L^T g1 (the cotangent of
  *   u) and *lbar += <g1, L u> - <g1, X' du1> - <g2, Y' du2> - <g3, Z' du3>,
  *   X' = dX/dlambda (interior rows (da, db, dc): (-1/2, 1, -1/2) for the
- *   reference coefficients, (-1, 2, -1) for the baseline ones).  lbar is
+ *   reference coefficients, (-1, 2, -1) for the plain ones).  lbar is
  *   one device double, accumulated in place; the sum is formed in a fixed
  *   order (same result on every run). */
 TRID_EXTERN_C tridStatus_t tridDadiSteps(double *u, double *work, int nx, int ny, int nz,

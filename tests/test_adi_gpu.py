@@ -24,7 +24,7 @@ def ref_init(nz, ny, nx):
     return u
 
 
-@pytest.mark.parametrize("kind", ["baseline", "reference"])
+@pytest.mark.parametrize("kind", ["plain", "reference"])
 def test_adi_64cube_10_steps(kind):
     nz = ny = nx = 64
     lam = 1.0
@@ -43,7 +43,7 @@ def test_adi_64cube_10_steps(kind):
 def test_adi_odd_shapes(shape):
     nz, ny, nx = shape
     u0 = np.random.default_rng(2).uniform(0, 1, shape)
-    a, b, c = COEFFS["baseline"][0](0.7)
+    a, b, c = COEFFS["plain"][0](0.7)
     expect = oracle.adi(u0.ravel(), nx, ny, nz, 3, 0.7, a, b, c).reshape(shape)
     u = torch.from_numpy(u0.copy()).cuda()
     ADI(shape, 0.7).step(u, 3)
@@ -90,7 +90,7 @@ def _dense_step(u, lam, kind, mask):
     return u + du3
 
 
-@pytest.mark.parametrize("kind", ["baseline", "reference"])
+@pytest.mark.parametrize("kind", ["plain", "reference"])
 def test_adi_checkpointed_adjoint_against_dense_autograd(kind):
     shape = (7, 9, 10)
     steps, every, lam = 6, 4, 0.8

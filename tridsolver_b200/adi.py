@@ -5,7 +5,8 @@ The reference app (apps/adi/src/adi_orig.c:147-240) advances
 with L the interior-masked 7-point Laplacian and X, Y, Z tridiagonal along
 x, y, z: interior rows (a, b, c), face rows identity.  Two coefficient sets:
     "reference": a = c = -lambda/2, b = 1 + lambda   (the reference app)
-    "baseline":  a = c = -lambda,   b = 1 + 2*lambda
+    "plain":     a = c = -lambda,   b = 1 + 2*lambda   (the plain implicit step)
+("baseline" is accepted as another name of "plain").
 Tensors are (nz, ny, nx) contiguous CUDA tensors (x fastest).
 
 ADI.run(u, n, graph=True) captures one step in a CUDA graph and replays it;
@@ -37,8 +38,9 @@ register({
 
 COEFFS = {
     "reference": (lambda lam: (-0.5 * lam, 1.0 + lam, -0.5 * lam), (-0.5, 1.0, -0.5)),
-    "baseline": (lambda lam: (-lam, 1.0 + 2.0 * lam, -lam), (-1.0, 2.0, -1.0)),
+    "plain": (lambda lam: (-lam, 1.0 + 2.0 * lam, -lam), (-1.0, 2.0, -1.0)),
 }
+COEFFS["baseline"] = COEFFS["plain"]
 
 
 def _check(st, what):
@@ -47,7 +49,7 @@ def _check(st, what):
 
 
 class ADI:
-    def __init__(self, shape, lam, coeffs="baseline", dtype=torch.float64, device="cuda"):
+    def __init__(self, shape, lam, coeffs="plain", dtype=torch.float64, device="cuda"):
         self.nz, self.ny, self.nx = (int(v) for v in shape)
         self.lam = float(lam)
         self.kind = coeffs
