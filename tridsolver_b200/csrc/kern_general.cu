@@ -31,6 +31,8 @@
 // shared memory by coalesced copies) and strided axes
 // (SB adjacent systems per CTA, thread = (system, chunk), interface rows
 // transposed through shared memory so one warp solves one system's block).
+#include <string.h>
+
 #include "partition.cuh"
 
 namespace tridb200 {
@@ -299,6 +301,67 @@ __global__ void __launch_bounds__(128) gen_x_kernel(Geom g, GenArgs<T> A) {
 }
 
 // --------------------------------------------------------- strided axes --
+// Whole blocks of forward systems whose rows are 16-byte aligned in every
+// array: each lane moves its chunk of M rows (64 bytes per array) as 16-byte
+// words straight between global memory and registers, with no shared-memory
+// staging (the staged kernel above stalls on its shared-memory traffic).
+template <typename T, int M>
+__device__ __forceinline__ void gx_ld16(const T *p, T (&v)[M], bool nc) {
+  constexpr int K = M * (int)sizeof(T) / 16;
+  static_assert(K * 16 == M * (int)sizeof(T), "whole 16-byte words");
+  const uint4 *q = reinterpret_cast<const uint4 *>(p);
+  uint4 w[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) w[k] = nc ? __ldg(q + k) : q[k];
+  memcpy(v, w, sizeof(w));
+}
+template <typename T, int M>
+__device__ __forceinline__ void gx_st16(T *p, const T (&v)[M]) {
+  constexpr int K = M * (int)sizeof(T) / 16;
+  uint4 w[K];
+  memcpy(w, v, sizeof(w));
+  uint4 *q = reinterpret_cast<uint4 *>(p);
+#pragma unroll
+  for (int k = 0; k < K; ++k) q[k] = w[k];
+}
+
+template <typename T, int M, int MODE, int PHASE>
+__global__ void __launch_bounds__(128) gen_xv_kernel(Geom g, GenArgs<T> A) {
+  static_assert(MODE == kFwd || MODE == kFwdInc, "forward modes");
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int wi = threadIdx.x / kWarp;
+  const int64_t item = (int64_t)blockIdx.x * (blockDim.x / kWarp) + wi;
+  const int64_t sys = item / A.nblk;
+  const int blk = (int)(item % A.nblk);
+  if (sys >= g.nsys) return;  // uniform per warp
+  int64_t off[5];
+  system_offsets(g, sys, off);
+  const int n = g.n;
+  const int rbase = blk * 32 * M + lane * M;
+  T al[M], be[M], ga[M], de[M];
+  gx_ld16<T, M>(A.a + off[kA] + rbase, al, true);
+  gx_ld16<T, M>(A.b + off[kB] + rbase, be, true);
+  gx_ld16<T, M>(A.c + off[kC] + rbase, ga, true);
+  gx_ld16<T, M>(A.rhs + off[kD] + rbase, de, false);  // d may be the output
+  if (rbase == 0) al[0] = T(0);
+  if (rbase + M == n) ga[M - 1] = T(0);
+  Row<T> F, L;
+  chunk_reduce<T, M>(al, be, ga, de, F, L);
+  T xF, xL;
+  block_step<T, PHASE>(A, sys, blk, g.nsys, F, L, lane, xF, xL);
+  if (PHASE == kReduce) return;
+  chunk_backsub<T, M>(al, ga, de, xF, xL);
+  if constexpr (MODE == kFwdInc) {
+    T uo[M];
+    gx_ld16<T, M>(A.out + off[kU] + rbase, uo, false);
+#pragma unroll
+    for (int j = 0; j < M; ++j) uo[j] += de[j];
+    gx_st16<T, M>(A.out + off[kU] + rbase, uo);
+  } else {
+    gx_st16<T, M>(A.out + off[kD] + rbase, de);
+  }
+}
+
 template <typename T, int M, int SB, int MODE, int PHASE>
 __global__ void __launch_bounds__(SB * kWarp) gen_s_kernel(Geom g, GenArgs<T> A) {
   __shared__ T red[8][kWarp][SB + 1];
@@ -355,6 +418,22 @@ static cudaError_t go_x(const Geom &g, const GenArgs<T> &A, cudaStream_t st) {
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev >= 64) return cudaErrorNotSupported;
+  if constexpr ((MODE == kFwd || MODE == kFwdInc) && sizeof(T) == 4 && M == 16) {
+    // FP32 whole blocks with every array's rows 16-byte aligned in every
+    // system (2,048 x 65,536: 0.934 -> 0.778 ms; FP64 8-row chunks measured
+    // the same either way, 1.72 against 1.73 ms, and keep the staged kernel)
+    bool vec = g.n % (32 * M) == 0;
+    const void *ptrs[5] = {A.a, A.b, A.c, A.rhs, A.out};
+    const int arr[5] = {kA, kB, kC, kD, MODE == kFwdInc ? kU : kD};
+    for (int q = 0; q < 5 && vec; ++q) {
+      vec = ((uintptr_t)ptrs[q] & 15) == 0;
+      for (int k = 0; k < g.nod && vec; ++k) vec = (g.ocum[arr[q]][k] * (int64_t)sizeof(T)) % 16 == 0;
+    }
+    if (vec) {
+      gen_xv_kernel<T, M, MODE, PHASE><<<dim3((unsigned)blocks), dim3(kW * kWarp), 0, st>>>(g, A);
+      return cudaGetLastError();
+    }
+  }
   // whole blocks (only instantiated for the 256-row blocks of long systems)
   const bool full = M == 8 && g.n % (32 * M) == 0;
   auto kern = full ? gen_x_kernel<T, M, MODE, PHASE, (M == 8)> : gen_x_kernel<T, M, MODE, PHASE, false>;
